@@ -1,0 +1,149 @@
+"""Generate tests/golden/hexa8_svk.json from the reference's golden Checker case.
+
+The reference ships exactly one case that pins the Hexa8 element loop, the upper-CSR
+assembly, the rearrangement boundary conditions and the Newton driver:
+Checker/Cases/NonLinear_FEA_3D_Hexa8_StVenant (96 Hexa8 elements, 195 nodes, St Venant-
+Kirchhoff, 50 load steps).  This script reads its input files (GiD-12 Mesh.dat, tables,
+time discretization) and its expected outputs (MARC displacement curves of node 11,
+NumOfIterRef.dat, the per-iteration NORM lines of Log_CEOS.txt) and writes them as one JSON
+fixture, so that the tests never read the reference tree at run time.
+
+Usage:  python tests/golden/make_golden.py /path/to/reference
+"""
+import json
+import os
+import re
+import sys
+
+CASE = "Checker/Cases/NonLinear_FEA_3D_Hexa8_StVenant"
+
+
+def _lines(path):
+    with open(path, "r", encoding="latin-1") as f:
+        return [ln.rstrip("\n") for ln in f]
+
+
+def read_mesh(path):
+    """Minimal GiD-12 reader (ModReadInputFile.f90:1396-1561, 1565-1709)."""
+    L = [ln.strip() for ln in _lines(path)]
+    i = 0
+    coords, conn, mat = {}, {}, {}
+    fixed, loads, disps = [], [], []
+    while i < len(L):
+        s = L[i].upper()
+        if s == "COORDINATES":
+            i += 1
+            while L[i].upper() != "END COORDINATES":
+                t = L[i].split()
+                coords[int(t[0])] = [float(v) for v in t[1:4]]
+                i += 1
+        elif s == "MATERIAL ID":
+            i += 2
+            while L[i].upper() != "END MATERIAL ID":
+                t = L[i].split()
+                mat[int(t[0])] = int(t[1])
+                i += 1
+        elif s == "CONNECTIVITY":
+            i += 1
+            while L[i].upper() != "END CONNECTIVITY":
+                t = [int(v) for v in L[i].split()]
+                conn[t[0]] = t[3:3 + t[2]]
+                i += 1
+        elif s == "FIXED SUPPORTS":
+            n = int(L[i + 1])
+            for k in range(n):
+                t = [int(v) for v in L[i + 2 + k].split()]
+                fixed.append(t)
+            i += 1 + n
+        elif s == "NODAL LOAD":
+            n = int(L[i + 1])
+            for k in range(n):
+                t = L[i + 2 + k].split()
+                loads.append([int(t[0])] + [[int(t[1 + 2 * d]), t[2 + 2 * d]] for d in range(3)])
+            i += 1 + n
+        elif s == "NODAL DISPLACEMENT":
+            n = int(L[i + 1])
+            for k in range(n):
+                t = L[i + 2 + k].split()
+                disps.append([int(t[0])] + [[int(t[1 + 2 * d]), t[2 + 2 * d]] for d in range(3)])
+            i += 1 + n
+        i += 1
+    nn, ne = len(coords), len(conn)
+    return {
+        "X": [c for k in range(1, nn + 1) for c in coords[k]],
+        "conn": [n for e in range(1, ne + 1) for n in conn[e]],
+        "mat_id": [mat[e] for e in range(1, ne + 1)],
+        "fixed": fixed,
+        "loads": loads,
+        "disps": disps,
+    }
+
+
+def read_table(path):
+    rows = []
+    for ln in _lines(path):
+        t = ln.split()
+        if len(t) >= 2:
+            try:
+                rows.append([float(t[0].replace("d", "e").replace("D", "e")),
+                             float(t[1].replace("d", "e").replace("D", "e"))])
+            except ValueError:
+                pass
+    return rows
+
+
+def read_two_cols(path):
+    out = []
+    for ln in _lines(path):
+        t = ln.split()
+        if len(t) >= 2:
+            try:
+                out.append([float(t[0]), float(t[1])])
+            except ValueError:
+                pass
+    return out
+
+
+def read_log_norms(path):
+    steps, cur = [], None
+    for ln in _lines(path):
+        m = re.match(r"\s*Step:\s+(\d+)", ln)
+        if m and "End" not in ln:
+            cur = []
+            steps.append(cur)
+        m = re.search(r"IT:\s+(\d+)\s+NORM:\s+([0-9.Ee+-]+)", ln)
+        if m and cur is not None:
+            cur.append(float(m.group(2)))
+    return steps
+
+
+def main(ref):
+    case = os.path.join(ref, CASE)
+    mesh = read_mesh(os.path.join(case, "Mesh.dat"))
+    fx = {
+        "source": CASE,
+        "material": {"model": "St_Venant_Kirchhoff", "YoungModulus": 100.0e9, "Poisson": 0.3},
+        "newton": {"tol": 1e-3, "itmax": 10, "max_cutbacks": 10},
+        "time": {"t0": 0.0, "t1": 1.0, "steps": 50},
+        "probe_node": 11,
+        "tables": {
+            "Table_Disp_Z": read_table(os.path.join(case, "Table_Disp_Z.tab")),
+            "Table_Load_Y": read_table(os.path.join(case, "Table_Load_Y.tab")),
+        },
+        "marc": {
+            "x": read_two_cols(os.path.join(case, "marc_disp_x.dat")),
+            "y": read_two_cols(os.path.join(case, "marc_disp_y.dat")),
+            "z": read_two_cols(os.path.join(case, "marc_disp_z.dat")),
+        },
+        "iterations_ref": read_two_cols(os.path.join(case, "NumOfIterRef.dat")),
+        "log_norms": read_log_norms(os.path.join(case, "Log_CEOS.txt")),
+    }
+    fx.update(mesh)
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hexa8_svk.json")
+    with open(out, "w") as f:
+        json.dump(fx, f, separators=(",", ":"))
+    print("wrote", out, "nodes", len(mesh["X"]) // 3, "elements", len(mesh["conn"]) // 8)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
