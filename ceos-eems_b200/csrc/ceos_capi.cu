@@ -1,0 +1,631 @@
+// ceos_capi.cu -- the C ABI (include/ceos_gpu.h): handle, CSR pattern, slot map, launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ceos_gpu.h"
+#include "ceos_handle.h"
+#include "element_kernel.cuh"
+
+namespace ceos {
+
+
+namespace {
+
+// dN table with the arithmetic of GetDifShapeFunctions_Hexa8 (ModElementHexa8.f90:211-268)
+// at the points of AllocateGaussPointsParameters_Hexa8 (:278-329).
+void hexa8_dN_table(double out[8][8][3]) {
+    const double x = 1.0 / std::sqrt(3.0);
+    for (int gp = 0; gp < 8; ++gp) {
+        const double xi = kSign[gp][0] * x, eta = kSign[gp][1] * x, zeta = kSign[gp][2] * x;
+        for (int i = 0; i < 8; ++i) {
+            out[gp][i][0] = kSign[i][0] * (1.0 + kSign[i][1] * eta) * (1.0 + kSign[i][2] * zeta) / 8.0;
+            out[gp][i][1] = kSign[i][1] * (1.0 + kSign[i][0] * xi) * (1.0 + kSign[i][2] * zeta) / 8.0;
+            out[gp][i][2] = kSign[i][2] * (1.0 + kSign[i][0] * xi) * (1.0 + kSign[i][1] * eta) / 8.0;
+        }
+    }
+}
+
+int model_nparams(int model) {
+    switch (model) {
+        case M_CNH: return ModelInfo<M_CNH>::nparams;
+        case M_SVK: return ModelInfo<M_SVK>::nparams;
+        case M_J2_SMALL: return ModelInfo<M_J2_SMALL>::nparams;
+        case M_VISCO_PRONY: return ModelInfo<M_VISCO_PRONY>::nparams;
+        case M_J2_FINITE: return ModelInfo<M_J2_FINITE>::nparams;
+    }
+    return -1;
+}
+int model_nstate(int model) {
+    switch (model) {
+        case M_CNH: return 0;
+        case M_SVK: return 0;
+        case M_J2_SMALL: return ModelInfo<M_J2_SMALL>::nstate;
+        case M_VISCO_PRONY: return ModelInfo<M_VISCO_PRONY>::nstate;
+        case M_J2_FINITE: return ModelInfo<M_J2_FINITE>::nstate;
+    }
+    return -1;
+}
+void model_init_state(int model, double* st) {
+    const int ns = model_nstate(model);
+    for (int i = 0; i < ns; ++i) st[i] = 0.0;
+    if (model == M_J2_FINITE) st[0] = st[1] = st[2] = 1.0;  // Cp^{-1} = I
+}
+
+#define CK(call)                                                              \
+    do {                                                                      \
+        cudaError_t err_ = (call);                                            \
+        if (err_ != cudaSuccess) {                                            \
+            h->msg = std::string(#call) + ": " + cudaGetErrorString(err_);   \
+            return CEOS_E_CUDA;                                               \
+        }                                                                     \
+    } while (0)
+
+template <typename T>
+size_t elem_smem() { return sizeof(ElemSmem<T>); }
+
+template <typename T, int MODEL>
+int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
+    ElemArgs<T> a;
+    a.n_elem = h->n_elem;
+    a.X = h->d_X;
+    a.U = dU;
+    a.conn = h->d_conn;
+    a.rs = h->d_rs;
+    a.nup = h->d_nup;
+    a.ranks = h->d_ranks;
+    a.fint = dfint;
+    a.kval = dkval;
+    a.st_old = reinterpret_cast<const T*>(h->d_state[h->cur_old]);
+    a.st_new = reinterpret_cast<T*>(h->d_state[1 - h->cur_old]);
+    a.params = reinterpret_cast<const T*>(h->d_params);
+    a.param_mode = h->param_mode;
+    a.n_params = h->n_params;
+    a.mat_id = h->d_mat_id;
+    a.dt = dt;
+    a.elem_status = h->d_elem_status;
+    a.status_count = h->d_status_count;
+    a.gp_stress = (h->options & CEOS_OPT_STORE_STRESS) ? reinterpret_cast<T*>(h->d_gp_stress) : nullptr;
+    const size_t smem = elem_smem<T>();
+    static bool attr_set = false;
+    if (!attr_set) {
+        CK(cudaFuncSetAttribute(element_loop_kernel<T, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    const int n_tiles = (h->n_elem + kTileE - 1) / kTileE;
+    int grid = std::min(n_tiles, h->grid_cap);
+    element_loop_kernel<T, MODEL><<<grid, kThreads, smem, s>>>(a);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+template <typename T>
+int launch_elem(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
+    switch (h->model) {
+        case M_CNH: return launch_model<T, M_CNH>(h, dt, dU, dfint, dkval, s);
+        case M_SVK: return launch_model<T, M_SVK>(h, dt, dU, dfint, dkval, s);
+        case M_J2_SMALL: return launch_model<T, M_J2_SMALL>(h, dt, dU, dfint, dkval, s);
+        case M_VISCO_PRONY: return launch_model<T, M_VISCO_PRONY>(h, dt, dU, dfint, dkval, s);
+        case M_J2_FINITE: return launch_model<T, M_J2_FINITE>(h, dt, dU, dfint, dkval, s);
+    }
+    return CEOS_E_MODEL;
+}
+
+template <typename T>
+int occupancy_grid(Handle* h) {
+    int per_sm = 1, dev = h->device, sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaSuccess;
+    switch (h->model) {
+        case M_CNH:
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_CNH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>());
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_CNH>, kThreads, elem_smem<T>());
+            break;
+        case M_SVK:
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_SVK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>());
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_SVK>, kThreads, elem_smem<T>());
+            break;
+        case M_J2_SMALL:
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_J2_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>());
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_J2_SMALL>, kThreads, elem_smem<T>());
+            break;
+        case M_VISCO_PRONY:
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_VISCO_PRONY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>());
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_VISCO_PRONY>, kThreads, elem_smem<T>());
+            break;
+        case M_J2_FINITE:
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_J2_FINITE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>());
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_J2_FINITE>, kThreads, elem_smem<T>());
+            break;
+    }
+    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    h->blocks_per_sm = per_sm;
+    return sms * per_sm;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// CSR pattern of AllocateKgSparseUpperTriangular (ModFEMAnalysis.f90:209-273): row 3n+k holds,
+// in increasing order, the columns 3n+k..3n+2 of its own node and the three DOFs of every
+// neighbour node with a larger id.  Built from sorted node adjacency lists, which gives the
+// same sorted distinct columns as the reference's per-row linked lists
+// (ModSparseVectorRoutines.f90:222-312) filtered to col >= row
+// (ModSparseMatrixRoutines.f90:573-609).
+// ---------------------------------------------------------------------------------------
+int build_pattern(Handle* h, const int* conn1) {
+    const int N = h->n_nodes, E = h->n_elem;
+    std::vector<int> deg(N + 1, 0);
+    // upper neighbours of each node: count candidate pairs, then sort + unique
+    std::vector<long long> cnt(N + 1, 0);
+    for (int e = 0; e < E; ++e)
+        for (int i = 0; i < 8; ++i) {
+            const int a = conn1[8 * e + i] - 1;
+            for (int j = 0; j < 8; ++j) {
+                const int b = conn1[8 * e + j] - 1;
+                if (b > a) cnt[a + 1]++;
+            }
+        }
+    for (int n = 0; n < N; ++n) cnt[n + 1] += cnt[n];
+    std::vector<int> buf(cnt[N]);
+    std::vector<long long> fill(cnt.begin(), cnt.end() - 1);
+    std::vector<char> used(N, 0);
+    for (int e = 0; e < E; ++e)
+        for (int i = 0; i < 8; ++i) {
+            const int a = conn1[8 * e + i] - 1;
+            used[a] = 1;
+            for (int j = 0; j < 8; ++j) {
+                const int b = conn1[8 * e + j] - 1;
+                if (b > a) buf[fill[a]++] = b;
+            }
+        }
+    for (int n = 0; n < N; ++n)
+        if (!used[n]) {
+            h->msg = "node " + std::to_string(n + 1) + " belongs to no element";
+            return CEOS_E_MESH;
+        }
+    h->up_ptr.assign(N + 1, 0);
+    h->up_list.clear();
+    h->up_list.reserve(cnt[N] / 4 + 16);
+    for (int n = 0; n < N; ++n) {
+        auto b0 = buf.begin() + cnt[n], b1 = buf.begin() + cnt[n + 1];
+        std::sort(b0, b1);
+        auto last = std::unique(b0, b1);
+        h->up_list.insert(h->up_list.end(), b0, last);
+        h->up_ptr[n + 1] = (long long)h->up_list.size();
+    }
+    // node row starts: row 3n has 3 + 3m entries, row 3n+1 2 + 3m, row 3n+2 1 + 3m
+    h->rs.assign(N, 0);
+    h->nup.assign(N, 0);
+    long long pos = 0;
+    for (int n = 0; n < N; ++n) {
+        const int m = (int)(h->up_ptr[n + 1] - h->up_ptr[n]);
+        h->rs[n] = pos;
+        h->nup[n] = m;
+        pos += 6 + 9LL * m;
+        if (m > 255) {
+            h->msg = "node with more than 255 neighbours";
+            return CEOS_E_MESH;
+        }
+    }
+    h->nnz = pos;
+    // per element: rank of the larger node among the smaller node's upper neighbours
+    h->ranks.assign((size_t)E * 32, 0);
+    for (int e = 0; e < E; ++e)
+        for (int i = 0; i < 8; ++i)
+            for (int j = i + 1; j < 8; ++j) {
+                const int A = conn1[8 * e + i] - 1, B = conn1[8 * e + j] - 1;
+                if (A == B) {
+                    h->msg = "element " + std::to_string(e + 1) + " repeats a node";
+                    return CEOS_E_MESH;
+                }
+                const int lo = std::min(A, B), hi = std::max(A, B);
+                const int* b0 = h->up_list.data() + h->up_ptr[lo];
+                const int* b1 = h->up_list.data() + h->up_ptr[lo + 1];
+                const int r = (int)(std::lower_bound(b0, b1, hi) - b0);
+                h->ranks[(size_t)e * 32 + pair_index(i, j)] = (uint8_t)r;
+            }
+    return 0;
+}
+
+}  // namespace ceos
+
+using namespace ceos;
+
+extern "C" int ceos_create(const ceos_mesh* mesh, const ceos_material* mats, int n_mat, int precision_mode,
+                           int device, void** handle) {
+    if (!mesh || !mats || n_mat < 1 || !handle || mesh->n_nodes < 1 || mesh->n_elem < 1 || !mesh->X || !mesh->conn)
+        return CEOS_E_ARG;
+    if (precision_mode != CEOS_FP64 && precision_mode != CEOS_MIXED) return CEOS_E_ARG;
+    Handle* h = new Handle();
+    *handle = nullptr;
+    h->n_nodes = mesh->n_nodes;
+    h->n_elem = mesh->n_elem;
+    h->precision = precision_mode;
+    h->device = device;
+    h->model = mats[0].model;
+    for (int k = 0; k < n_mat; ++k)
+        if (mats[k].model != h->model) { delete h; return CEOS_E_MODEL; }
+    h->n_params = model_nparams(h->model);
+    h->nstate = model_nstate(h->model);
+    if (h->n_params < 0) { delete h; return CEOS_E_MODEL; }
+    for (int k = 0; k < n_mat; ++k)
+        if (mats[k].n_params < h->n_params || !mats[k].params) { delete h; return CEOS_E_ARG; }
+    for (long long i = 0; i < 8LL * mesh->n_elem; ++i)
+        if (mesh->conn[i] < 1 || mesh->conn[i] > mesh->n_nodes) { delete h; return CEOS_E_MESH; }
+    int rc = build_pattern(h, mesh->conn);
+    if (rc) { std::fprintf(stderr, "ceos_create: %s\n", h->msg.c_str()); delete h; return rc; }
+    cudaError_t ce = cudaSetDevice(device);
+    if (ce != cudaSuccess) { delete h; return CEOS_E_CUDA; }
+    rc = h->allocate_device(mesh, mats, n_mat);
+    if (rc) { std::fprintf(stderr, "ceos_create: %s\n", h->msg.c_str()); delete h; return rc; }
+    h->grid_cap = (precision_mode == CEOS_FP64) ? occupancy_grid<double>(h) : occupancy_grid<float>(h);
+    {
+        double tab[8][8][3];
+        hexa8_dN_table(tab);
+        if (cudaMemcpyToSymbol(c_dN, tab, sizeof(tab)) != cudaSuccess) { delete h; return CEOS_E_CUDA; }
+    }
+    *handle = h;
+    return 0;
+}
+
+extern "C" int ceos_pattern(void* handle, int* n_dof, long long* nnz, int* rowmap, int* col, int* row) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h) return CEOS_E_ARG;
+    const int N = h->n_nodes;
+    if (n_dof) *n_dof = 3 * N;
+    if (nnz) *nnz = h->nnz;
+    if (h->nnz > 2147483646LL && (rowmap || col || row)) return CEOS_E_ARG;  // 1-based int32 export
+    long long k = 0;
+    for (int n = 0; n < N; ++n) {
+        const long long b0 = h->up_ptr[n], b1 = h->up_ptr[n + 1];
+        for (int r = 0; r < 3; ++r) {
+            const int irow = 3 * n + r + 1;
+            if (rowmap) rowmap[irow - 1] = (int)(k + 1);
+            for (int c = r; c < 3; ++c) {
+                if (col) col[k] = 3 * n + c + 1;
+                if (row) row[k] = irow;
+                ++k;
+            }
+            for (long long q = b0; q < b1; ++q)
+                for (int c = 0; c < 3; ++c) {
+                    if (col) col[k] = 3 * h->up_list[q] + c + 1;
+                    if (row) row[k] = irow;
+                    ++k;
+                }
+        }
+    }
+    if (rowmap) rowmap[3 * N] = (int)(h->nnz + 1);
+    return 0;
+}
+
+extern "C" int ceos_slot_map(void* handle, long long* out) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !out) return CEOS_E_ARG;
+    // The same arithmetic the kernel uses (element_kernel.cuh, phase B scatter).
+    for (int e = 0; e < h->n_elem; ++e) {
+        long long* o = out + (size_t)e * 576;
+        for (int i = 0; i < 576; ++i) o[i] = -1;
+        for (int a = 0; a < 8; ++a)
+            for (int b = 0; b < 8; ++b) {
+                const int A = h->conn0[8 * (size_t)e + a], B = h->conn0[8 * (size_t)e + b];
+                if (A > B) continue;
+                const long long r0 = h->rs[A];
+                const int m = h->nup[A];
+                const long long rowstart[3] = {r0, r0 + 3 + 3 * m, r0 + 5 + 6LL * m};
+                for (int k = 0; k < 3; ++k)
+                    for (int l = 0; l < 3; ++l) {
+                        long long pos;
+                        if (A == B) {
+                            if (l < k) continue;
+                            pos = rowstart[k] + (l - k);
+                        } else {
+                            const int r = h->ranks[(size_t)e * 32 + pair_index(std::min(a, b), std::max(a, b))];
+                            pos = rowstart[k] + (3 - k) + 3 * r + l;
+                        }
+                        o[(3 * a + k) * 24 + 3 * b + l] = pos;
+                    }
+            }
+    }
+    return 0;
+}
+
+namespace ceos {
+int evaluate_device(Handle* h, double time, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
+    CK(cudaSetDevice(h->device));
+    const double dt = time - h->time_old;
+    h->time_eval = time;
+    CK(cudaMemsetAsync(h->d_status_count, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(dfint, 0, sizeof(double) * 3 * (size_t)h->n_nodes, s));
+    if (dkval) CK(cudaMemsetAsync(dkval, 0, sizeof(double) * (size_t)h->nnz, s));
+    int rc = (h->precision == CEOS_FP64) ? launch_elem<double>(h, dt, dU, dfint, dkval, s)
+                                         : launch_elem<float>(h, dt, dU, dfint, dkval, s);
+    if (rc) return rc;
+    h->evaluated = true;
+    return 0;
+}
+}  // namespace ceos
+
+extern "C" int ceos_evaluate_device(void* handle, double time, const double* U_device, double* fint_device,
+                                    double* kval_device, void* stream) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !U_device || !fint_device) return CEOS_E_ARG;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    return evaluate_device(h, time, U_device, fint_device, kval_device, s);
+}
+
+extern "C" int ceos_status(void* handle, int* n_failed) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h) return CEOS_E_ARG;
+    int cnt = 0;
+    CK(cudaMemcpy(&cnt, h->d_status_count, sizeof(int), cudaMemcpyDeviceToHost));
+    if (n_failed) *n_failed = cnt;
+    if (!cnt) return 0;
+    std::vector<uint8_t> st(h->n_elem);
+    CK(cudaMemcpy(st.data(), h->d_elem_status, h->n_elem, cudaMemcpyDeviceToHost));
+    int worst = 0;
+    for (uint8_t v : st) worst |= v;
+    if (worst & 1) return 1;
+    if (worst & 2) return 2;
+    return 3;
+}
+
+extern "C" int ceos_evaluate(void* handle, double time, const double* U, double* fint, double* kval, int* n_failed) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !U || !fint) return CEOS_E_ARG;
+    CK(cudaSetDevice(h->device));
+    cudaStream_t s = h->stream;
+    const size_t nd = 3 * (size_t)h->n_nodes;
+    CK(cudaMemcpyAsync(h->d_U, U, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+    int rc = evaluate_device(h, time, h->d_U, h->d_fint, kval ? h->d_kval : nullptr, s);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(fint, h->d_fint, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (kval) CK(cudaMemcpyAsync(kval, h->d_kval, (size_t)h->nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return ceos_status(handle, n_failed);
+}
+
+extern "C" int ceos_commit_state(void* handle) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h) return CEOS_E_ARG;
+    // The state written by the last evaluation becomes the committed one (the reference copies
+    // new into old; swapping the buffers is the same as long as an evaluation happened since the
+    // last commit, which the flag guarantees).
+    if (h->evaluated) {
+        h->cur_old = 1 - h->cur_old;
+        h->evaluated = false;
+        CK(cudaSetDevice(h->device));
+        if (h->nstate)
+            CK(cudaMemcpyAsync(h->d_state[1 - h->cur_old], h->d_state[h->cur_old], h->state_bytes(),
+                               cudaMemcpyDeviceToDevice, h->stream));
+    }
+    h->time_old = h->time_eval;
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+extern "C" int ceos_set_committed_time(void* handle, double t) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h) return CEOS_E_ARG;
+    h->time_old = t;
+    h->time_eval = t;
+    return 0;
+}
+
+extern "C" int ceos_last_error(void* handle, int* elem_ids, int max_ids, char* msg, int msg_len) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h) return CEOS_E_ARG;
+    std::vector<uint8_t> st(h->n_elem);
+    CK(cudaMemcpy(st.data(), h->d_elem_status, h->n_elem, cudaMemcpyDeviceToHost));
+    int n = 0, worst = 0;
+    for (int e = 0; e < h->n_elem; ++e)
+        if (st[e]) {
+            if (elem_ids && n < max_ids) elem_ids[n] = e + 1;
+            ++n;
+            worst |= st[e];
+        }
+    if (msg && msg_len > 0) {
+        std::string m;
+        if (!n) m = h->msg.empty() ? "no error" : h->msg;
+        else if (worst & 1) m = "Determinant of the Jacobian Matrix <= 0.0d0 in " + std::to_string(n) + " element(s)";
+        else if (worst & 2) m = "Max Iteration in Local Newton-Raphson in " + std::to_string(n) + " element(s)";
+        else m = "Non-finite stress in " + std::to_string(n) + " element(s)";
+        std::strncpy(msg, m.c_str(), msg_len - 1);
+        msg[msg_len - 1] = 0;
+    }
+    return n;
+}
+
+extern "C" int ceos_state_size(void* handle, int* nvars) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !nvars) return CEOS_E_ARG;
+    *nvars = h->nstate;
+    return 0;
+}
+
+extern "C" int ceos_get_state(void* handle, int which, double* out) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !out) return CEOS_E_ARG;
+    if (!h->nstate) return 0;
+    const int buf = which ? 1 - h->cur_old : h->cur_old;
+    const size_t n = (size_t)h->nstate * 8 * h->n_elem;
+    std::vector<double> tmp(n);
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->precision == CEOS_FP64) {
+        CK(cudaMemcpy(tmp.data(), h->d_state[buf], n * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> f(n);
+        CK(cudaMemcpy(f.data(), h->d_state[buf], n * sizeof(float), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; ++i) tmp[i] = f[i];
+    }
+    // device [v][gp][e] -> host [e][gp][v]
+    const int E = h->n_elem, V = h->nstate;
+    for (int v = 0; v < V; ++v)
+        for (int g = 0; g < 8; ++g)
+            for (int e = 0; e < E; ++e) out[((size_t)e * 8 + g) * V + v] = tmp[((size_t)v * 8 + g) * E + e];
+    return 0;
+}
+
+extern "C" int ceos_set_state(void* handle, int which, const double* in) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !in) return CEOS_E_ARG;
+    if (!h->nstate) return 0;
+    const int buf = which ? 1 - h->cur_old : h->cur_old;
+    const int E = h->n_elem, V = h->nstate;
+    const size_t n = (size_t)V * 8 * E;
+    std::vector<double> tmp(n);
+    for (int v = 0; v < V; ++v)
+        for (int g = 0; g < 8; ++g)
+            for (int e = 0; e < E; ++e) tmp[((size_t)v * 8 + g) * E + e] = in[((size_t)e * 8 + g) * V + v];
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->precision == CEOS_FP64) {
+        CK(cudaMemcpy(h->d_state[buf], tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(tmp.begin(), tmp.end());
+        CK(cudaMemcpy(h->d_state[buf], f.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return 0;
+}
+
+extern "C" int ceos_set_options(void* handle, int options) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h) return CEOS_E_ARG;
+    h->options = options;
+    if ((options & CEOS_OPT_STORE_STRESS) && !h->d_gp_stress) {
+        CK(cudaSetDevice(h->device));
+        CK(cudaMalloc(&h->d_gp_stress, (size_t)6 * 8 * h->n_elem * h->elem_bytes()));
+    }
+    return 0;
+}
+
+extern "C" int ceos_gp_stress(void* handle, double* out) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !out || !h->d_gp_stress) return CEOS_E_ARG;
+    const int E = h->n_elem;
+    const size_t n = (size_t)6 * 8 * E;
+    std::vector<double> tmp(n);
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->precision == CEOS_FP64) {
+        CK(cudaMemcpy(tmp.data(), h->d_gp_stress, n * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> f(n);
+        CK(cudaMemcpy(f.data(), h->d_gp_stress, n * sizeof(float), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; ++i) tmp[i] = f[i];
+    }
+    for (int k = 0; k < 6; ++k)
+        for (int g = 0; g < 8; ++g)
+            for (int e = 0; e < E; ++e) out[((size_t)e * 8 + g) * 6 + k] = tmp[((size_t)k * 8 + g) * E + e];
+    return 0;
+}
+
+extern "C" void ceos_destroy(void* handle) {
+    Handle* h = static_cast<Handle*>(handle);
+    delete h;
+}
+
+// ---------------------------------------------------------------------------------------
+// Device allocation (Handle::allocate_device)
+// ---------------------------------------------------------------------------------------
+namespace ceos {
+
+int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, int n_mat) {
+    Handle* h = this;
+    const size_t N = n_nodes, E = n_elem;
+    conn0.resize(8 * E);
+    for (size_t i = 0; i < 8 * E; ++i) conn0[i] = mesh->conn[i] - 1;
+    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CK(cudaMalloc(&d_X, 3 * N * sizeof(double)));
+    CK(cudaMemcpy(d_X, mesh->X, 3 * N * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&d_U, 3 * N * sizeof(double)));
+    CK(cudaMemset(d_U, 0, 3 * N * sizeof(double)));
+    CK(cudaMalloc(&d_fint, 3 * N * sizeof(double)));
+    CK(cudaMalloc(&d_kval, (size_t)nnz * sizeof(double)));
+    CK(cudaMalloc(&d_conn, 8 * E * sizeof(int)));
+    CK(cudaMemcpy(d_conn, conn0.data(), 8 * E * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&d_rs, N * sizeof(long long)));
+    CK(cudaMemcpy(d_rs, rs.data(), N * sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&d_nup, N * sizeof(int)));
+    CK(cudaMemcpy(d_nup, nup.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&d_ranks, E * 32));
+    CK(cudaMemcpy(d_ranks, ranks.data(), E * 32, cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&d_elem_status, E));
+    CK(cudaMemset(d_elem_status, 0, E));
+    CK(cudaMalloc(&d_status_count, sizeof(int)));
+    CK(cudaMemset(d_status_count, 0, sizeof(int)));
+    // parameters
+    const size_t eb = elem_bytes();
+    std::vector<double> P;
+    bool any_per_element = false;
+    for (int k = 0; k < n_mat; ++k) any_per_element |= mats[k].per_element != 0;
+    if (any_per_element) {
+        param_mode = 1;
+        P.assign((size_t)n_params * E, 0.0);
+        for (size_t e = 0; e < E; ++e) {
+            const int mid = mesh->mat_id ? mesh->mat_id[e] : 0;
+            if (mid < 0 || mid >= n_mat) { msg = "bad mat_id"; return CEOS_E_MESH; }
+            const ceos_material& m = mats[mid];
+            const double* src = m.per_element ? m.params + e * (size_t)m.n_params : m.params;
+            for (int k = 0; k < n_params; ++k) P[(size_t)k * E + e] = src[k];
+        }
+    } else if (n_mat == 1) {
+        param_mode = 0;
+        P.assign(mats[0].params, mats[0].params + n_params);
+    } else {
+        param_mode = 2;
+        P.resize((size_t)n_mat * n_params);
+        for (int m = 0; m < n_mat; ++m)
+            for (int k = 0; k < n_params; ++k) P[(size_t)m * n_params + k] = mats[m].params[k];
+        std::vector<int> mid(E);
+        for (size_t e = 0; e < E; ++e) {
+            mid[e] = mesh->mat_id ? mesh->mat_id[e] : 0;
+            if (mid[e] < 0 || mid[e] >= n_mat) { msg = "bad mat_id"; return CEOS_E_MESH; }
+        }
+        CK(cudaMalloc(&d_mat_id, E * sizeof(int)));
+        CK(cudaMemcpy(d_mat_id, mid.data(), E * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    host_params = P;
+    CK(cudaMalloc(&d_params, P.size() * eb));
+    if (precision == CEOS_FP64) {
+        CK(cudaMemcpy(d_params, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(P.begin(), P.end());
+        CK(cudaMemcpy(d_params, f.data(), P.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    // state: virgin state in both buffers, device layout [v][gp][e]
+    if (nstate) {
+        std::vector<double> init(nstate);
+        model_init_state(model, init.data());
+        std::vector<double> S((size_t)nstate * 8 * E);
+        for (int v = 0; v < nstate; ++v)
+            std::fill(S.begin() + (size_t)v * 8 * E, S.begin() + (size_t)(v + 1) * 8 * E, init[v]);
+        for (int b = 0; b < 2; ++b) {
+            CK(cudaMalloc(&d_state[b], state_bytes()));
+            if (precision == CEOS_FP64) {
+                CK(cudaMemcpy(d_state[b], S.data(), state_bytes(), cudaMemcpyHostToDevice));
+            } else {
+                std::vector<float> f(S.begin(), S.end());
+                CK(cudaMemcpy(d_state[b], f.data(), state_bytes(), cudaMemcpyHostToDevice));
+            }
+        }
+    }
+    return 0;
+}
+
+Handle::~Handle() {
+    if (stream) cudaStreamSynchronize(stream);
+    void* ptrs[] = {d_X, d_U, d_fint, d_kval, d_conn, d_rs, d_nup, d_ranks, d_elem_status, d_status_count,
+                    d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+}  // namespace ceos

@@ -1,0 +1,53 @@
+// ceos_handle.h -- the state behind one ceos_gpu.h handle.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/ceos_gpu.h"
+
+namespace ceos {
+
+struct Handle {
+    // mesh and pattern (host copies)
+    int n_nodes = 0, n_elem = 0, precision = 0, device = 0, model = 0, n_params = 0, nstate = 0;
+    long long nnz = 0;
+    std::vector<int> conn0;               // [8*n_elem] 0-based
+    std::vector<long long> up_ptr;        // upper-neighbour lists (CSR over nodes)
+    std::vector<int> up_list;
+    std::vector<long long> rs;            // CSR position of row 3n
+    std::vector<int> nup;                 // number of upper neighbours of node n
+    std::vector<uint8_t> ranks;           // [n_elem*32] slot ranks per local pair
+    std::vector<double> host_params;
+    int param_mode = 0;
+    // device buffers
+    cudaStream_t stream = nullptr;
+    double *d_X = nullptr, *d_U = nullptr, *d_fint = nullptr, *d_kval = nullptr;
+    int* d_conn = nullptr;
+    long long* d_rs = nullptr;
+    int* d_nup = nullptr;
+    uint32_t* d_ranks = nullptr;
+    uint8_t* d_elem_status = nullptr;
+    int* d_status_count = nullptr;
+    void* d_params = nullptr;
+    int* d_mat_id = nullptr;
+    void* d_state[2] = {nullptr, nullptr};
+    void* d_gp_stress = nullptr;
+    int cur_old = 0;                      // index of the committed state buffer
+    bool evaluated = false;
+    double time_old = 0.0, time_eval = 0.0;
+    int options = 0;
+    int grid_cap = 148, blocks_per_sm = 1;
+    std::string msg;
+
+    size_t elem_bytes() const { return precision == CEOS_FP64 ? sizeof(double) : sizeof(float); }
+    size_t state_bytes() const { return (size_t)nstate * 8 * n_elem * elem_bytes(); }
+    int allocate_device(const ceos_mesh* mesh, const ceos_material* mats, int n_mat);
+    ~Handle();
+};
+
+int evaluate_device(Handle* h, double time, const double* dU, double* dfint, double* dkval, cudaStream_t s);
+
+}  // namespace ceos

@@ -1,0 +1,144 @@
+/*
+ * ceos_gpu.h -- C ABI of the B200 (sm_100a) element loop for CEOS.
+ *
+ * Replaces, as a drop-in, the three serial passes that the CEOS Newton "system of
+ * equations" plugin runs per iteration (reference paths relative to SourceCode/):
+ *   SolveConstitutiveModel  FEM/Subroutines/SubSolveConstitutiveModel.f90:13
+ *   InternalForce           FEM/Subroutines/SubInternalForce.f90:13
+ *   TangentStiffnessMatrix  FEM/Subroutines/SubTangentStiffnessMatrix.f90:13 (FEM branch :294-311)
+ *     + AssembleGlobalMatrixUpperTriangular  FEM/Subroutines/SubAssembleGlobalMatrixUpperTriangular.f90:13
+ * as called by EvaluateR / EvaluateKt (FEM/Modules/ModFEMSystemOfEquations.f90:40-93), and the
+ * CSR allocation AllocateKgSparseUpperTriangular (FEM/ModFEMAnalysis.f90:209-273).
+ *
+ * Conventions follow the reference's ClassGlobalSparseMatrix (Tools/MathTools/
+ * SparseMatrixRoutines/ModGlobalSparseMatrix.f90:18-25): DOF order 3*(node-1)+d, 1-based
+ * CSR of the upper triangle with sorted columns, real(8) values, as PARDISO consumes them.
+ * All ints are 32-bit except nnz and slot positions (64-bit).  All pointers are host
+ * pointers unless the name says _device.  One host thread per handle.
+ *
+ * Return codes mirror ClassStatus (Tools/ModStatus.f90:3-49): 0 success;
+ *   1 element geometry (det J <= 1e-13, ModElement.f90:555,1254,1396),
+ *   2 local constitutive Newton not converged (ModViscoelasticMatrix.f90:565),
+ *   3 non-finite stress;
+ * negative values are usage, CUDA or allocation errors (CEOS_E_*).
+ */
+#ifndef CEOS_GPU_H
+#define CEOS_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Material model ids: reference registry ids (ConstitutiveModelsLibrary/
+ * ModConstitutiveModelLibrary.f90:39-56) and project-defined models (>= 101). */
+enum ceos_model_id {
+    CEOS_J2_SMALL = 2,       /* ModJ2Plasticity.f90, params [E, nu, YieldStress, HardeningModulus]      */
+    CEOS_SVK = 5,            /* ModStVenantKirchhoff.f90, params [YoungModulus, Poisson]                  */
+    CEOS_CNH = 7,            /* ModCompressibleNeoHookean.f90, params [Mu, Lambda]                        */
+    CEOS_VISCO_VAR = 12,     /* ModViscoelasticMatrix.f90, params [K_inf, Mu_inf, Lambda_inf, K_e, Mu_e, Ni_v] */
+    CEOS_VISCO_PRONY = 101,  /* finite-strain generalized Maxwell, params [mu, K, nb, beta1, tau1, .. beta4, tau4] */
+    CEOS_J2_FINITE = 102     /* multiplicative J2 (Simo 1988), params [E, nu, sigma_y0, H]                 */
+};
+
+enum ceos_precision {
+    CEOS_FP64 = 0,   /* every operation in FP64 (the reference's real(8))                             */
+    CEOS_MIXED = 1   /* FP32 element arithmetic and state; FP64 det F, ln J, return mapping, K, f_int */
+};
+
+enum ceos_error {
+    CEOS_E_ARG = -1, CEOS_E_CUDA = -2, CEOS_E_ALLOC = -3, CEOS_E_MESH = -4, CEOS_E_MODEL = -5
+};
+
+/* Mesh as the reference holds it: CoordX interleaved [3*n_nodes] (ModNodes.f90:55),
+ * connectivity [8*n_elem] 1-based in the Hexa8 node order (ModElementHexa8.f90:185-192),
+ * mat_id [n_elem] 0-based into the material table (NULL: all 0). */
+typedef struct ceos_mesh {
+    int n_nodes, n_elem;
+    const double* X;
+    const int* conn;
+    const int* mat_id;
+} ceos_mesh;
+
+/* One material (the reference's MaterialList entry, SubMaterialConstructor.f90:13-60).
+ * per_element = 0: params[n_params] shared by every Gauss point of this material, as the
+ * reference shares its Properties pointer (:58-60); per_element = 1: params[n_params*n_elem]
+ * element-major (a build feature the reference does not have).  All materials of one
+ * handle must use the same model id. */
+typedef struct ceos_material {
+    int model;
+    int per_element;
+    int n_params;
+    const double* params;
+} ceos_material;
+
+/* Build the handle: uploads the mesh, builds the upper CSR pattern
+ * (AllocateKgSparseUpperTriangular, ModFEMAnalysis.f90:209-273) and the element-to-CSR
+ * slot map, allocates Gauss-point state (virgin state, ConstitutiveModelConstructor) and
+ * one CUDA stream.  device = CUDA ordinal. */
+int ceos_create(const ceos_mesh* mesh, const ceos_material* mats, int n_mat, int precision_mode,
+                int device, void** handle);
+
+/* Export the pattern: rowmap [n_dof+1], col [nnz], row [nnz] (Kg%RowMap, Kg%Col, Kg%Row),
+ * 1-based.  Any array pointer may be NULL. */
+int ceos_pattern(void* handle, int* n_dof, long long* nnz, int* rowmap, int* col, int* row);
+
+/* Export the element-to-CSR slot map expanded to the reference's form: for element e and
+ * local pair (i,j) with GM(j) >= GM(i), out[(e*24+i)*24+j] = 0-based position in Kg%Val that
+ * AssembleGlobalMatrixUpperTriangular's linear search finds
+ * (SubAssembleGlobalMatrixUpperTriangular.f90:43-65); -1 for GM(j) < GM(i). */
+int ceos_slot_map(void* handle, long long* out);
+
+/* One Newton evaluation (EvaluateR + the K part of EvaluateKt before BCs):
+ * per Gauss point F, stress, state and tangent; f_int = sum_e B^T sigma; when kval != NULL,
+ * Kg%Val = sum_e assembled (B^T D B + G^T S G).  Host buffers: U [n_dof], fint [n_dof],
+ * kval [nnz] or NULL.  time is the reference's analysis time (dt = time - committed time).
+ * n_failed (may be NULL) receives the number of failed elements.  Synchronous. */
+int ceos_evaluate(void* handle, double time, const double* U, double* fint, double* kval, int* n_failed);
+
+/* Same with device-resident buffers, enqueued on `stream` (NULL: the handle's stream);
+ * asynchronous: the status is read by ceos_status() after the caller synchronizes. */
+int ceos_evaluate_device(void* handle, double time, const double* U_device, double* fint_device,
+                         double* kval_device, void* stream);
+int ceos_status(void* handle, int* n_failed);
+
+/* SwitchConvergedState (ModFEMAnalysis.f90:1349-1353) for every Gauss point; the time of the
+ * last evaluation becomes the committed time. */
+int ceos_commit_state(void* handle);
+
+/* Failed element ids (1-based, as ErrorElement.txt lists them, SubSolveConstitutiveModel.f90:69-83)
+ * and a message for the last evaluation. */
+int ceos_last_error(void* handle, int* elem_ids, int max_ids, char* msg, int msg_len);
+
+/* Gauss-point state and stress access (host FP64 arrays [n_elem][8][nvars]); which = 0 for the
+ * committed state, 1 for the state of the last evaluation.  ceos_gp_stress needs
+ * ceos_set_options(handle, CEOS_OPT_STORE_STRESS) before the evaluation. */
+int ceos_state_size(void* handle, int* nvars);
+int ceos_get_state(void* handle, int which, double* out);
+int ceos_set_state(void* handle, int which, const double* in);
+int ceos_gp_stress(void* handle, double* out);
+enum { CEOS_OPT_STORE_STRESS = 1 };
+int ceos_set_options(void* handle, int options);
+int ceos_set_committed_time(void* handle, double t);
+
+/* Release every device buffer and the stream. */
+void ceos_destroy(void* handle);
+
+/* ---- Host driver above the boundary (the Fortran host's role, restated in C++) ----------
+ * Quasi-static analysis of one load case: QuasiStaticAnalysisFEM (ModFEMAnalysis.f90:1136-1374),
+ * NewtonRaphsonFull_Solve (ModNewtonRaphsonFull.f90:44-168) and ApplyBoundaryConditionsNEW
+ * (ModBoundaryConditions.f90:246-340), calling ceos_evaluate every iteration and a host
+ * sparse LDL^T in place of PARDISO.  Arrays as in the reference: dofs 1-based,
+ * *_init/_final item-major [n_items*n_steps]; norm_mode 0 relative, 1 absolute;
+ * norm_type 2 max-abs, 1 L2.  Outputs as documented for each array. */
+int ceos_analysis(void* handle, int n_steps, const double* step_t0, const double* step_dt,
+                  int n_fixed, const int* fixed_dofs,
+                  int n_presc, const int* presc_dofs, const double* presc_init, const double* presc_final,
+                  int n_force, const int* force_dofs, const double* force_init, const double* force_final,
+                  double tol, int itmax, int norm_mode, int norm_type, int max_cutbacks,
+                  int* iters, int* cutbacks, int n_probe, const int* probe_dofs, double* probe_out,
+                  int max_log, double* norm_log, int* n_log, double* U_final);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CEOS_GPU_H */
