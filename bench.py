@@ -1,0 +1,304 @@
+"""Benchmark of the fused element loop (Gauss-point update + f_int + K assembly).
+
+Workload: the viscoelastic scale-up configuration -- unit cube, 64x64x64 Hexa8 (262,144
+elements, 2,097,152 Gauss points), interior nodes jittered +-5% (seed 0), Neo-Hookean ground
+state (mu = 1, K = 100) with 3 generalized-Maxwell branches (beta = 0.3, 0.2, 0.1;
+tau = 0.01, 0.1, 1 s), FP32 Gauss-point state with FP64 det F / ln J and FP64 K / f_int
+(CEOS_MIXED), cyclic simple shear of amplitude 0.3 at 1 Hz with dt = 0.025 s.  One step = one
+Newton evaluation of the whole mesh through the C ABI (the work the reference does in
+SolveConstitutiveModel + InternalForce + TangentStiffnessMatrix per iteration).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's CPU element loop: the Fortran is not buildable here
+(no Fortran compiler, no MKL), so its FP64 C++ restatement (oracle/) runs on all host cores
+on a bounded slab of the same mesh.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ceos-eems_b200"))
+
+NX = 64
+PRONY = [1.0, 100.0, 3, 0.3, 0.01, 0.2, 0.1, 0.1, 1.0, 0.0, 1.0]
+DT = 0.025
+WORKLOAD = "visco-Prony 64^3 Hexa8 (262144 elements, 2097152 GPs), cyclic simple shear"
+METRIC = "GP updates/s"
+UNIT = "GP updates/s"
+
+
+def shear_u(X, t):
+    gamma = 0.3 * np.sin(2.0 * np.pi * t)
+    U = np.zeros_like(X)
+    U[:, 0] = gamma * X[:, 2]
+    return U.reshape(-1)
+
+
+def cpu_slab(X, conn, nz_layers):
+    """The first nz_layers element layers of the mesh with nodes renumbered compactly."""
+    nx = round((conn.shape[0]) ** (1.0 / 3.0))
+    ne = nx * nx * nz_layers
+    c = conn[:ne]
+    used = np.unique(c)
+    newid = np.zeros(X.shape[0] + 1, np.int64)
+    newid[used] = np.arange(1, used.size + 1)
+    return X[used - 1], newid[c].astype(np.int32)
+
+
+def run_cpu_sample(X, conn, threads, nz_layers=4, reps=1):
+    """Time the oracle (reference CPU element loop restated in FP64 C++) on a slab."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    Xs, cs = cpu_slab(X, conn, nz_layers)
+    m = O.Model(Xs, cs, [O.VISCO_PRONY], PRONY)
+    U = shear_u(Xs, 2 * DT)
+    m.evaluate_sample(DT, shear_u(Xs, DT), cs.shape[0], threads)  # one increment of history
+    m.commit()
+    m.set_time_old(DT)
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        m.evaluate_sample(2 * DT, U, cs.shape[0], threads)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    n_gp = 8 * cs.shape[0]
+    return n_gp / best, n_gp, best
+
+
+def clocks_sampler_start(path):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        return subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except OSError:
+        return None
+
+
+def clocks_summary(path, dev):
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    try:
+        for ln in open(path):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9 or not f[0].isdigit() or int(f[0]) != dev:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+    except OSError:
+        pass
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the element kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "element_loop_visco_prony_64cube.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+def algorithmic_bytes(n_nodes, n_elem, n_gp, n_dof, nnz, nb=3):
+    nodes = 48 * n_nodes                  # X + U, FP64
+    connectivity = 32 * n_elem            # 8 int32 node ids
+    state = n_gp * (6 + 6 * nb) * 4 * 2   # FP32 state read + write
+    fint = 8 * n_dof
+    kval = 8 * nnz
+    return nodes + connectivity + state + fint + kval
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from ceos_b200 import meshgen
+    X, conn = meshgen.structured_box(args.nx, args.nx, args.nx, jitter=0.05, seed=0)
+    n_elem, n_gp = conn.shape[0], 8 * conn.shape[0]
+    config = {"workload": WORKLOAD, "mesh": f"{args.nx}^3 Hexa8", "elements": int(n_elem), "gauss_points": int(n_gp),
+              "material": "Neo-Hookean mu=1 K=100 + 3 Maxwell branches (0.3,0.01s),(0.2,0.1s),(0.1,1s)",
+              "precision": "FP32 element arithmetic/state, FP64 detF/lnJ/K/f_int",
+              "l2": "inputs larger than L2 (K 262 MB + state 403 MB per step)", "parallelism": f"replicas x{args.gpus}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        reps = max(1, min(args.steps, 3))
+        rate, n_sample, secs = run_cpu_sample(X, conn, threads, nz_layers=args.nx, reps=reps)
+        sample = f"whole mesh ({n_sample // 8} elements, {n_sample} GPs) per step, FP64, best of {reps}"
+        line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": warmup, "ms_per_step": secs * 1e3 * n_gp / n_sample,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "note": "reference Fortran not buildable (no Fortran compiler/MKL); FP64 C++ restatement of its "
+                        "serial element loop with linear-search assembly, OpenMP over element colours"}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import ceos_b200 as G
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = local_rank
+    torch.cuda.set_device(dev)
+
+    g = G.ElementLoop(X, conn, G.VISCO_PRONY, PRONY, precision=G.MIXED, device=dev)
+    n_dof, nnz = g.n_dof, g.nnz
+    # two committed increments of cyclic shear give the Maxwell branches a non-trivial history
+    for k in (1, 2):
+        t = k * DT
+        _, _, rc, _ = g.evaluate(t, shear_u(X, t), tangent=False)
+        assert rc == 0, rc
+        g.commit()
+    t_eval = 3 * DT
+    U_host = shear_u(X, t_eval)
+    dU = torch.tensor(U_host, dtype=torch.float64, device=f"cuda:{dev}")
+    dfint = torch.zeros(n_dof, dtype=torch.float64, device=f"cuda:{dev}")
+    dK = torch.zeros(nnz, dtype=torch.float64, device=f"cuda:{dev}")
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+
+    def step():
+        g.evaluate_device(t_eval, dU, dfint, dK, stream=sp)
+
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            step()
+    torch.cuda.synchronize()
+    rc, nf = g.status()
+    assert rc == 0, ("element failures", rc, nf)
+
+    clk_path = os.path.join(ROOT, "gpurun_out", f"bench_clocks_r{rank}.csv")
+    os.makedirs(os.path.dirname(clk_path), exist_ok=True)
+    sampler = clocks_sampler_start(clk_path)
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # kernel-only durations for the roofline (events around the element-loop launch)
+    g.set_options(G.OPT_TIME_KERNELS)
+    kms, cms = [], []
+    for _ in range(max(5, min(args.steps, 20))):
+        g.evaluate_device(t_eval, dU, dfint, dK, stream=sp)
+        k_ms, c_ms = g.kernel_time_ms()
+        kms.append(k_ms)
+        cms.append(c_ms)
+    g.set_options(0)
+    if sampler:
+        sampler.terminate()
+        sampler.wait()
+    clocks = clocks_summary(clk_path, dev)
+
+    # end to end through the C ABI with pinned host buffers: H2D of U, D2H of f_int and K
+    U_pin = torch.from_numpy(U_host).pin_memory()
+    f_pin = torch.zeros(n_dof, dtype=torch.float64).pin_memory()
+    K_pin = torch.zeros(nnz, dtype=torch.float64).pin_memory()
+    lib = G.lib()
+    import ctypes as C
+    nfail = C.c_int(0)
+
+    def e2e_step():
+        return lib.ceos_evaluate(g.handle, t_eval, C.c_void_p(U_pin.data_ptr()), C.c_void_p(f_pin.data_ptr()),
+                                 C.c_void_p(K_pin.data_ptr()), C.byref(nfail))
+
+    for _ in range(2):
+        assert e2e_step() == 0
+    e2e_steps = max(3, min(args.steps, 10))
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    # sanity: the device result equals the host result
+    assert torch.allclose(dfint.cpu(), f_pin, rtol=0, atol=0)
+
+    ms_step = ms / args.steps
+    value = world * n_gp * args.steps / (ms * 1e-3)
+    alg = algorithmic_bytes(g.n_nodes, n_elem, n_gp, n_dof, nnz)
+    kmean = float(np.mean(kms)) * 1e-3
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg / kmean / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": warmup,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic", "config": config,
+            "e2e": {"value": world * n_gp / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * n_dof,
+                    "d2h_bytes_per_step": 8 * (n_dof + nnz)},
+            "gpu_launches": 2 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profile_traffic(), "peak_kind": peak_kind,
+                         "kernel": "element_loop_kernel<float,101,1>", "kernel_ms": kmean * 1e3,
+                         "conversion_kernel_ms": float(np.mean(cms)),
+                         "algorithmic_bytes_per_launch": alg},
+            "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        rate, n_sample, secs = run_cpu_sample(X, conn, threads, nz_layers=args.nx)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"one evaluation of the whole mesh ({n_sample // 8} elements), FP64 "
+                                          f"oracle on {threads} threads, {secs:.2f} s"}
+    if rank == 0:
+        print(json.dumps(line))
+    g.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -19,6 +19,7 @@ LIBPATH = os.path.join(HERE, "lib", "libceos_b200.so")
 J2_SMALL, SVK, CNH, VISCO_VAR, VISCO_PRONY, J2_FINITE = 2, 5, 7, 12, 101, 102
 FP64, MIXED = 0, 1
 OPT_STORE_STRESS = 1
+OPT_TIME_KERNELS = 2
 
 _lib = None
 
@@ -68,6 +69,7 @@ def lib():
         L.ceos_gp_stress.argtypes = [P, P]
         L.ceos_set_options.argtypes = [P, I]
         L.ceos_set_committed_time.argtypes = [P, D]
+        L.ceos_kernel_time.argtypes = [P, C.POINTER(C.c_float)]
         L.ceos_destroy.argtypes = [P]
         L.ceos_destroy.restype = None
         L.ceos_analysis.argtypes = [P, I, P, P, I, P, I, P, P, P, I, P, P, P, D, I, I, I, I, P, P, I, P, P, I, P,
@@ -205,8 +207,17 @@ class ElementLoop:
         st = _f64(st).reshape(-1)
         _check(lib().ceos_set_state(self._h, which, _ptr(st)))
 
+    def set_options(self, options):
+        _check(lib().ceos_set_options(self._h, options))
+
     def store_stress(self, on=True):
-        _check(lib().ceos_set_options(self._h, OPT_STORE_STRESS if on else 0))
+        self.set_options(OPT_STORE_STRESS if on else 0)
+
+    def kernel_time_ms(self):
+        """(element-loop kernel ms, K conversion kernel ms) of the last evaluation."""
+        ms = (C.c_float * 2)()
+        _check(lib().ceos_kernel_time(self._h, ms))
+        return ms[0], ms[1]
 
     def gp_stress(self):
         out = np.zeros(self.n_elem * 8 * 6)

@@ -67,13 +67,23 @@ void model_init_state(int model, double* st) {
     } while (0)
 
 template <typename T>
-size_t elem_smem() { return sizeof(ElemSmem<T>); }
+size_t elem_smem(const Handle* h) { return SmemLayout<T>(h->ns_used).total; }
 
 template <typename T, int MODEL>
 int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
     ElemArgs<T> a;
     a.n_elem = h->n_elem;
+    a.e_begin = 0;
+    a.e_end = h->n_elem;
+    for (int k = 0; k < 12; ++k) a.pu[k] = T(0);
+    if (h->param_mode == 0)
+        for (int k = 0; k < h->n_params && k < 12; ++k) a.pu[k] = (T)h->host_params[k];
+    for (int k = 0; k < 4; ++k) a.ebr[k] = T(0);
+    if (MODEL == M_VISCO_PRONY && h->param_mode == 0)
+        for (int k = 0; k < 4 && k < (int)h->host_params[2]; ++k)
+            a.ebr[k] = (T)std::exp(-dt / (2.0 * h->host_params[4 + 2 * k]));
     a.X = h->d_X;
+    a.Xf = h->d_Xf;
     a.U = dU;
     a.conn = h->d_conn;
     a.rs = h->d_rs;
@@ -83,6 +93,8 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
     a.kval = dkval;
     a.st_old = reinterpret_cast<const T*>(h->d_state[h->cur_old]);
     a.st_new = reinterpret_cast<T*>(h->d_state[1 - h->cur_old]);
+    a.ld = h->ld;
+    a.ns_used = h->ns_used;
     a.params = reinterpret_cast<const T*>(h->d_params);
     a.param_mode = h->param_mode;
     a.n_params = h->n_params;
@@ -91,16 +103,23 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
     a.elem_status = h->d_elem_status;
     a.status_count = h->d_status_count;
     a.gp_stress = (h->options & CEOS_OPT_STORE_STRESS) ? reinterpret_cast<T*>(h->d_gp_stress) : nullptr;
-    const size_t smem = elem_smem<T>();
-    static bool attr_set = false;
-    if (!attr_set) {
-        CK(cudaFuncSetAttribute(element_loop_kernel<T, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
-    const int n_tiles = (h->n_elem + kTileE - 1) / kTileE;
+    a.kblk = h->d_kblk;
+    const size_t smem = elem_smem<T>(h);
+    CK(cudaFuncSetAttribute(element_loop_kernel<T, MODEL, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int n_tiles = (a.e_end - a.e_begin + kTileE - 1) / kTileE;
     int grid = std::min(n_tiles, h->grid_cap);
-    element_loop_kernel<T, MODEL><<<grid, kThreads, smem, s>>>(a);
+    const bool timed = (h->options & CEOS_OPT_TIME_KERNELS) && h->ev_k0;
+    if (timed) CK(cudaEventRecord(h->ev_k0, s));
+    element_loop_kernel<T, MODEL, (sizeof(T) == 4)><<<grid, kThreads, smem, s>>>(a);
     CK(cudaGetLastError());
+    if (timed) CK(cudaEventRecord(h->ev_k1, s));
+    if (sizeof(T) == 4 && dkval) {
+        // FP32 node-pair blocks -> FP64 CSR (every K entry written once), scratch re-zeroed
+        const int cgrid = h->grid_cap > 0 ? 148 * 8 : 1184;
+        kblock_to_csr_kernel<<<cgrid, 256, 0, s>>>(h->n_nodes, h->d_rs, h->d_nup, h->d_kblk, dkval);
+        CK(cudaGetLastError());
+    }
+    if (timed) CK(cudaEventRecord(h->ev_k2, s));
     return 0;
 }
 
@@ -123,24 +142,24 @@ int occupancy_grid(Handle* h) {
     cudaError_t e = cudaSuccess;
     switch (h->model) {
         case M_CNH:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_CNH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>());
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_CNH>, kThreads, elem_smem<T>());
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_CNH, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_CNH, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
             break;
         case M_SVK:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_SVK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>());
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_SVK>, kThreads, elem_smem<T>());
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_SVK, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_SVK, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
             break;
         case M_J2_SMALL:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_J2_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>());
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_J2_SMALL>, kThreads, elem_smem<T>());
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_J2_SMALL, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_J2_SMALL, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
             break;
         case M_VISCO_PRONY:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_VISCO_PRONY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>());
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_VISCO_PRONY>, kThreads, elem_smem<T>());
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_VISCO_PRONY, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_VISCO_PRONY, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
             break;
         case M_J2_FINITE:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_J2_FINITE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>());
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_J2_FINITE>, kThreads, elem_smem<T>());
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_J2_FINITE, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_J2_FINITE, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
             break;
     }
     if (e != cudaSuccess || per_sm < 1) per_sm = 1;
@@ -342,7 +361,9 @@ int evaluate_device(Handle* h, double time, const double* dU, double* dfint, dou
     h->time_eval = time;
     CK(cudaMemsetAsync(h->d_status_count, 0, sizeof(int), s));
     CK(cudaMemsetAsync(dfint, 0, sizeof(double) * 3 * (size_t)h->n_nodes, s));
-    if (dkval) CK(cudaMemsetAsync(dkval, 0, sizeof(double) * (size_t)h->nnz, s));
+    // FP64 mode accumulates straight into K (zeroed here); the mixed mode writes every K entry
+    // from its FP32 block scratch, so K needs no clearing.
+    if (dkval && h->precision == CEOS_FP64) CK(cudaMemsetAsync(dkval, 0, sizeof(double) * (size_t)h->nnz, s));
     int rc = (h->precision == CEOS_FP64) ? launch_elem<double>(h, dt, dU, dfint, dkval, s)
                                          : launch_elem<float>(h, dt, dU, dfint, dkval, s);
     if (rc) return rc;
@@ -453,7 +474,7 @@ extern "C" int ceos_get_state(void* handle, int which, double* out) {
     if (!h || !out) return CEOS_E_ARG;
     if (!h->nstate) return 0;
     const int buf = which ? 1 - h->cur_old : h->cur_old;
-    const size_t n = (size_t)h->nstate * 8 * h->n_elem;
+    const size_t n = (size_t)h->nstate * 8 * h->ld;
     std::vector<double> tmp(n);
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
@@ -464,11 +485,12 @@ extern "C" int ceos_get_state(void* handle, int which, double* out) {
         CK(cudaMemcpy(f.data(), h->d_state[buf], n * sizeof(float), cudaMemcpyDeviceToHost));
         for (size_t i = 0; i < n; ++i) tmp[i] = f[i];
     }
-    // device [v][gp][e] -> host [e][gp][v]
+    // device [v][gp][e] (leading dimension ld) -> host [e][gp][v]
     const int E = h->n_elem, V = h->nstate;
+    const size_t LD = h->ld;
     for (int v = 0; v < V; ++v)
         for (int g = 0; g < 8; ++g)
-            for (int e = 0; e < E; ++e) out[((size_t)e * 8 + g) * V + v] = tmp[((size_t)v * 8 + g) * E + e];
+            for (int e = 0; e < E; ++e) out[((size_t)e * 8 + g) * V + v] = tmp[((size_t)v * 8 + g) * LD + e];
     return 0;
 }
 
@@ -478,11 +500,12 @@ extern "C" int ceos_set_state(void* handle, int which, const double* in) {
     if (!h->nstate) return 0;
     const int buf = which ? 1 - h->cur_old : h->cur_old;
     const int E = h->n_elem, V = h->nstate;
-    const size_t n = (size_t)V * 8 * E;
-    std::vector<double> tmp(n);
+    const size_t LD = h->ld;
+    const size_t n = (size_t)V * 8 * LD;
+    std::vector<double> tmp(n, 0.0);
     for (int v = 0; v < V; ++v)
         for (int g = 0; g < 8; ++g)
-            for (int e = 0; e < E; ++e) tmp[((size_t)v * 8 + g) * E + e] = in[((size_t)e * 8 + g) * V + v];
+            for (int e = 0; e < E; ++e) tmp[((size_t)v * 8 + g) * LD + e] = in[((size_t)e * 8 + g) * V + v];
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     if (h->precision == CEOS_FP64) {
@@ -498,10 +521,25 @@ extern "C" int ceos_set_options(void* handle, int options) {
     Handle* h = static_cast<Handle*>(handle);
     if (!h) return CEOS_E_ARG;
     h->options = options;
+    if ((options & CEOS_OPT_TIME_KERNELS) && !h->ev_k0) {
+        CK(cudaSetDevice(h->device));
+        CK(cudaEventCreate(&h->ev_k0));
+        CK(cudaEventCreate(&h->ev_k1));
+        CK(cudaEventCreate(&h->ev_k2));
+    }
     if ((options & CEOS_OPT_STORE_STRESS) && !h->d_gp_stress) {
         CK(cudaSetDevice(h->device));
         CK(cudaMalloc(&h->d_gp_stress, (size_t)6 * 8 * h->n_elem * h->elem_bytes()));
     }
+    return 0;
+}
+
+extern "C" int ceos_kernel_time(void* handle, float* ms) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !ms || !h->ev_k0) return CEOS_E_ARG;
+    CK(cudaEventSynchronize(h->ev_k2));
+    CK(cudaEventElapsedTime(&ms[0], h->ev_k0, h->ev_k1));
+    CK(cudaEventElapsedTime(&ms[1], h->ev_k1, h->ev_k2));
     return 0;
 }
 
@@ -539,11 +577,19 @@ namespace ceos {
 int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, int n_mat) {
     Handle* h = this;
     const size_t N = n_nodes, E = n_elem;
+    ld = (n_elem + 31) / 32 * 32;
     conn0.resize(8 * E);
     for (size_t i = 0; i < 8 * E; ++i) conn0[i] = mesh->conn[i] - 1;
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     CK(cudaMalloc(&d_X, 3 * N * sizeof(double)));
     CK(cudaMemcpy(d_X, mesh->X, 3 * N * sizeof(double), cudaMemcpyHostToDevice));
+    if (precision == CEOS_MIXED) {
+        std::vector<float> xf(4 * N, 0.f);
+        for (size_t n = 0; n < N; ++n)
+            for (int d = 0; d < 3; ++d) xf[4 * n + d] = (float)mesh->X[3 * n + d];
+        CK(cudaMalloc(&d_Xf, 4 * N * sizeof(float)));
+        CK(cudaMemcpy(d_Xf, xf.data(), 4 * N * sizeof(float), cudaMemcpyHostToDevice));
+    }
     CK(cudaMalloc(&d_U, 3 * N * sizeof(double)));
     CK(cudaMemset(d_U, 0, 3 * N * sizeof(double)));
     CK(cudaMalloc(&d_fint, 3 * N * sizeof(double)));
@@ -592,6 +638,15 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
         CK(cudaMemcpy(d_mat_id, mid.data(), E * sizeof(int), cudaMemcpyHostToDevice));
     }
     host_params = P;
+    if (precision == CEOS_MIXED) {
+        // blocked FP32 assembly scratch and per-node arrival counters
+        n_blocks = (long long)N + (nnz - 6LL * (long long)N) / 9;
+        CK(cudaMalloc(&d_kblk, (size_t)n_blocks * 12 * sizeof(float)));
+        CK(cudaMemset(d_kblk, 0, (size_t)n_blocks * 12 * sizeof(float)));
+    }
+    // state variables actually used (the Prony model reads/writes only nb of its 4 branch slots)
+    ns_used = nstate;
+    if (model == M_VISCO_PRONY && param_mode == 0) ns_used = 6 + 6 * std::max(0, std::min(4, (int)P[2]));
     CK(cudaMalloc(&d_params, P.size() * eb));
     if (precision == CEOS_FP64) {
         CK(cudaMemcpy(d_params, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -603,9 +658,9 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
     if (nstate) {
         std::vector<double> init(nstate);
         model_init_state(model, init.data());
-        std::vector<double> S((size_t)nstate * 8 * E);
+        std::vector<double> S((size_t)nstate * 8 * ld);
         for (int v = 0; v < nstate; ++v)
-            std::fill(S.begin() + (size_t)v * 8 * E, S.begin() + (size_t)(v + 1) * 8 * E, init[v]);
+            std::fill(S.begin() + (size_t)v * 8 * ld, S.begin() + (size_t)(v + 1) * 8 * ld, init[v]);
         for (int b = 0; b < 2; ++b) {
             CK(cudaMalloc(&d_state[b], state_bytes()));
             if (precision == CEOS_FP64) {
@@ -622,9 +677,12 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
 Handle::~Handle() {
     if (stream) cudaStreamSynchronize(stream);
     void* ptrs[] = {d_X, d_U, d_fint, d_kval, d_conn, d_rs, d_nup, d_ranks, d_elem_status, d_status_count,
-                    d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress};
+                    d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress, d_kblk, d_Xf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (ev_k0) cudaEventDestroy(ev_k0);
+    if (ev_k1) cudaEventDestroy(ev_k1);
+    if (ev_k2) cudaEventDestroy(ev_k2);
     if (stream) cudaStreamDestroy(stream);
 }
 

@@ -53,10 +53,11 @@ CEOS_HD void inv3(const T A[3][3], T d, T B[3][3]) {
     B[2][0] = A[1][0] * A[2][1] - A[1][1] * A[2][0];
     B[2][1] = A[0][1] * A[2][0] - A[0][0] * A[2][1];
     B[2][2] = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+    const T r = T(1) / d;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) B[i][j] = B[i][j] / d;
+        for (int j = 0; j < 3; ++j) B[i][j] = B[i][j] * r;
 }
 
 // b = F F^T (Voigt)
@@ -97,12 +98,13 @@ CEOS_HD void push_sym(const T F[3][3], const T S[6], T out[6]) {
 template <typename T>
 CEOS_HD void inv_sym(const T c[6], T d, T ci[6]) {
     // c = [[c0 c3 c5],[c3 c1 c4],[c5 c4 c2]]
-    ci[0] = (c[1] * c[2] - c[4] * c[4]) / d;
-    ci[1] = (c[0] * c[2] - c[5] * c[5]) / d;
-    ci[2] = (c[0] * c[1] - c[3] * c[3]) / d;
-    ci[3] = (c[5] * c[4] - c[3] * c[2]) / d;
-    ci[4] = (c[3] * c[5] - c[0] * c[4]) / d;
-    ci[5] = (c[3] * c[4] - c[5] * c[1]) / d;
+    const T r = T(1) / d;
+    ci[0] = (c[1] * c[2] - c[4] * c[4]) * r;
+    ci[1] = (c[0] * c[2] - c[5] * c[5]) * r;
+    ci[2] = (c[0] * c[1] - c[3] * c[3]) * r;
+    ci[3] = (c[5] * c[4] - c[3] * c[2]) * r;
+    ci[4] = (c[3] * c[5] - c[0] * c[4]) * r;
+    ci[5] = (c[3] * c[4] - c[5] * c[1]) * r;
 }
 // upper-triangular packed index of (i <= j) in a 6x6 symmetric matrix
 CEOS_HD constexpr int up21(int i, int j) { return i * 6 - (i * (i - 1)) / 2 + (j - i); }

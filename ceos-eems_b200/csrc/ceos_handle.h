@@ -13,6 +13,8 @@ namespace ceos {
 struct Handle {
     // mesh and pattern (host copies)
     int n_nodes = 0, n_elem = 0, precision = 0, device = 0, model = 0, n_params = 0, nstate = 0;
+    int ld = 0;       // leading dimension of state arrays: n_elem rounded up to 32
+    int ns_used = 0;  // state variables the kernel reads and writes
     long long nnz = 0;
     std::vector<int> conn0;               // [8*n_elem] 0-based
     std::vector<long long> up_ptr;        // upper-neighbour lists (CSR over nodes)
@@ -25,6 +27,7 @@ struct Handle {
     // device buffers
     cudaStream_t stream = nullptr;
     double *d_X = nullptr, *d_U = nullptr, *d_fint = nullptr, *d_kval = nullptr;
+    float4* d_Xf = nullptr;               // mixed mode: reference coordinates in FP32
     int* d_conn = nullptr;
     long long* d_rs = nullptr;
     int* d_nup = nullptr;
@@ -35,15 +38,18 @@ struct Handle {
     int* d_mat_id = nullptr;
     void* d_state[2] = {nullptr, nullptr};
     void* d_gp_stress = nullptr;
+    float* d_kblk = nullptr;              // mixed mode: FP32 node-pair block scratch
+    long long n_blocks = 0;
     int cur_old = 0;                      // index of the committed state buffer
     bool evaluated = false;
     double time_old = 0.0, time_eval = 0.0;
     int options = 0;
+    cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr, ev_k2 = nullptr;
     int grid_cap = 148, blocks_per_sm = 1;
     std::string msg;
 
     size_t elem_bytes() const { return precision == CEOS_FP64 ? sizeof(double) : sizeof(float); }
-    size_t state_bytes() const { return (size_t)nstate * 8 * n_elem * elem_bytes(); }
+    size_t state_bytes() const { return (size_t)nstate * 8 * ld * elem_bytes(); }
     int allocate_device(const ceos_mesh* mesh, const ceos_material* mats, int n_mat);
     ~Handle();
 };

@@ -36,7 +36,9 @@ __constant__ double c_dN[8][8][3];
 template <typename T>
 struct ElemArgs {
     int n_elem;
+    int e_begin, e_end;     // element range of this launch
     const double* X;        // [3*n_nodes] reference coordinates (CoordX)
+    const float4* Xf;       // [n_nodes] reference coordinates in FP32 (CEOS_MIXED)
     const double* U;        // [3*n_nodes] displacements, DOF 3n+d
     const int* conn;        // [n_elem*8] 0-based node ids
     const long long* rs;    // [n_nodes] CSR position of the first entry of row 3n (0-based)
@@ -44,108 +46,292 @@ struct ElemArgs {
     const uint32_t* ranks;  // [n_elem*8] 28 uint8 slot ranks per element (32 bytes)
     double* fint;           // [3*n_nodes]
     double* kval;           // [nnz] or nullptr (no tangent)
-    const T* st_old;        // [nstate][8][n_elem]
+    const T* st_old;        // [nstate][8][ld]
     T* st_new;
+    int ld;                 // leading dimension of the state arrays (n_elem rounded up to 32)
+    int ns_used;            // state variables the model reads and writes
     const T* params;        // see param_mode
-    int param_mode;         // 0 uniform params[k]; 1 per element params[k*n_elem+e]; 2 per material
+    int param_mode;         // 0 uniform (pu[]); 1 per element params[k*n_elem+e]; 2 per material
     int n_params;
     const int* mat_id;      // per material: params[mat_id[e]*n_params+k]
+    T pu[12];               // uniform parameters (kernel-argument space: broadcast reads)
+    T ebr[4];               // Prony relaxation factors exp(-dt/(2 tau_a)) when parameters are uniform
     double dt;
     uint8_t* elem_status;   // [n_elem]
     int* status_count;      // failed elements
     T* gp_stress;           // [6][8][n_elem] or nullptr
+    // Blocked FP32 assembly (CEOS_MIXED): node-pair blocks of 3 rows x 4 floats, node n's row
+    // block starts at block n + (rs[n] - 6n)/9 (diagonal block, then one per upper neighbour).
+    float* kblk;            // [n_blocks*12] accumulation scratch, zero between evaluations
 };
 
+// Dynamic shared-memory layout of one CTA.  Arrays indexed [..][e] with the element index
+// innermost, so that 32 lanes (32 consecutive elements) access consecutive words or 16-byte
+// vectors: every access is bank-conflict free.  Node data and state of the NEXT tile are
+// prefetched with cp.async while the current tile computes (software pipeline).
 template <typename T>
-struct __align__(16) ElemSmem {
-    double x[8][3][kTileE];  // reference coordinates
-    double u[8][3][kTileE];  // displacements
-    long long rs[8][kTileE];
-    int nup[8][kTileE];
-    int node[8][kTileE];
-    uint32_t ranks[kTileE][8];
-    T g[8][8][3][kTileE];    // [gp][node][d][e] current-configuration gradients
-    T D[8][21][kTileE];      // [gp][k][e] w*detJ*D (upper)
-    T s[8][6][kTileE];       // [gp][k][e] w*detJ*sigma
-    int status[kTileE];
+struct SmemLayout {
+    size_t g, ds, st, x, u, xf, rs, nup, node, ranks, status, total;
+    CEOS_HD explicit SmemLayout(int ns) {
+        size_t o = 0;
+        auto take = [&](size_t bytes) { size_t r = o; o += (bytes + 15) & ~size_t(15); return r; };
+        g = take(sizeof(T) * 8 * 8 * kTileE * 4);        // [gp][node][e][4]: grad N (current)
+        ds = take(sizeof(T) * 8 * 7 * kTileE * 4);       // [gp][quad][e][4]: w detJ (D upper 21, sigma 6)
+        st = take(sizeof(T) * (size_t)(ns > 0 ? ns : 1) * 8 * kTileE);  // [v][gp][e]: committed state
+        x = take(sizeof(T) == 4 ? 16 : sizeof(double) * 8 * kTileE * 3);  // [node][e][3] (FP64 mode)
+        u = take(sizeof(double) * 8 * kTileE * 3);
+        xf = take(sizeof(T) == 4 ? sizeof(float) * 8 * kTileE * 8 : 16);  // [node][e][X 4 | U 4] in FP32
+        rs = take(sizeof(long long) * 2 * 8 * kTileE);  // double-buffered [buf][node][e]
+        nup = take(sizeof(int) * 2 * 8 * kTileE);
+        node = take(sizeof(int) * 2 * 8 * kTileE);
+        ranks = take(sizeof(uint32_t) * 2 * kTileE * 8); // [buf][e][8]
+        status = take(sizeof(int) * kTileE);
+        total = o;
+    }
+};
+
+CEOS_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+CEOS_D void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(dst)), "l"(src));
+}
+CEOS_D void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src));
+}
+CEOS_D void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src));
+}
+CEOS_D void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+CEOS_D void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Gauss-point state access: committed values from the prefetched shared copy, new values
+// streamed to global memory with the evict-first hint (L2 is kept for the K scatter).
+template <typename T>
+struct StateIO {
+    const T* sm;    // &st[0][gp][el]
+    T* new_;
+    size_t ld8;     // 8 * ld (row stride of one state variable)
+    size_t off;     // gp * ld + e
+    CEOS_D T ld(int v) const { return sm[v * 8 * kTileE]; }
+    CEOS_D void st(int v, T x) const { __stcs(new_ + (size_t)v * ld8 + off, x); }
 };
 
 template <typename T, int MODEL>
-CEOS_D void run_material(const T F[3][3], const T* p, double dt, const T* st, T* stn, T sig[6], T D[21]) {
-    if constexpr (MODEL == M_CNH) cnh_update<T>(F, p, sig, D);
-    else if constexpr (MODEL == M_SVK) svk_update<T>(F, p, sig, D);
-    else if constexpr (MODEL == M_J2_SMALL) j2_small_update<T>(F, p, st, stn, sig, D);
-    else if constexpr (MODEL == M_VISCO_PRONY) visco_prony_update<T>(F, p, dt, st, stn, sig, D);
-    else if constexpr (MODEL == M_J2_FINITE) j2_finite_update<T>(F, p, st, stn, sig, D);
+CEOS_D void run_material(const T F[3][3], const T* p, const T* ebr, const StateIO<T>& io, T sig[6], T D[21]) {
+    constexpr int NS = ModelInfo<MODEL>::nstate;
+    if constexpr (MODEL == M_CNH) {
+        cnh_update<T>(F, p, sig, D);
+    } else if constexpr (MODEL == M_SVK) {
+        svk_update<T>(F, p, sig, D);
+    } else if constexpr (MODEL == M_VISCO_PRONY) {
+        visco_prony_update<T>(F, p, ebr, io, sig, D);
+    } else {
+        T st[NS], stn[NS];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) st[k] = io.ld(k);
+        if constexpr (MODEL == M_J2_SMALL) j2_small_update<T>(F, p, st, stn, sig, D);
+        else if constexpr (MODEL == M_J2_FINITE) j2_finite_update<T>(F, p, st, stn, sig, D);
+#pragma unroll
+        for (int k = 0; k < NS; ++k) io.st(k, stn[k]);
+    }
 }
 
-template <typename T, int MODEL>
-__global__ void __launch_bounds__(kThreads) element_loop_kernel(ElemArgs<T> a) {
-    constexpr int NS = ModelInfo<MODEL>::nstate;
+template <typename T>
+CEOS_D void st4(T* p, T a, T b, T c, T d) {
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+    } else {
+        *reinterpret_cast<double2*>(p) = make_double2(a, b);
+        *reinterpret_cast<double2*>(p + 2) = make_double2(c, d);
+    }
+}
+template <typename T>
+CEOS_D void ld4(const T* p, T& a, T& b, T& c, T& d) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        a = v.x; b = v.y; c = v.z; d = v.w;
+    } else {
+        const double2 v0 = *reinterpret_cast<const double2*>(p);
+        const double2 v1 = *reinterpret_cast<const double2*>(p + 2);
+        a = v0.x; b = v0.y; c = v1.x; d = v1.y;
+    }
+}
+
+// Stage the connectivity and slot ranks of tile `tile` into buffer `buf` (async).
+template <typename T>
+CEOS_D void prefetch_conn(const ElemArgs<T>& a, int e0, int* node_s, uint32_t* ranks_s, int t) {
+    const int e = t >> 3, n = t & 7;
+    if (e0 + e < a.e_end) {
+        cp_async4(node_s + n * kTileE + e, a.conn + (size_t)(e0 + e) * 8 + n);
+        cp_async4(ranks_s + e * 8 + n, a.ranks + (size_t)(e0 + e) * 8 + n);
+    }
+}
+
+// Gather node data (X, U, CSR row start, upper-neighbour count) and the committed state of a
+// tile whose node ids are already in node_s (async).
+template <typename T>
+CEOS_D void prefetch_nodes_state(const ElemArgs<T>& a, int e0, const int* node_s, double* xs, double* us,
+                                 float* xf, long long* rs_s, int* nup_s, T* st_s, int t) {
+    const int lane = t & 31, n = t >> 5;
+    if (e0 + lane < a.e_end) {
+        const int node = node_s[n * kTileE + lane];
+        const double* Up = a.U + 3 * (size_t)node;
+        double* ud = us + (n * kTileE + lane) * 3;
+        if constexpr (sizeof(T) == 4) {
+            cp_async16(xf + (n * kTileE + lane) * 8, a.Xf + node);
+        } else {
+            const double* Xp = a.X + 3 * (size_t)node;
+            double* xd = xs + (n * kTileE + lane) * 3;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) cp_async8(xd + d, Xp + d);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) cp_async8(ud + d, Up + d);
+        cp_async8(rs_s + n * kTileE + lane, a.rs + node);
+        cp_async4(nup_s + n * kTileE + lane, a.nup + node);
+    }
+    if (a.ns_used > 0) {
+        constexpr int per_chunk = 16 / sizeof(T);      // elements per 16-byte chunk
+        constexpr int cpr = kTileE / per_chunk;        // chunks per (v, gp) row
+        const int total = a.ns_used * 8 * cpr;
+        for (int c = t; c < total; c += kThreads) {
+            const int row = c / cpr, part = c - row * cpr;   // row = v*8 + gp
+            cp_async16(st_s + row * kTileE + part * per_chunk, a.st_old + (size_t)row * a.ld + e0 + part * per_chunk);
+        }
+    }
+}
+
+CEOS_D void red_v4(float* p, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+
+// Convert the row block of `node` from the FP32 block scratch into its three FP64 CSR rows and
+// zero the scratch again.  Executed by a whole warp: lanes walk each CSR row segment in order,
+// so every store instruction writes 32 consecutive doubles (full sectors).
+CEOS_D void finalize_row_block(int node, long long rs, int m, float* kblk, double* K, int lane) {
+    const long long bb = (long long)node + (rs - 6LL * node) / 9;  // first block of this node
+    const float* blk = kblk + bb * 12;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        // row 3n+k: the diagonal-block entries l >= k, then 3 entries per upper neighbour block
+        const long long rstart = rs + (k == 0 ? 0LL : (k == 1 ? 3LL + 3LL * m : 5LL + 6LL * m));
+        const int nd = 3 - k, len = nd + 3 * m;
+        for (int p = lane; p < len; p += 32) {
+            int j, l;
+            if (p < nd) { j = 0; l = k + p; }
+            else { const int pp = p - nd; j = 1 + pp / 3; l = pp - 3 * (pp / 3); }
+            K[rstart + p] = (double)__ldcg(blk + j * 12 + 4 * k + l);
+        }
+    }
+    __syncwarp();
+    float4* z = reinterpret_cast<float4*>(kblk + bb * 12);
+    for (int q = lane; q < 3 * (1 + m); q += 32) __stcg(z + q, make_float4(0.f, 0.f, 0.f, 0.f));
+}
+
+// Block scratch -> FP64 CSR values of K, one warp per node row block; leaves the scratch zero.
+__global__ void __launch_bounds__(256) kblock_to_csr_kernel(int n_nodes, const long long* __restrict__ rs,
+                                                            const int* __restrict__ nup, float* kblk, double* K) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; n < n_nodes; n += warps)
+        finalize_row_block(n, __ldg(rs + n), __ldg(nup + n), kblk, K, lane);
+}
+
+template <typename T, int MODEL, bool BLOCKED>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop_kernel(ElemArgs<T> a) {
     constexpr int NP = ModelInfo<MODEL>::nparams;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    ElemSmem<T>& sm = *reinterpret_cast<ElemSmem<T>*>(smem_raw);
+    const SmemLayout<T> L(a.ns_used);
+    T* sg = reinterpret_cast<T*>(smem_raw + L.g);
+    T* sds = reinterpret_cast<T*>(smem_raw + L.ds);
+    T* sst = reinterpret_cast<T*>(smem_raw + L.st);
+    double* sx = reinterpret_cast<double*>(smem_raw + L.x);
+    double* su = reinterpret_cast<double*>(smem_raw + L.u);
+    float* sxf = reinterpret_cast<float*>(smem_raw + L.xf);
+    long long* srs = reinterpret_cast<long long*>(smem_raw + L.rs);
+    int* snup = reinterpret_cast<int*>(smem_raw + L.nup);
+    int* snode = reinterpret_cast<int*>(smem_raw + L.node);
+    uint32_t* sranks = reinterpret_cast<uint32_t*>(smem_raw + L.ranks);
+    int* sstatus = reinterpret_cast<int*>(smem_raw + L.status);
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
-    const int n_tiles = (a.n_elem + kTileE - 1) / kTileE;
+    const int n_tiles = (a.e_end - a.e_begin + kTileE - 1) / kTileE;
+    constexpr int NB = 8 * kTileE;  // one buffer of [node][e] ints
 
-    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        const int e0 = tile * kTileE;
-        // ---------------- gather: thread (node = warp, element = lane) ----------------------
-        {
-            const int e = e0 + lane;
-            const int n = warp;
-            if (e < a.n_elem) {
-                const int node = __ldg(a.conn + (size_t)e * 8 + n);
-                sm.node[n][lane] = node;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    sm.x[n][d][lane] = __ldg(a.X + 3 * (size_t)node + d);
-                    sm.u[n][d][lane] = __ldg(a.U + 3 * (size_t)node + d);
-                }
-                sm.rs[n][lane] = __ldg(a.rs + node);
-                sm.nup[n][lane] = __ldg(a.nup + node);
-            }
-            // slot ranks: 8 words per element, read coalesced as one 1 KB block per tile
-            const int ew = t >> 3, wd = t & 7;
-            if (e0 + ew < a.n_elem) sm.ranks[ew][wd] = __ldg(a.ranks + (size_t)(e0 + ew) * 8 + wd);
-            if (t < kTileE) sm.status[t] = 0;
+    int tile = blockIdx.x;
+    if (tile >= n_tiles) return;
+    // prologue: connectivity of the first tile, then its node data and state
+    prefetch_conn(a, a.e_begin + tile * kTileE, snode, sranks, t);
+    cp_commit();
+    if (t < kTileE) sstatus[t] = 0;
+    cp_wait_all();
+    __syncthreads();
+    prefetch_nodes_state(a, a.e_begin + tile * kTileE, snode, sx, su, sxf, srs, snup, sst, t);
+    cp_commit();
+
+    for (int it = 0; tile < n_tiles; ++it, tile += gridDim.x) {
+        const int buf = it & 1;
+        const int e0 = a.e_begin + tile * kTileE;
+        const int next = tile + gridDim.x;
+        const int e0n = a.e_begin + next * kTileE;
+        int* node_c = snode + buf * NB;
+        long long* rs_c = srs + buf * NB;
+        int* nup_c = snup + buf * NB;
+        const uint32_t* ranks_c = sranks + buf * NB;
+        cp_wait_all();
+        __syncthreads();  // node data and state of this tile are in shared memory
+        if (next < n_tiles) {
+            prefetch_conn(a, e0n, snode + (buf ^ 1) * NB, sranks + (buf ^ 1) * NB, t);
+            cp_commit();
         }
-        __syncthreads();
+        if constexpr (sizeof(T) == 4) {
+            // one FP64 -> FP32 conversion per (node, element) instead of one per Gauss point
+            const int n = warp, el = lane;
+            const double* up = su + (n * kTileE + el) * 3;
+            float4* dst = reinterpret_cast<float4*>(sxf + (n * kTileE + el) * 8);
+            dst[1] = make_float4((float)up[0], (float)up[1], (float)up[2], 0.f);
+            __syncthreads();
+        }
 
         // ---------------- phase A: thread (gp = warp, element = lane) -----------------------
         {
             const int gp = warp, el = lane, e = e0 + el;
-            if (e < a.n_elem) {
+            if (e < a.e_end) {
                 int status = 0;
-                // Jacobian on the reference configuration and F = I + sum u (x) grad_X N
-                T JX[3][3], Jc[3][3];
+                T JX[3][3] = {}, Jc[3][3] = {};
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
+                for (int n = 0; n < 8; ++n) {
+                    T X[3], x[3];
+                    if constexpr (sizeof(T) == 4) {
+                        const float4* q = reinterpret_cast<const float4*>(sxf + (n * kTileE + el) * 8);
+                        const float4 xv = q[0], uv = q[1];
+                        X[0] = xv.x; X[1] = xv.y; X[2] = xv.z;
+                        x[0] = xv.x + uv.x; x[1] = xv.y + uv.y; x[2] = xv.z + uv.z;
+                    } else {
+                        const double* xp = sx + (n * kTileE + el) * 3;
+                        const double* up = su + (n * kTileE + el) * 3;
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        T sx = T(0), sc = T(0);
-#pragma unroll
-                        for (int n = 0; n < 8; ++n) {
-                            const T dn = (T)c_dN[gp][n][i];
-                            const double X = sm.x[n][j][el];
-                            sx += dn * (T)X;
-                            sc += dn * (T)(X + sm.u[n][j][el]);
+                        for (int d = 0; d < 3; ++d) {
+                            X[d] = (T)xp[d];
+                            x[d] = (T)(xp[d] + up[d]);
                         }
-                        JX[i][j] = sx;
-                        Jc[i][j] = sc;
                     }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const T dn = (T)c_dN[gp][n][i];
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) {
+                            JX[i][j] += dn * X[j];
+                            Jc[i][j] += dn * x[j];
+                        }
+                    }
+                }
                 const T detJX = det3(JX);
                 const T detJ = det3(Jc);
                 if (!(detJX > T(1.0e-13)) || !(detJ > T(1.0e-13))) status |= 1;
                 T JXi[3][3], Jci[3][3];
                 inv3(JX, detJX, JXi);
                 inv3(Jc, detJ, Jci);
-                T F[3][3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) F[i][j] = (i == j) ? T(1) : T(0);
+                T F[3][3] = {{T(1), T(0), T(0)}, {T(0), T(1), T(0)}, {T(0), T(0), T(1)}};
 #pragma unroll
                 for (int n = 0; n < 8; ++n) {
                     const T d0 = (T)c_dN[gp][n][0], d1 = (T)c_dN[gp][n][1], d2 = (T)c_dN[gp][n][2];
@@ -153,40 +339,50 @@ __global__ void __launch_bounds__(kThreads) element_loop_kernel(ElemArgs<T> a) {
 #pragma unroll
                     for (int j = 0; j < 3; ++j) {
                         gX[j] = JXi[j][0] * d0 + JXi[j][1] * d1 + JXi[j][2] * d2;
-                        gx[j] = Jci[j][0] * d0 + Jci[j][1] * d1 + Jci[j][2] * d2;
-                        sm.g[gp][n][j][el] = (status & 1) ? T(0) : gx[j];
+                        gx[j] = (status & 1) ? T(0) : Jci[j][0] * d0 + Jci[j][1] * d1 + Jci[j][2] * d2;
+                    }
+                    st4<T>(sg + ((gp * 8 + n) * kTileE + el) * 4, gx[0], gx[1], gx[2], T(0));
+                    T uu[3];
+                    if constexpr (sizeof(T) == 4) {
+                        const float4 uv = reinterpret_cast<const float4*>(sxf + (n * kTileE + el) * 8)[1];
+                        uu[0] = uv.x; uu[1] = uv.y; uu[2] = uv.z;
+                    } else {
+                        const double* up = su + (n * kTileE + el) * 3;
+                        uu[0] = (T)up[0]; uu[1] = (T)up[1]; uu[2] = (T)up[2];
                     }
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
-                        const T ui = (T)sm.u[n][i][el];
 #pragma unroll
-                        for (int j = 0; j < 3; ++j) F[i][j] += ui * gX[j];
+                        for (int j = 0; j < 3; ++j) F[i][j] += uu[i] * gX[j];
                     }
                 }
                 // constitutive update
                 T p[NP];
 #pragma unroll
                 for (int k = 0; k < NP; ++k) {
-                    if (a.param_mode == 0) p[k] = a.params[k];
+                    if (a.param_mode == 0) p[k] = a.pu[k];
                     else if (a.param_mode == 1) p[k] = a.params[(size_t)k * a.n_elem + e];
                     else p[k] = a.params[(size_t)__ldg(a.mat_id + e) * a.n_params + k];
                 }
-                T st[NS > 0 ? NS : 1], stn[NS > 0 ? NS : 1];
-#pragma unroll
-                for (int k = 0; k < NS; ++k) st[k] = a.st_old[((size_t)k * 8 + gp) * a.n_elem + e];
+                StateIO<T> io{sst + gp * kTileE + el, a.st_new, (size_t)8 * a.ld, (size_t)gp * a.ld + e};
                 T sig[6], D[21];
                 if (status & 1) {
 #pragma unroll
                     for (int k = 0; k < 6; ++k) sig[k] = T(0);
 #pragma unroll
                     for (int k = 0; k < 21; ++k) D[k] = T(0);
-#pragma unroll
-                    for (int k = 0; k < NS; ++k) stn[k] = st[k];
+                    for (int k = 0; k < a.ns_used; ++k) io.st(k, io.ld(k));
                 } else {
-                    run_material<T, MODEL>(F, p, a.dt, st, stn, sig, D);
-                }
+                    T ebr[4];
 #pragma unroll
-                for (int k = 0; k < NS; ++k) a.st_new[((size_t)k * 8 + gp) * a.n_elem + e] = stn[k];
+                    for (int k = 0; k < 4; ++k) {
+                        if (MODEL == M_VISCO_PRONY && a.param_mode != 0)
+                            ebr[k] = texp<T>((T)(-a.dt) / (T(2) * p[4 + 2 * k]));
+                        else
+                            ebr[k] = a.ebr[k];
+                    }
+                    run_material<T, MODEL>(F, p, ebr, io, sig, D);
+                }
                 bool finite = true;
 #pragma unroll
                 for (int k = 0; k < 6; ++k) finite = finite && isfinite(sig[k]);
@@ -196,24 +392,35 @@ __global__ void __launch_bounds__(kThreads) element_loop_kernel(ElemArgs<T> a) {
                     for (int k = 0; k < 6; ++k) a.gp_stress[((size_t)k * 8 + gp) * a.n_elem + e] = sig[k];
                 }
                 const T w = (status & 5) ? T(0) : detJ;  // Gauss weight is 1 (Hexa8 full integration)
+                T* dst = sds + (size_t)gp * 7 * kTileE * 4 + el * 4;
 #pragma unroll
-                for (int k = 0; k < 6; ++k) sm.s[gp][k][el] = w * sig[k];
-#pragma unroll
-                for (int k = 0; k < 21; ++k) sm.D[gp][k][el] = w * D[k];
-                if (status) atomicOr(&sm.status[el], status);
+                for (int q = 0; q < 5; ++q)
+                    st4<T>(dst + q * kTileE * 4, w * D[4 * q], w * D[4 * q + 1], w * D[4 * q + 2], w * D[4 * q + 3]);
+                st4<T>(dst + 5 * kTileE * 4, w * D[20], w * sig[0], w * sig[1], w * sig[2]);
+                st4<T>(dst + 6 * kTileE * 4, w * sig[3], w * sig[4], w * sig[5], T(0));
+                if (status) atomicOr(&sstatus[el], status);
             }
         }
-        __syncthreads();
-        if (t < kTileE && e0 + t < a.n_elem) {
-            const int st = sm.status[t];
-            a.elem_status[e0 + t] = (uint8_t)st;
-            if (st) atomicAdd(a.status_count, 1);
+        cp_wait_all();    // connectivity of the next tile has landed
+        __syncthreads();  // phase A results visible; x, u and state buffers are free
+        if (next < n_tiles) {
+            prefetch_nodes_state(a, e0n, snode + (buf ^ 1) * NB, sx, su, sxf, srs + (buf ^ 1) * NB,
+                                 snup + (buf ^ 1) * NB, sst, t);
+            cp_commit();
+        }
+        if (t < kTileE) {
+            if (e0 + t < a.e_end) {
+                const int st = sstatus[t];
+                a.elem_status[e0 + t] = (uint8_t)st;
+                if (st) atomicAdd(a.status_count, 1);
+            }
+            sstatus[t] = 0;
         }
 
         // ---------------- phase B: thread (node b = warp, element = lane) -------------------
         {
             const int b = warp, el = lane, e = e0 + el;
-            if (e < a.n_elem) {
+            if (e < a.e_end) {
                 const int npair = (b < 4) ? 4 : 3;  // off-diagonal partners a = b+1..b+npair (mod 8)
                 T f0 = 0, f1 = 0, f2 = 0;
                 T Kd[6] = {0, 0, 0, 0, 0, 0};
@@ -224,12 +431,16 @@ __global__ void __launch_bounds__(kThreads) element_loop_kernel(ElemArgs<T> a) {
                     for (int k = 0; k < 9; ++k) Ko[o][k] = T(0);
 #pragma unroll 1
                 for (int gp = 0; gp < 8; ++gp) {
-                    const T gx = sm.g[gp][b][0][el], gy = sm.g[gp][b][1][el], gz = sm.g[gp][b][2][el];
-                    T Dm[21];
+                    const T* src = sds + (size_t)gp * 7 * kTileE * 4 + el * 4;
+                    T Dm[21], s0, s1, s2, s3, s4, s5, pad;
 #pragma unroll
-                    for (int k = 0; k < 21; ++k) Dm[k] = sm.D[gp][k][el];
-                    const T s0 = sm.s[gp][0][el], s1 = sm.s[gp][1][el], s2 = sm.s[gp][2][el], s3 = sm.s[gp][3][el],
-                            s4 = sm.s[gp][4][el], s5 = sm.s[gp][5][el];
+                    for (int q = 0; q < 5; ++q)
+                        ld4<T>(src + q * kTileE * 4, Dm[4 * q], Dm[4 * q + 1], Dm[4 * q + 2], Dm[4 * q + 3]);
+                    ld4<T>(src + 5 * kTileE * 4, Dm[20], s0, s1, s2);
+                    ld4<T>(src + 6 * kTileE * 4, s3, s4, s5, pad);
+                    const T* gsrc = sg + (size_t)gp * 8 * kTileE * 4 + el * 4;
+                    T gx, gy, gz;
+                    ld4<T>(gsrc + b * kTileE * 4, gx, gy, gz, pad);
                     // sigma g_b: the internal force of node b and the geometric term
                     const T q0 = s0 * gx + s3 * gy + s5 * gz;
                     const T q1 = s3 * gx + s1 * gy + s4 * gz;
@@ -252,21 +463,19 @@ __global__ void __launch_bounds__(kThreads) element_loop_kernel(ElemArgs<T> a) {
                     // diagonal block (b,b), upper 6
                     {
                         const T geo = gx * q0 + gy * q1 + gz * q2;
-                        T M[3][3];
-#pragma unroll
-                        for (int l = 0; l < 3; ++l) {
-                            M[0][l] = gx * DB[0][l] + gy * DB[3][l] + gz * DB[5][l];
-                            M[1][l] = gy * DB[1][l] + gx * DB[3][l] + gz * DB[4][l];
-                            M[2][l] = gz * DB[2][l] + gy * DB[4][l] + gx * DB[5][l];
-                        }
-                        Kd[0] += M[0][0] + geo; Kd[1] += M[0][1]; Kd[2] += M[0][2];
-                        Kd[3] += M[1][1] + geo; Kd[4] += M[1][2]; Kd[5] += M[2][2] + geo;
+                        Kd[0] += gx * DB[0][0] + gy * DB[3][0] + gz * DB[5][0] + geo;
+                        Kd[1] += gx * DB[0][1] + gy * DB[3][1] + gz * DB[5][1];
+                        Kd[2] += gx * DB[0][2] + gy * DB[3][2] + gz * DB[5][2];
+                        Kd[3] += gy * DB[1][1] + gx * DB[3][1] + gz * DB[4][1] + geo;
+                        Kd[4] += gy * DB[1][2] + gx * DB[3][2] + gz * DB[4][2];
+                        Kd[5] += gz * DB[2][2] + gy * DB[4][2] + gx * DB[5][2] + geo;
                     }
 #pragma unroll
                     for (int o = 0; o < 4; ++o) {
                         if (o < npair) {
                             const int an = (b + 1 + o) & 7;
-                            const T ax = sm.g[gp][an][0][el], ay = sm.g[gp][an][1][el], az = sm.g[gp][an][2][el];
+                            T ax, ay, az;
+                            ld4<T>(gsrc + an * kTileE * 4, ax, ay, az, pad);
                             const T geo = ax * q0 + ay * q1 + az * q2;
 #pragma unroll
                             for (int l = 0; l < 3; ++l) {
@@ -279,14 +488,14 @@ __global__ void __launch_bounds__(kThreads) element_loop_kernel(ElemArgs<T> a) {
                     }
                 }
                 // ---- scatter ----
-                const int Bn = sm.node[b][el];
+                const int Bn = node_c[b * kTileE + el];
                 atomicAdd(a.fint + 3 * (size_t)Bn + 0, (double)f0);
                 atomicAdd(a.fint + 3 * (size_t)Bn + 1, (double)f1);
                 atomicAdd(a.fint + 3 * (size_t)Bn + 2, (double)f2);
-                if (a.kval) {
+                if (a.kval && !BLOCKED) {
                     {
-                        const long long r0 = sm.rs[b][el];
-                        const int m = sm.nup[b][el];
+                        const long long r0 = rs_c[b * kTileE + el];
+                        const int m = nup_c[b * kTileE + el];
                         const long long r1 = r0 + 3 + 3 * m, r2 = r1 + 2 + 3 * m;
                         double* K = a.kval;
                         atomicAdd(K + r0 + 0, (double)Kd[0]);
@@ -296,18 +505,18 @@ __global__ void __launch_bounds__(kThreads) element_loop_kernel(ElemArgs<T> a) {
                         atomicAdd(K + r1 + 1, (double)Kd[4]);
                         atomicAdd(K + r2 + 0, (double)Kd[5]);
                     }
-                    const uint8_t* rk = reinterpret_cast<const uint8_t*>(&sm.ranks[el][0]);
+                    const uint8_t* rk = reinterpret_cast<const uint8_t*>(ranks_c + el * 8);
 #pragma unroll
                     for (int o = 0; o < 4; ++o) {
                         if (o < npair) {
                             const int an = (b + 1 + o) & 7;
-                            const int An = sm.node[an][el];
+                            const int An = node_c[an * kTileE + el];
                             const int lo_local = an < b ? an : b, hi_local = an < b ? b : an;
                             const int r = rk[pair_index(lo_local, hi_local)];
                             const bool a_low = An < Bn;  // rows belong to the smaller global node
                             const int lo_n = a_low ? an : b;
-                            const long long r0 = sm.rs[lo_n][el];
-                            const int m = sm.nup[lo_n][el];
+                            const long long r0 = rs_c[lo_n * kTileE + el];
+                            const int m = nup_c[lo_n * kTileE + el];
                             const long long row0 = r0 + 3 + 3 * r;
                             const long long row1 = r0 + (3 + 3 * m) + 2 + 3 * r;
                             const long long row2 = r0 + (3 + 3 * m) + (2 + 3 * m) + 1 + 3 * r;
@@ -330,10 +539,44 @@ __global__ void __launch_bounds__(kThreads) element_loop_kernel(ElemArgs<T> a) {
                         }
                     }
                 }
+                if (a.kval && BLOCKED) {
+                    // node-pair blocks: one 16-byte vector reduction per block row
+                    {
+                        const long long r0 = rs_c[b * kTileE + el];
+                        float* blk = a.kblk + ((long long)Bn + (r0 - 6LL * Bn) / 9) * 12;
+                        red_v4(blk + 0, (float)Kd[0], (float)Kd[1], (float)Kd[2], 0.f);
+                        red_v4(blk + 4, 0.f, (float)Kd[3], (float)Kd[4], 0.f);
+                        red_v4(blk + 8, 0.f, 0.f, (float)Kd[5], 0.f);
+                    }
+                    const uint8_t* rk = reinterpret_cast<const uint8_t*>(ranks_c + el * 8);
+#pragma unroll
+                    for (int o = 0; o < 4; ++o) {
+                        if (o < npair) {
+                            const int an = (b + 1 + o) & 7;
+                            const int An = node_c[an * kTileE + el];
+                            const int lo_local = an < b ? an : b, hi_local = an < b ? b : an;
+                            const int r = rk[pair_index(lo_local, hi_local)];
+                            const bool a_low = An < Bn;
+                            const int lo_n = a_low ? an : b;
+                            const int lo_node = a_low ? An : Bn;
+                            const long long r0 = rs_c[lo_n * kTileE + el];
+                            float* blk = a.kblk + ((long long)lo_node + (r0 - 6LL * lo_node) / 9 + 1 + r) * 12;
+                            if (a_low) {  // rows of node a: M[k][:]
+                                red_v4(blk + 0, (float)Ko[o][0], (float)Ko[o][1], (float)Ko[o][2], 0.f);
+                                red_v4(blk + 4, (float)Ko[o][3], (float)Ko[o][4], (float)Ko[o][5], 0.f);
+                                red_v4(blk + 8, (float)Ko[o][6], (float)Ko[o][7], (float)Ko[o][8], 0.f);
+                            } else {      // rows of node b: M[:][l]
+                                red_v4(blk + 0, (float)Ko[o][0], (float)Ko[o][3], (float)Ko[o][6], 0.f);
+                                red_v4(blk + 4, (float)Ko[o][1], (float)Ko[o][4], (float)Ko[o][7], 0.f);
+                                red_v4(blk + 8, (float)Ko[o][2], (float)Ko[o][5], (float)Ko[o][8], 0.f);
+                            }
+                        }
+                    }
+                }
             }
         }
-        __syncthreads();
     }
+    cp_wait_all();
 }
 
 }  // namespace ceos

@@ -157,58 +157,63 @@ CEOS_D void j2_small_update(const T F[3][3], const T* p, const T* st, T* stn, T 
 //   c = c_vol + (1 + sum beta_a e_a) c_iso.
 // params [mu, K, nb, beta1, tau1, ..., beta4, tau4]; state [S_iso^n (6), Q_1..Q_4 (6 each)].
 // ---------------------------------------------------------------------------------------
-template <typename T>
-CEOS_D void visco_prony_update(const T F[3][3], const T* p, double dt, const T* st, T* stn, T sig[6], T D[21]) {
+template <typename T, typename IO>
+CEOS_D void visco_prony_update(const T F[3][3], const T* p, const T* ebr, const IO& io, T sig[6], T D[21]) {
+    // ebr[a] = exp(-dt / (2 tau_a)) for the branches (computed once per launch)
     const T mu = p[0], K = p[1];
     const int nb = (int)p[2];
-    T C[6], b[6];
+    T C[6];
     fTf(F, C);
-    ffT(F, b);
     const double Jd = det3_fp64(F);
     const double lnJd = log(Jd);
     const T J = (T)Jd, lnJ = (T)lnJd;
-    const T J23 = (T)exp(-2.0 / 3.0 * lnJd);
-    T Ci[6];
-    inv_sym(C, (T)(Jd * Jd), Ci);
-    const T trC = C[0] + C[1] + C[2];
+    const T J23 = texp<T>(T(-2.0 / 3.0) * lnJ);
     T Siso[6];
+    {
+        T Ci[6];
+        inv_sym(C, (T)(Jd * Jd), Ci);
+        const T trC3 = (C[0] + C[1] + C[2]) * T(1.0 / 3.0);
+        const T muJ = mu * J23;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) Siso[k] = mu * J23 * ((T)delta6(k) - trC / T(3) * Ci[k]);
+        for (int k = 0; k < 6; ++k) Siso[k] = muJ * ((T)delta6(k) - trC3 * Ci[k]);
+    }
     T Qs[6] = {0, 0, 0, 0, 0, 0};
     T dsum = T(0);
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         if (a < nb) {
-            const T beta = p[3 + 2 * a], tau = p[4 + 2 * a];
-            const T e = texp<T>((T)(-dt) / (T(2) * tau));
+            const T beta = p[3 + 2 * a];
+            const T e = ebr[a];
+            const T be = beta * e;
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
-                const T q = e * (e * st[6 + 6 * a + k] - beta * st[k]) + beta * e * Siso[k];
-                stn[6 + 6 * a + k] = q;
+                const T q = e * (e * io.ld(6 + 6 * a + k) - beta * io.ld(k)) + be * Siso[k];
+                io.st(6 + 6 * a + k, q);
                 Qs[k] += q;
             }
-            dsum += beta * e;
-        } else {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) stn[6 + 6 * a + k] = T(0);
+            dsum += be;
         }
     }
 #pragma unroll
-    for (int k = 0; k < 6; ++k) stn[k] = Siso[k];
+    for (int k = 0; k < 6; ++k) io.st(k, Siso[k]);
     T tq[6];
     push_sym(F, Qs, tq);
+    T b[6];
+    ffT(F, b);
     const T trb = b[0] + b[1] + b[2];
     T tiso[6];
     const T invJ = T(1) / J;
     const T pv = K * lnJ * invJ;
+    const T muJ = mu * J23;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-        tiso[k] = mu * J23 * (b[k] - trb / T(3) * (T)delta6(k));
+        tiso[k] = muJ * (b[k] - trb * T(1.0 / 3.0) * (T)delta6(k));
         sig[k] = pv * (T)delta6(k) + (tiso[k] + tq[k]) * invJ;
     }
     const T I1b = J23 * trb;
     const T f = (T(1) + dsum) * invJ;
     const T kj = K * invJ;
+    const T c23 = T(2.0 / 3.0) * mu * I1b;
 #pragma unroll
     for (int a = 0; a < 6; ++a)
 #pragma unroll
@@ -216,8 +221,7 @@ CEOS_D void visco_prony_update(const T F[3][3], const T* p, double dt, const T* 
             const T Is = (a == c ? (a < 3 ? T(1) : T(0.5)) : T(0));
             const T dd = (T)(delta6(a) * delta6(c));
             const T vol = kj * dd - T(2) * pv * Is;
-            const T iso = T(2.0 / 3.0) * mu * I1b * (Is - dd / T(3)) -
-                          T(2.0 / 3.0) * (tiso[a] * (T)delta6(c) + (T)delta6(a) * tiso[c]);
+            const T iso = c23 * (Is - dd * T(1.0 / 3.0)) - T(2.0 / 3.0) * (tiso[a] * (T)delta6(c) + (T)delta6(a) * tiso[c]);
             D[up21(a, c)] = vol + f * iso;
         }
 }
