@@ -127,6 +127,26 @@ int ceos_set_committed_time(void* handle, double t);
 /* Release every device buffer and the stream. */
 void ceos_destroy(void* handle);
 
+/* Allocation-free assembly (no counterpart in the reference: CEOS assembles on the host).
+ * For callers that cannot call cudaMalloc while they assemble, because the GPU memory belongs
+ * to their own allocator or pool: one evaluation of the compressible Neo-Hookean element loop
+ * (Gauss-point update, f_int, K into the upper CSR) in FP32 element arithmetic, taking only
+ * caller-owned device buffers -- X [3*n_nodes] and U [3*n_nodes] (FP64), conn [8*n_elem]
+ * (1-based), the 1-based upper CSR pattern rowmap [3*n_nodes+1] / col [nnz] exactly as
+ * ceos_pattern exports it, outputs fint [3*n_nodes] and kval [nnz] (FP64) -- on the current
+ * CUDA device and `stream` (NULL: default stream).  The FP32 node-pair block scratch is a static
+ * 8 MiB device array inside the library (held by every GPU that loads it until exit), so a
+ * call accepts at most 174,762 node pairs, i.e. n_nodes + (nnz - 6*n_nodes)/9 <= 174,762
+ * (about 12,000 nodes of a structured Hexa8 mesh); larger meshes return CEOS_E_ARG.  It calls no
+ * cudaMalloc or cudaFree.  The first call on a device resolves the scratch address there
+ * (cudaGetSymbolAddress) and should come before any stream capture.  Calls share the scratch:
+ * each clears what it uses first, and calls that overlap on the GPU race.  Synchronous;
+ * returns 0, 1 (det J <= 1e-13 somewhere) or a negative CEOS_E_* code. */
+int ceos_cnh_assemble_noalloc(int n_nodes, int n_elem, const double* X_device, const double* U_device,
+                              const int* conn_device, const int* rowmap_device, const int* col_device,
+                              long long nnz, double mu, double lambda, double* fint_device,
+                              double* kval_device, void* stream);
+
 /* ---- Host driver above the boundary (the Fortran host's role, restated in C++) ----------
  * Quasi-static analysis of one load case: QuasiStaticAnalysisFEM (ModFEMAnalysis.f90:1136-1374),
  * NewtonRaphsonFull_Solve (ModNewtonRaphsonFull.f90:44-168) and ApplyBoundaryConditionsNEW
