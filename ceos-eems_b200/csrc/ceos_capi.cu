@@ -38,6 +38,7 @@ int model_nparams(int model) {
         case M_J2_SMALL: return ModelInfo<M_J2_SMALL>::nparams;
         case M_VISCO_PRONY: return ModelInfo<M_VISCO_PRONY>::nparams;
         case M_J2_FINITE: return ModelInfo<M_J2_FINITE>::nparams;
+        case M_VISCO_VAR: return ModelInfo<M_VISCO_VAR>::nparams;
     }
     return -1;
 }
@@ -48,6 +49,7 @@ int model_nstate(int model) {
         case M_J2_SMALL: return ModelInfo<M_J2_SMALL>::nstate;
         case M_VISCO_PRONY: return ModelInfo<M_VISCO_PRONY>::nstate;
         case M_J2_FINITE: return ModelInfo<M_J2_FINITE>::nstate;
+        case M_VISCO_VAR: return ModelInfo<M_VISCO_VAR>::nstate;
     }
     return -1;
 }
@@ -55,6 +57,7 @@ void model_init_state(int model, double* st) {
     const int ns = model_nstate(model);
     for (int i = 0; i < ns; ++i) st[i] = 0.0;
     if (model == M_J2_FINITE) st[0] = st[1] = st[2] = 1.0;  // Cp^{-1} = I
+    if (model == M_VISCO_VAR) st[0] = st[4] = st[8] = 1.0;  // Fv = I (ModViscoelasticMatrix.f90:124-131)
 }
 
 #define CK(call)                                                              \
@@ -131,6 +134,7 @@ int launch_elem(Handle* h, double dt, const double* dU, double* dfint, double* d
         case M_J2_SMALL: return launch_model<T, M_J2_SMALL>(h, dt, dU, dfint, dkval, s);
         case M_VISCO_PRONY: return launch_model<T, M_VISCO_PRONY>(h, dt, dU, dfint, dkval, s);
         case M_J2_FINITE: return launch_model<T, M_J2_FINITE>(h, dt, dU, dfint, dkval, s);
+        case M_VISCO_VAR: return launch_model<T, M_VISCO_VAR>(h, dt, dU, dfint, dkval, s);
     }
     return CEOS_E_MODEL;
 }
@@ -160,6 +164,10 @@ int occupancy_grid(Handle* h) {
         case M_J2_FINITE:
             e = cudaFuncSetAttribute(element_loop_kernel<T, M_J2_FINITE, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
             if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_J2_FINITE, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
+            break;
+        case M_VISCO_VAR:
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_VISCO_VAR, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_VISCO_VAR, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
             break;
     }
     if (e != cudaSuccess || per_sm < 1) per_sm = 1;

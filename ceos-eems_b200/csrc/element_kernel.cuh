@@ -23,6 +23,7 @@
 #pragma once
 #include "ceos_common.cuh"
 #include "materials.cuh"
+#include "visco_var.cuh"
 
 namespace ceos {
 
@@ -116,8 +117,10 @@ struct StateIO {
 };
 
 template <typename T, int MODEL>
-CEOS_D void run_material(const T F[3][3], const T* p, const T* ebr, const StateIO<T>& io, T sig[6], T D[21]) {
+CEOS_D int run_material(const T F[3][3], const T* p, const T* ebr, double dt, const StateIO<T>& io, T sig[6],
+                        T D[21]) {
     constexpr int NS = ModelInfo<MODEL>::nstate;
+    int status = 0;
     if constexpr (MODEL == M_CNH) {
         cnh_update<T>(F, p, sig, D);
     } else if constexpr (MODEL == M_SVK) {
@@ -130,9 +133,11 @@ CEOS_D void run_material(const T F[3][3], const T* p, const T* ebr, const StateI
         for (int k = 0; k < NS; ++k) st[k] = io.ld(k);
         if constexpr (MODEL == M_J2_SMALL) j2_small_update<T>(F, p, st, stn, sig, D);
         else if constexpr (MODEL == M_J2_FINITE) j2_finite_update<T>(F, p, st, stn, sig, D);
+        else if constexpr (MODEL == M_VISCO_VAR) status = vv::update<T>(F, p, dt, st, stn, sig, D);
 #pragma unroll
         for (int k = 0; k < NS; ++k) io.st(k, stn[k]);
     }
+    return status;
 }
 
 template <typename T>
@@ -381,7 +386,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                         else
                             ebr[k] = a.ebr[k];
                     }
-                    run_material<T, MODEL>(F, p, ebr, io, sig, D);
+                    status |= run_material<T, MODEL>(F, p, ebr, a.dt, io, sig, D);
                 }
                 bool finite = true;
 #pragma unroll

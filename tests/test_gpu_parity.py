@@ -17,6 +17,7 @@ SVK_P = [100.0e9, 0.3]
 J2S_P = [200.0e3, 0.3, 250.0, 1000.0]
 J2F_P = [200.0e3, 0.3, 250.0, 1000.0]
 PRONY_P = [1.0, 100.0, 3, 0.3, 0.01, 0.2, 0.1, 0.1, 1.0, 0.0, 1.0]
+VV_P = [0.0, 1.0, 100.0 - 2.0 / 3.0, 0.0, 0.5, 0.2]   # K_inf, Mu_inf, Lambda_inf, K_e, Mu_e, Ni_v
 
 
 def smooth_u(X, amp, seed=1):
@@ -69,7 +70,7 @@ def _pair(model, params, X, conn, precision=G.FP64, per_element=False):
 
 @pytest.mark.parametrize("model,params,amp", [
     (G.CNH, CNH_P, 0.08), (G.SVK, SVK_P, 0.05), (G.J2_SMALL, J2S_P, 0.01),
-    (G.J2_FINITE, J2F_P, 0.01), (G.VISCO_PRONY, PRONY_P, 0.08)])
+    (G.J2_FINITE, J2F_P, 0.01), (G.VISCO_PRONY, PRONY_P, 0.08), (G.VISCO_VAR, VV_P, 0.05)])
 def test_evaluate_fp64(model, params, amp):
     X, conn = meshgen.structured_box(6, 5, 4, jitter=0.05, seed=2)
     g, o = _pair(model, params, X, conn)
@@ -92,7 +93,8 @@ def test_evaluate_fp64(model, params, amp):
 
 
 @pytest.mark.parametrize("model,params,amp,tol", [
-    (G.CNH, CNH_P, 0.08, 2e-5), (G.VISCO_PRONY, PRONY_P, 0.08, 2e-5), (G.J2_FINITE, J2F_P, 0.01, 5e-5)])
+    (G.CNH, CNH_P, 0.08, 2e-5), (G.VISCO_PRONY, PRONY_P, 0.08, 2e-5), (G.J2_FINITE, J2F_P, 0.01, 5e-5),
+    (G.VISCO_VAR, VV_P, 0.05, 2e-5)])
 def test_evaluate_mixed(model, params, amp, tol):
     X, conn = meshgen.structured_box(6, 5, 4, jitter=0.05, seed=2)
     g, o = _pair(model, params, X, conn, precision=G.MIXED)

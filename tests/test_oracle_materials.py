@@ -132,3 +132,38 @@ def test_j2_small_return_mapping_consistency():
     s = sig - np.r_[np.full(3, p), np.zeros(3)]
     q = np.sqrt(1.5 * ((s[:3] ** 2).sum() + 2 * (s[3:] ** 2).sum()))
     assert np.isclose(q, J2_P[2] + J2_P[3] * st_new[6], rtol=1e-12)
+
+
+VV_P = [0.0, 1.0, 100.0 - 2.0 / 3.0, 0.0, 0.5, 0.2]  # K_inf, Mu_inf, Lambda_inf, K_e, Mu_e, Ni_v
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_visco_var_tangent_consistency_and_incompressible_flow(seed):
+    """The reference's variational model (ModViscoelasticMatrix.f90): the consistent tangent of
+    the local-Newton solution matches finite differences, and the converged viscous flow keeps
+    det Fv = 1 to the local tolerance."""
+    st0 = O.init_state(O.VISCO_VAR, VV_P)
+    _, _, st1, rc = O.material_point(O.VISCO_VAR, VV_P, rand_F(seed + 5, 0.05), 0.1, st0)
+    assert rc == 0
+    assert abs(np.linalg.det(st1[:9].reshape(3, 3, order="F")) - 1.0) < 1e-5
+    D, Dfd = fd_tangent(O.VISCO_VAR, VV_P, rand_F(seed, 0.05), dt=0.1, st_old=st1, h=1e-6)
+    assert np.abs(D - Dfd).max() <= 1e-5 * np.abs(D).max()
+
+
+def test_visco_var_relaxes_to_equilibrium_branch():
+    """Held isochoric stretch: after a long time the Maxwell branch relaxes and the stress tends to
+    the equilibrium Neo-Hookean branch alone (Mu_inf, Lambda_inf).  (The viscous flow is
+    isochoric, J_v = 1, so a volumetric stretch would keep a residual branch stress.)"""
+    F = np.diag([1.05, 1.05 ** -0.5, 1.05 ** -0.5])
+    st = O.init_state(O.VISCO_VAR, VV_P)
+    s_first = None
+    for k in range(60):
+        sig, _, st, rc = O.material_point(O.VISCO_VAR, VV_P, F, 0.5, st)
+        assert rc == 0
+        if s_first is None:
+            s_first = sig.copy()
+    eq = list(VV_P)
+    eq[4] = 1e-12  # no Maxwell branch
+    s_eq, _, _, _ = O.material_point(O.VISCO_VAR, eq, F, 0.5, O.init_state(O.VISCO_VAR, eq))
+    assert abs(s_first[0] - s_eq[0]) > 1e-3 * abs(s_eq[0])   # the branch carries stress at first
+    assert np.allclose(sig, s_eq, rtol=1e-4, atol=1e-8)     # and has relaxed at the end
