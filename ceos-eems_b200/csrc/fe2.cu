@@ -1,0 +1,960 @@
+// fe2.cu -- batched FE^2 micro problems: many periodic RVEs solved together on one GPU.
+//
+// The reference solves ONE representative volume element at a time under a prescribed macro
+// deformation gradient (MultiScale/ModMultiscaleAnalysis.f90:445-470, periodic constraints by
+// the elimination K_red = T^T K T in FEM/Modules/ModMultiscalePeriodicFEMSoE.f90:77-182) and
+// homogenizes the first Piola stress (HomogenizeStress, ModMultiscaleAnalysis.f90:140-329).  The
+// batched solver here has no reference counterpart:
+//   * all RVEs form one disjoint Hexa8 mesh evaluated by the fused element kernel (FP64);
+//   * periodicity: node (i,j,k) of an n^3 RVE carries the fluctuation of independent node
+//     (i mod n, j mod n, k mod n); independent node 0 is held fixed (rigid translation);
+//     u = (Fbar - I) X + w(independent node);
+//   * Newton on the fluctuations; every linear system T^T K T dw = -T^T f_int is solved by
+//     fe2_minres_kernel: a persistent kernel, one CTA per RVE taken from a work queue ordered
+//     by size (largest first), block-Jacobi (3x3 nodal, SPD) preconditioned MINRES in FP32
+//     shared memory with FP64 iterative refinement of the residual to a relative 1e-8 (MINRES
+//     rather than CG because T^T K T turns indefinite when compressed fibres buckle);
+//   * Pbar = (1/V0) sum_a f_int,a (x) X_a (virtual work with the affine modes, equal to the
+//     Gauss-point integral of HomogenizeStress for the same quadrature) and the 9x9 tangent
+//     dPbar/dFbar = (Z^T K Z - M^T (T^T K T)^{-1} M)/V0 with M = T^T K Z (static condensation).
+// Every loop has an iteration cap; no kernel waits on another CTA.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cmath>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/ceos_gpu.h"
+#include "ceos_handle.h"
+
+namespace {
+
+using ceos::Handle;
+
+constexpr int kSolveThreads = 512;
+constexpr int kMaxCells = 14;  // largest RVE (cells per side) the shared-memory solver holds
+
+struct Fe2 {
+    int n_rve = 0, device = 0;
+    double force_floor = 0.0;            // residual norm below which an RVE counts as converged
+    int n_sub = 1;                       // macro load sub-increments per solve
+    std::vector<int> n;                  // cells per side of each RVE
+    std::vector<double> vf_nominal, vf_actual;
+    Handle* loop = nullptr;              // element loop over the union of all RVE meshes
+    int n_nodes = 0;
+    long long nnz = 0;
+    // per RVE offsets (host and device)
+    std::vector<int> node_off, red_off, nodes_of;  // node_off[r], reduced dof offset, node count
+    int n_red = 0;
+    int* d_node_off = nullptr;  // [n_rve+1]
+    int* d_red_off = nullptr;   // [n_rve+1]
+    int* d_ncell = nullptr;     // [n_rve]
+    int* d_rve_of_node = nullptr;
+    int* d_rve_of_elem = nullptr;  // [n_elem]
+    int* d_fail = nullptr;         // [n_rve] failed-element flag of the last assembly
+    int* d_op = nullptr;           // [n_rve] per-RVE vector operation (rve_op_kernel)
+    double* d_wc = nullptr;        // [n_red] fluctuations at the last converged load level
+    double* d_eta = nullptr;       // [n_rve] relative tolerance of each RVE's linear solve
+    int* d_fmap = nullptr;      // [3*n_nodes] global reduced dof or -1
+    int* d_col = nullptr;       // [nnz] 0-based column of the upper CSR
+    int* d_rcol = nullptr;      // [nnz] column as RVE-local reduced dof, -1 on the fixed node
+    float* d_kf = nullptr;      // [nnz] FP32 copy of the CSR values
+    int* d_order = nullptr;     // RVEs by decreasing size
+    int* d_queue = nullptr;     // work-queue counter
+    double* d_Fbar = nullptr;   // [n_rve*9] row-major
+    double* d_w = nullptr;      // [n_red] fluctuations
+    double* d_u = nullptr;      // [3*n_nodes]
+    double* d_rhs = nullptr;    // [n_red]
+    double* d_dx = nullptr;     // [n_red]
+    double* d_r64 = nullptr;    // [n_red]
+    double* d_y64 = nullptr;    // [3*n_nodes] FP64 SpMV scratch
+    float* d_minv = nullptr;    // [n_red/3 + n_rve][9] inverse nodal diagonal blocks
+    double* d_rnorm = nullptr;  // [n_rve]
+    int* d_cg_iters = nullptr;  // [n_rve]
+    int* d_active = nullptr;    // [n_rve]
+    double* d_P = nullptr;      // [n_rve*9]
+    double* d_A = nullptr;      // [n_rve*81]
+    double* d_nn = nullptr;     // [n_rve] Newton residual norms
+    double* d_Z = nullptr;      // [n_rve*81] Z^T K Z
+    double* d_M = nullptr;      // [9*n_red] M = T^T K Z (column-major per mode)
+    double* d_X9 = nullptr;     // [9*n_red] solutions of the 9 condensation systems
+    std::string msg;
+    ~Fe2() {
+        void* p[] = {d_node_off, d_red_off, d_ncell, d_rve_of_node, d_fmap, d_col, d_order, d_queue, d_Fbar, d_w,
+                     d_u, d_rhs, d_dx, d_r64, d_y64, d_minv, d_rnorm, d_cg_iters, d_active, d_P, d_A, d_nn, d_Z, d_M, d_X9,
+                     d_rve_of_elem, d_fail, d_op, d_wc, d_eta, d_rcol, d_kf};
+        for (void* q : p)
+            if (q) cudaFree(q);
+        if (loop) ceos_destroy(loop);
+    }
+};
+
+#define CKF(call)                                                                  \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            f->msg = std::string(#call) + ": " + cudaGetErrorString(e_);          \
+            return CEOS_E_CUDA;                                                    \
+        }                                                                          \
+    } while (0)
+
+// ---------------------------------------------------------------------------------------------
+// small kernels
+// ---------------------------------------------------------------------------------------------
+__global__ void expand_u_kernel(int n_nodes, const double* X, const int* rve_of_node, const double* Fbar,
+                                const int* fmap, const double* w, double* u) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * n_nodes) return;
+    const int a = i / 3, d = i - 3 * a;
+    const double* F = Fbar + 9 * rve_of_node[a];
+    double v = (F[3 * d + 0] - (d == 0)) * X[3 * a] + (F[3 * d + 1] - (d == 1)) * X[3 * a + 1] +
+               (F[3 * d + 2] - (d == 2)) * X[3 * a + 2];
+    const int q = fmap[i];
+    if (q >= 0) v += w[q];
+    u[i] = v;
+}
+
+// T^T f: fold the full-dof vector onto the reduced dofs (sign flipped: rhs = -R)
+__global__ void fold_kernel(int n_dof, const int* fmap, const double* f, double* out, double sgn) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_dof) return;
+    const int q = fmap[i];
+    if (q >= 0) atomicAdd(out + q, sgn * f[i]);
+}
+
+// Block-Jacobi: per independent node, the sum of the diagonal 3x3 blocks of the nodes mapped to
+// it (nodes n cells apart never share an element, so no off-diagonal block couples them).
+__global__ void diag_blocks_kernel(int n_nodes, const long long* rs, const int* nup, const double* K, const int* fmap,
+                                   double* acc /* [n_red/3][9] FP64 */) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_nodes) return;
+    const int q = fmap[3 * a];
+    if (q < 0) return;
+    const long long r0 = rs[a];
+    const int m = nup[a];
+    const long long r1 = r0 + 3 + 3LL * m, r2 = r1 + 2 + 3LL * m;
+    const double k00 = K[r0], k01 = K[r0 + 1], k02 = K[r0 + 2], k11 = K[r1], k12 = K[r1 + 1], k22 = K[r2];
+    double* b = acc + 3 * (size_t)q;  // q is a multiple of 3: block index q/3 -> offset 9*(q/3) = 3q
+    atomicAdd(b + 0, k00); atomicAdd(b + 1, k01); atomicAdd(b + 2, k02);
+    atomicAdd(b + 3, k01); atomicAdd(b + 4, k11); atomicAdd(b + 5, k12);
+    atomicAdd(b + 6, k02); atomicAdd(b + 7, k12); atomicAdd(b + 8, k22);
+}
+
+// SPD block-Jacobi preconditioner: the inverse of each positive definite nodal block; a block
+// that is not positive definite (compressed stiff fibre, negative geometric stiffness) falls back
+// to the inverse of its |diagonal|, so the preconditioner stays symmetric positive definite.
+__global__ void invert_blocks_kernel(int n_blk, const double* acc, float* minv) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n_blk) return;
+    const double* A = acc + 9 * (size_t)b;
+    double c[9];
+    c[0] = A[4] * A[8] - A[5] * A[7];
+    c[1] = A[2] * A[7] - A[1] * A[8];
+    c[2] = A[1] * A[5] - A[2] * A[4];
+    c[3] = A[5] * A[6] - A[3] * A[8];
+    c[4] = A[0] * A[8] - A[2] * A[6];
+    c[5] = A[2] * A[3] - A[0] * A[5];
+    c[6] = A[3] * A[7] - A[4] * A[6];
+    c[7] = A[1] * A[6] - A[0] * A[7];
+    c[8] = A[0] * A[4] - A[1] * A[3];
+    const double det = A[0] * c[0] + A[1] * c[3] + A[2] * c[6];
+    // leading principal minors, relative to the diagonal products
+    const bool pd = A[0] > 0.0 && c[8] > 1e-6 * A[0] * A[4] && det > 1e-6 * A[0] * A[4] * A[8];
+    if (pd) {
+        const double r = 1.0 / det;
+        for (int k = 0; k < 9; ++k) minv[9 * (size_t)b + k] = (float)(c[k] * r);
+    } else {
+        const double amax = fmax(fabs(A[0]), fmax(fabs(A[4]), fabs(A[8])));
+        const double fl = amax > 0.0 ? 1e-6 * amax : 1.0;
+        for (int k = 0; k < 9; ++k) minv[9 * (size_t)b + k] = 0.f;
+        minv[9 * (size_t)b + 0] = (float)(1.0 / fmax(fabs(A[0]), fl));
+        minv[9 * (size_t)b + 4] = (float)(1.0 / fmax(fabs(A[4]), fl));
+        minv[9 * (size_t)b + 8] = (float)(1.0 / fmax(fabs(A[8]), fl));
+    }
+}
+
+// FP32 copy of the CSR values for the inner iterations
+__global__ void to_f32_kernel(long long n, const double* a, float* b) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+
+// per-RVE Euclidean norm of a reduced vector (one CTA per RVE)
+__device__ __forceinline__ double block_sum_d(double v, double* red);
+__global__ void rve_norm_kernel(int n_rve, const int* red_off, const double* v, double* out) {
+    __shared__ double red[32];
+    const int rve = blockIdx.x;
+    double s = 0.0;
+    for (int q = red_off[rve] + threadIdx.x; q < red_off[rve + 1]; q += blockDim.x) s += v[q] * v[q];
+    s = block_sum_d(s, red);
+    if (threadIdx.x == 0) out[rve] = sqrt(s);
+}
+
+// RVEs with a failed element (det J <= 1e-13) in the last element-loop evaluation
+__global__ void rve_fail_kernel(int n_elem, const uint8_t* elem_status, const int* rve_of_elem, int* fail) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n_elem && elem_status[e]) atomicOr(fail + rve_of_elem[e], 1);
+}
+// Per-RVE operations on the reduced vectors (one CTA per RVE):
+//   1 backtrack: w -= dx/2, dx /= 2   2 restore: w = wc   3 save: wc = w
+enum { kOpNone = 0, kOpBacktrack = 1, kOpRestore = 2, kOpSave = 3 };
+__global__ void rve_op_kernel(int n_rve, const int* red_off, const int* op, double* w, double* dx, double* wc) {
+    const int rve = blockIdx.x;
+    const int o = op[rve];
+    if (o == kOpNone) return;
+    for (int q = red_off[rve] + threadIdx.x; q < red_off[rve + 1]; q += blockDim.x) {
+        if (o == kOpBacktrack) {
+            w[q] -= 0.5 * dx[q];
+            dx[q] *= 0.5;
+        } else if (o == kOpRestore) {
+            w[q] = wc[q];
+        } else {
+            wc[q] = w[q];
+        }
+    }
+}
+
+// w += dx on the RVEs that solved for a Newton correction
+__global__ void rve_step_kernel(int n_rve, const int* red_off, const int* sel, const double* dx, double* w) {
+    const int rve = blockIdx.x;
+    if (!sel[rve]) return;
+    for (int q = red_off[rve] + threadIdx.x; q < red_off[rve + 1]; q += blockDim.x) w[q] += dx[q];
+}
+
+// ---------------------------------------------------------------------------------------------
+// persistent block-Jacobi MINRES: one CTA per RVE
+// ---------------------------------------------------------------------------------------------
+// T^T K T is symmetric but INDEFINITE once the stiff fibres are compressed past their
+// micro-buckling load (negative geometric stiffness), where CG breaks down.  MINRES (Paige and
+// Saunders, SIAM J. Numer. Anal. 12, 1975) minimises the residual over the same Krylov space at
+// the same cost per iteration (one SpMV, two block reductions) and only needs a symmetric
+// positive definite preconditioner.
+struct SolveArgs {
+    int n_rve, max_inner, max_outer;
+    double inner_floor;    // smallest relative reduction asked of one FP32 cycle
+    const double* eta;     // [n_rve] target relative residual of each RVE's solve
+    const int* order;      // RVE indices, largest first
+    int* queue;            // work counter
+    const int* active;     // RVE participates in this solve
+    const int* node_off;   // [n_rve+1]
+    const int* red_off;    // [n_rve+1]
+    const int* fmap;       // full dof -> global reduced dof or -1
+    const long long* rs;   // CSR row start of row 3a
+    const int* nup;
+    const int* rcol;       // [nnz] column mapped to the RVE-local reduced dof, or -1
+    const double* K;       // upper CSR values (FP64), refinement residuals
+    const float* Kf;       // the same values in FP32, inner iterations
+    const float* minv;     // SPD block-Jacobi inverse per independent node
+    int nrhs;              // right-hand sides solved one after another
+    const double* rhs;     // [nrhs][n_red]
+    double* x;             // [nrhs][n_red] solution
+    double* r64;           // [n_red] FP64 residual scratch
+    int* iters;            // [n_rve] total inner iterations (last rhs)
+    double* rnorm;         // [n_rve] final relative residual (last rhs)
+    int n_red;
+};
+
+__device__ __forceinline__ float block_sum_f(float v, float* red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    float s = 0.f;
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) red[0] = s;
+    }
+    __syncthreads();
+    return red[0];
+}
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) red[0] = s;
+    }
+    __syncthreads();
+    return red[0];
+}
+
+// y += T^T K T x over the full rows of one RVE, directly in its local reduced numbering (warp
+// per full row, lanes over the row's upper entries, the transposed half by shared atomics).
+// Two different dofs of one element never map to the same reduced dof for n >= 2 (periodic
+// images are n cells apart), so c == ir only on the diagonal.
+template <typename V, typename KV>
+__device__ void rve_spmv_red(int row0, int nrow, int q0, const int* fmap, const long long* rs, const int* nup,
+                             const int* rcol, const KV* K, const V* x, V* y) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int lr = warp; lr < nrow; lr += nw) {
+        const int row = row0 + lr;
+        const int g = fmap[row];
+        if (g < 0) continue;  // the fixed independent node (warp-uniform)
+        const int ir = g - q0;
+        const int a = row / 3, k = row - 3 * a;
+        const int m = nup[a];
+        const long long start = rs[a] + (k == 0 ? 0LL : (k == 1 ? 3LL + 3LL * m : 5LL + 6LL * m));
+        const int len = (3 - k) + 3 * m;
+        const V xr = x[ir];
+        V acc = 0;
+        for (int p = lane; p < len; p += 32) {
+            const int c = rcol[start + p];
+            if (c < 0) continue;
+            const V v = (V)K[start + p];
+            acc += v * x[c];
+            if (c != ir) atomicAdd(y + c, v * xr);
+        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) atomicAdd(y + ir, acc);
+    }
+}
+
+__device__ __forceinline__ void apply_block(const float* Mb, const float r[3], float z[3]) {
+    z[0] = Mb[0] * r[0] + Mb[1] * r[1] + Mb[2] * r[2];
+    z[1] = Mb[3] * r[0] + Mb[4] * r[1] + Mb[5] * r[2];
+    z[2] = Mb[6] * r[0] + Mb[7] * r[1] + Mb[8] * r[2];
+}
+
+__global__ void __launch_bounds__(kSolveThreads) fe2_minres_kernel(SolveArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double red_d[32];
+    __shared__ float red_f[32];
+    __shared__ int rve_s;
+    const int tid = threadIdx.x, bs = blockDim.x;
+    for (;;) {
+        if (tid == 0) {
+            const int t = atomicAdd(A.queue, 1);
+            rve_s = t < A.n_rve ? A.order[t] : -1;
+        }
+        __syncthreads();
+        const int rve = rve_s;
+        __syncthreads();
+        if (rve < 0) return;
+        const int na0 = A.node_off[rve], na1 = A.node_off[rve + 1];
+        const int nf = 3 * (na1 - na0), dof0 = 3 * na0;
+        const int q0 = A.red_off[rve], m = A.red_off[rve + 1] - q0, nb3 = m / 3;
+        if (!A.active[rve]) continue;  // x of RVEs not solving is left as it is
+        const float* Mr = A.minv + 3 * (size_t)q0;  // block of independent node j at Mr + 9 j
+        // shared views: FP32 inner phase [xs][bufA][bufB][bufC][v][wa][wb] (m each);
+        // FP64 refinement phase [xd][yd] (m each) over the same bytes
+        float* xs = reinterpret_cast<float*>(smem);
+        float* bufA = xs + m;
+        float* bufB = bufA + m;
+        float* bufC = bufB + m;
+        float* v = bufC + m;
+        float* wa = v + m;
+        float* wb = wa + m;
+        double* xd = reinterpret_cast<double*>(smem);
+        double* yd = xd + m;
+        for (int rh = 0; rh < A.nrhs; ++rh) {
+            const double* b = A.rhs + (size_t)rh * A.n_red + q0;
+            double* x = A.x + (size_t)rh * A.n_red + q0;
+            double* r64 = A.r64 + q0;
+            double bb = 0.0;
+            for (int i = tid; i < m; i += bs) { x[i] = 0.0; r64[i] = b[i]; bb += b[i] * b[i]; }
+            const double nb = sqrt(block_sum_d(bb, red_d));
+            int total_it = 0;
+            double rel = nb > 0.0 ? 1.0 : 0.0;
+            const double eta = A.eta[rve];
+            for (int outer = 0; outer < A.max_outer && nb > 0.0 && rel > eta; ++outer) {
+                // ---- inner FP32 MINRES on the current FP64 residual scaled to unit norm ----
+                double rr = 0.0;
+                for (int i = tid; i < m; i += bs) rr += r64[i] * r64[i];
+                const double nr = sqrt(block_sum_d(rr, red_d));
+                const double sc = 1.0 / nr;
+                // this cycle aims a little below the target, but no lower than FP32 can reach
+                const float cyc_tol = (float)fmax(0.5 * eta * nb / nr, A.inner_floor);
+                float* r1 = bufA;
+                float* r2 = bufB;
+                float* y = bufC;
+                float b1 = 0.f;
+                for (int j = tid; j < nb3; j += bs) {
+                    float rv[3], z[3];
+                    for (int c = 0; c < 3; ++c) rv[c] = (float)(r64[3 * j + c] * sc);
+                    apply_block(Mr + 9 * (size_t)j, rv, z);
+                    for (int c = 0; c < 3; ++c) {
+                        r1[3 * j + c] = rv[c];
+                        r2[3 * j + c] = rv[c];
+                        y[3 * j + c] = z[c];
+                        xs[3 * j + c] = 0.f;
+                        wa[3 * j + c] = 0.f;
+                        wb[3 * j + c] = 0.f;
+                    }
+                    b1 += rv[0] * z[0] + rv[1] * z[1] + rv[2] * z[2];
+                }
+                b1 = block_sum_f(b1, red_f);
+                const float beta1 = b1 > 0.f ? sqrtf(b1) : 0.f;
+                float beta = beta1, oldb = 0.f, dbar = 0.f, epsln = 0.f, phibar = beta1, cs = -1.f, sn = 0.f;
+                int it = 0;
+                while (it < A.max_inner && beta > 0.f) {
+                    // v = y / beta;  y = K_red v - (beta/oldb) r1
+                    const float s = 1.f / beta;
+                    for (int i = tid; i < m; i += bs) { v[i] = s * y[i]; y[i] = 0.f; }
+                    __syncthreads();
+                    rve_spmv_red<float, float>(dof0, nf, q0, A.fmap, A.rs, A.nup, A.rcol, A.Kf, v, y);
+                    __syncthreads();
+                    const float f1 = it > 0 ? beta / oldb : 0.f;
+                    float al = 0.f;
+                    for (int i = tid; i < m; i += bs) {
+                        const float yi = y[i] - f1 * r1[i];
+                        y[i] = yi;
+                        al += v[i] * yi;
+                    }
+                    const float alfa = block_sum_f(al, red_f);
+                    // y -= (alfa/beta) r2;  z = M y into r1's buffer;  beta = sqrt(y . z)
+                    const float f2 = alfa / beta;
+                    float bt = 0.f;
+                    for (int j = tid; j < nb3; j += bs) {
+                        float yv[3], z[3];
+                        for (int c = 0; c < 3; ++c) {
+                            yv[c] = y[3 * j + c] - f2 * r2[3 * j + c];
+                            y[3 * j + c] = yv[c];
+                        }
+                        apply_block(Mr + 9 * (size_t)j, yv, z);
+                        for (int c = 0; c < 3; ++c) r1[3 * j + c] = z[c];
+                        bt += yv[0] * z[0] + yv[1] * z[1] + yv[2] * z[2];
+                    }
+                    bt = block_sum_f(bt, red_f);
+                    {  // rotate: r1 <- r2, r2 <- y, y <- z
+                        float* t = r1;
+                        r1 = r2;
+                        r2 = y;
+                        y = t;
+                    }
+                    oldb = beta;
+                    beta = bt > 0.f ? sqrtf(bt) : 0.f;
+                    // Givens rotation of the tridiagonal Lanczos matrix
+                    const float oldeps = epsln;
+                    const float delta = cs * dbar + sn * alfa;
+                    const float gbar = sn * dbar - cs * alfa;
+                    epsln = sn * beta;
+                    dbar = -cs * beta;
+                    const float gamma = fmaxf(sqrtf(gbar * gbar + beta * beta), 1e-30f);
+                    cs = gbar / gamma;
+                    sn = beta / gamma;
+                    const float phi = cs * phibar;
+                    phibar *= sn;
+                    const float dn = 1.f / gamma;
+                    for (int i = tid; i < m; i += bs) {
+                        const float t = wa[i];
+                        const float wn = (v[i] - oldeps * wb[i] - delta * t) * dn;
+                        wb[i] = t;
+                        wa[i] = wn;
+                        xs[i] += phi * wn;
+                    }
+                    ++it;
+                    if (phibar < cyc_tol * beta1) break;
+                }
+                total_it += it;
+                // ---- FP64 refinement: x += nr * xs; r64 = b - K_red x ----
+                __syncthreads();
+                for (int i = tid; i < m; i += bs) x[i] += nr * (double)xs[i];
+                __syncthreads();
+                for (int i = tid; i < m; i += bs) { xd[i] = x[i]; yd[i] = 0.0; }
+                __syncthreads();
+                rve_spmv_red<double, double>(dof0, nf, q0, A.fmap, A.rs, A.nup, A.rcol, A.K, xd, yd);
+                __syncthreads();
+                double rs2 = 0.0;
+                for (int i = tid; i < m; i += bs) {
+                    const double ri = b[i] - yd[i];
+                    r64[i] = ri;
+                    rs2 += ri * ri;
+                }
+                rel = sqrt(block_sum_d(rs2, red_d)) / nb;
+            }
+            if (tid == 0) {
+                A.iters[rve] = total_it;
+                A.rnorm[rve] = rel;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Homogenized first Piola stress and the Z^T K Z term, one CTA per RVE.
+//   Pbar_iJ = (1/V0) sum_a f_{a,i} X_{a,J};  (Z^T K Z)_{iJ,kL} = sum_a X_{a,J} (K z_kL)_{a,i}
+__global__ void homogenize_kernel(int n_rve, const int* node_off, const double* X, const double* f, double* P,
+                                  double V0) {
+    __shared__ double red[32];
+    const int rve = blockIdx.x;
+    if (rve >= n_rve) return;
+    const int a0 = node_off[rve], a1 = node_off[rve + 1];
+    for (int c = 0; c < 9; ++c) {
+        const int i = c / 3, J = c % 3;
+        double s = 0.0;
+        for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) s += f[3 * a + i] * X[3 * a + J];
+        s = block_sum_d(s, red);
+        if (threadIdx.x == 0) P[9 * rve + c] = s / V0;
+    }
+}
+
+// Affine mode z_kL (u_{a,k} = X_{a,L}) of every RVE into u; y = K_sym u computed by a plain
+// upper-CSR SpMV with FP64 atomics.
+__global__ void affine_mode_kernel(int n_nodes, const double* X, int kL, double* u) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * n_nodes) return;
+    const int a = i / 3, d = i - 3 * a, k = kL / 3, L = kL % 3;
+    u[i] = d == k ? X[3 * a + L] : 0.0;
+}
+__global__ void spmv_upper_kernel(int n_dof, const long long* rs, const int* nup, const int* col, const double* K,
+                                  const double* x, double* y) {
+    const int lane = threadIdx.x & 31;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (row >= n_dof) return;
+    const int a = row / 3, k = row - 3 * a;
+    const int m = nup[a];
+    const long long start = rs[a] + (k == 0 ? 0LL : (k == 1 ? 3LL + 3LL * m : 5LL + 6LL * m));
+    const int len = (3 - k) + 3 * m;
+    const double xr = x[row];
+    double acc = 0.0;
+    for (int p = lane; p < len; p += 32) {
+        const int c = col[start + p];
+        const double v = K[start + p];
+        acc += v * x[c];
+        if (c != row) atomicAdd(y + c, v * xr);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) atomicAdd(y + row, acc);
+}
+// ZKZ_{iJ,kL} += sum_a X_{a,J} y_{a,i}
+__global__ void zkz_kernel(int n_rve, const int* node_off, const double* X, const double* y, int kL, double* Z,
+                           double V0) {
+    __shared__ double red[32];
+    const int rve = blockIdx.x;
+    const int a0 = node_off[rve], a1 = node_off[rve + 1];
+    for (int c = 0; c < 9; ++c) {
+        const int i = c / 3, J = c % 3;
+        double s = 0.0;
+        for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) s += y[3 * a + i] * X[3 * a + J];
+        s = block_sum_d(s, red);
+        if (threadIdx.x == 0) Z[81 * rve + 9 * c + kL] = s / V0;
+    }
+}
+// A_{iJ,kL} = ZKZ - (1/V0) sum_q M_iJ[q] X_kL[q] per RVE
+__global__ void condense_kernel(int n_rve, const int* red_off, int n_red, const double* M, const double* Xs,
+                                const double* Z, double* A, double V0) {
+    __shared__ double red[32];
+    const int rve = blockIdx.x;
+    const int q0 = red_off[rve], q1 = red_off[rve + 1];
+    for (int c = 0; c < 81; ++c) {
+        const int u = c / 9, v = c % 9;
+        double s = 0.0;
+        for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) s += M[(size_t)u * n_red + q] * Xs[(size_t)v * n_red + q];
+        s = block_sum_d(s, red);
+        if (threadIdx.x == 0) A[81 * rve + c] = Z[81 * rve + c] - s / V0;
+    }
+}
+
+// shared memory of the solver: 7 FP32 vectors (or 2 FP64 vectors) of the largest reduced size
+size_t solve_smem_bytes(int max_m) { return std::max(sizeof(float) * 7, sizeof(double) * 2) * (size_t)max_m; }
+
+// Solve T^T K T x = rhs for the RVEs flagged in d_active, each to its relative tolerance d_eta.
+int run_solver(Fe2* f, int nrhs, const double* rhs, double* x, int max_inner, int max_outer) {
+    Handle* h = f->loop;
+    int max_m = 0;
+    for (int r = 0; r < f->n_rve; ++r) max_m = std::max(max_m, f->red_off[r + 1] - f->red_off[r]);
+    const size_t smem = solve_smem_bytes(max_m);
+    CKF(cudaFuncSetAttribute(fe2_minres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, f->device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fe2_minres_kernel, kSolveThreads, smem);
+    SolveArgs a;
+    a.n_rve = f->n_rve;
+    a.max_inner = max_inner;
+    a.max_outer = max_outer;
+    a.inner_floor = 1e-4;
+    a.eta = f->d_eta;
+    a.order = f->d_order;
+    a.queue = f->d_queue;
+    a.active = f->d_active;
+    a.node_off = f->d_node_off;
+    a.red_off = f->d_red_off;
+    a.fmap = f->d_fmap;
+    a.rs = h->d_rs;
+    a.nup = h->d_nup;
+    a.rcol = f->d_rcol;
+    a.K = h->d_kval;
+    a.Kf = f->d_kf;
+    a.minv = f->d_minv;
+    a.nrhs = nrhs;
+    a.rhs = rhs;
+    a.x = x;
+    a.r64 = f->d_r64;
+    a.iters = f->d_cg_iters;
+    a.rnorm = f->d_rnorm;
+    a.n_red = f->n_red;
+    CKF(cudaMemsetAsync(f->d_queue, 0, sizeof(int), h->stream));
+    const int grid = std::max(1, std::min(f->n_rve, sms * std::max(per_sm, 1)));
+    fe2_minres_kernel<<<grid, kSolveThreads, smem, h->stream>>>(a);
+    CKF(cudaGetLastError());
+    return 0;
+}
+
+// Newton iteration pieces: u, element loop (f_int, K), rhs = -T^T f_int, block-Jacobi inverse.
+int assemble(Fe2* f) {
+    Handle* h = f->loop;
+    const int nd = 3 * f->n_nodes;
+    expand_u_kernel<<<(nd + 255) / 256, 256, 0, h->stream>>>(f->n_nodes, h->d_X, f->d_rve_of_node, f->d_Fbar,
+                                                              f->d_fmap, f->d_w, f->d_u);
+    CKF(cudaGetLastError());
+    int rc = ceos::evaluate_device(h, 0.0, f->d_u, h->d_fint, h->d_kval, h->stream);
+    if (rc) return rc;
+    CKF(cudaMemsetAsync(f->d_rhs, 0, sizeof(double) * f->n_red, h->stream));
+    fold_kernel<<<(nd + 255) / 256, 256, 0, h->stream>>>(nd, f->d_fmap, h->d_fint, f->d_rhs, -1.0);
+    CKF(cudaGetLastError());
+    const int n_blk = f->n_red / 3;
+    double* acc = f->d_y64;  // FP64 block accumulator: 9 n_red/3 doubles (d_y64 holds max(3 n_nodes, 3 n_red))
+    CKF(cudaMemsetAsync(acc, 0, sizeof(double) * 9 * (size_t)n_blk, h->stream));
+    diag_blocks_kernel<<<(f->n_nodes + 255) / 256, 256, 0, h->stream>>>(f->n_nodes, h->d_rs, h->d_nup, h->d_kval,
+                                                                        f->d_fmap, acc);
+    CKF(cudaGetLastError());
+    invert_blocks_kernel<<<(n_blk + 255) / 256, 256, 0, h->stream>>>(n_blk, acc, f->d_minv);
+    CKF(cudaGetLastError());
+    to_f32_kernel<<<(unsigned)((f->nnz + 255) / 256), 256, 0, h->stream>>>(f->nnz, h->d_kval, f->d_kf);
+    CKF(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace
+
+// -------------------------------------------------------------------------------------------------
+extern "C" int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, double mu_matrix, double stiff_ratio,
+                               double k_over_mu, int device, void** handle) {
+    if (n_rve < 1 || !n_cells || !vf || !handle) return CEOS_E_ARG;
+    Fe2* f = new Fe2();
+    *handle = nullptr;
+    f->n_rve = n_rve;
+    f->device = device;
+    // round-off level of the nodal forces of a unit RVE with the stiffer phase
+    f->force_floor = 1e-11 * mu_matrix * std::max(1.0, stiff_ratio);
+    f->n.assign(n_cells, n_cells + n_rve);
+    f->vf_nominal.assign(vf, vf + n_rve);
+    // ---- union mesh: RVE r = unit cube, n^3 cells; fibre along z through the centre ----
+    std::vector<double> X;
+    std::vector<int> conn, mat_id, fmap_host;
+    f->node_off.assign(n_rve + 1, 0);
+    f->red_off.assign(n_rve + 1, 0);
+    f->nodes_of.assign(n_rve, 0);
+    f->vf_actual.assign(n_rve, 0.0);
+    for (int r = 0; r < n_rve; ++r) {
+        const int n = f->n[r];
+        // the solver keeps 7 FP32 vectors of 3(n^3-1) entries in shared memory: n <= 14 fits
+        // the 227 KB a CTA can hold
+        if (n < 2 || n > kMaxCells) { delete f; return CEOS_E_ARG; }
+        const int m = n + 1;
+        const int base = f->node_off[r];
+        f->nodes_of[r] = m * m * m;
+        f->node_off[r + 1] = base + m * m * m;
+        f->red_off[r + 1] = f->red_off[r] + 3 * (n * n * n - 1);
+        for (int k = 0; k < m; ++k)
+            for (int j = 0; j < m; ++j)
+                for (int i = 0; i < m; ++i) {
+                    X.push_back((double)i / n);
+                    X.push_back((double)j / n);
+                    X.push_back((double)k / n);
+                    const int ind = (k % n) * n * n + (j % n) * n + (i % n);  // independent node
+                    for (int d = 0; d < 3; ++d) fmap_host.push_back(ind == 0 ? -1 : f->red_off[r] + 3 * (ind - 1) + d);
+                }
+        const double rad2 = vf[r] / M_PI;
+        int nfib = 0;
+        for (int k = 0; k < n; ++k)
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                    auto id = [&](int a, int b, int c) { return base + (c * m + b) * m + a + 1; };
+                    const int e[8] = {id(i, j, k), id(i + 1, j, k), id(i + 1, j + 1, k), id(i, j + 1, k),
+                                      id(i, j, k + 1), id(i + 1, j, k + 1), id(i + 1, j + 1, k + 1), id(i, j + 1, k + 1)};
+                    conn.insert(conn.end(), e, e + 8);
+                    const double xc = (i + 0.5) / n - 0.5, yc = (j + 0.5) / n - 0.5;
+                    const int fib = (xc * xc + yc * yc < rad2) ? 1 : 0;
+                    mat_id.push_back(fib);
+                    nfib += fib;
+                }
+        f->vf_actual[r] = (double)nfib / (n * n * n);
+    }
+    f->n_nodes = f->node_off[n_rve];
+    f->n_red = f->red_off[n_rve];
+    // ---- element loop: compressible Neo-Hookean phases (ModCompressibleNeoHookean.f90) ----
+    const double mu_m = mu_matrix, mu_f = mu_matrix * stiff_ratio;
+    const double pm[2] = {mu_m, k_over_mu * mu_m - 2.0 * mu_m / 3.0};
+    const double pf[2] = {mu_f, k_over_mu * mu_f - 2.0 * mu_f / 3.0};
+    ceos_material mats[2] = {{CEOS_CNH, 0, 2, pm}, {CEOS_CNH, 0, 2, pf}};
+    ceos_mesh mesh{f->n_nodes, (int)(conn.size() / 8), X.data(), conn.data(), mat_id.data()};
+    void* lh = nullptr;
+    int rc = ceos_create(&mesh, mats, 2, CEOS_FP64, device, &lh);
+    if (rc) { delete f; return rc; }
+    f->loop = static_cast<Handle*>(lh);
+    f->nnz = f->loop->nnz;
+    // ---- device arrays ----
+    std::vector<int> rve_of_node(f->n_nodes), rve_of_elem;
+    for (int r = 0; r < n_rve; ++r) {
+        for (int a = f->node_off[r]; a < f->node_off[r + 1]; ++a) rve_of_node[a] = r;
+        rve_of_elem.insert(rve_of_elem.end(), (size_t)f->n[r] * f->n[r] * f->n[r], r);
+    }
+    std::vector<int> col(f->nnz), rowmap(3 * f->n_nodes + 1);
+    ceos_pattern(f->loop, nullptr, nullptr, rowmap.data(), col.data(), nullptr);
+    for (auto& c : col) c -= 1;
+    std::vector<int> rcol(f->nnz);
+    for (long long p = 0; p < f->nnz; ++p) {
+        const int g = fmap_host[col[p]];
+        rcol[p] = g < 0 ? -1 : g - f->red_off[rve_of_node[col[p] / 3]];
+    }
+    std::vector<int> order(n_rve);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return f->n[a] > f->n[b]; });
+    std::vector<int> ncell(f->n), ones(n_rve, 1);
+    const size_t nd = 3 * (size_t)f->n_nodes;
+    auto up = [&](void** dst, const void* src, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(dst, bytes);
+        if (e == cudaSuccess && src) e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+        return e;
+    };
+    cudaSetDevice(device);
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = up((void**)&f->d_node_off, f->node_off.data(), sizeof(int) * (n_rve + 1));
+    if (e == cudaSuccess) e = up((void**)&f->d_red_off, f->red_off.data(), sizeof(int) * (n_rve + 1));
+    if (e == cudaSuccess) e = up((void**)&f->d_ncell, ncell.data(), sizeof(int) * n_rve);
+    if (e == cudaSuccess) e = up((void**)&f->d_rve_of_node, rve_of_node.data(), sizeof(int) * f->n_nodes);
+    if (e == cudaSuccess) e = up((void**)&f->d_fmap, fmap_host.data(), sizeof(int) * nd);
+    if (e == cudaSuccess) e = up((void**)&f->d_col, col.data(), sizeof(int) * f->nnz);
+    if (e == cudaSuccess) e = up((void**)&f->d_rcol, rcol.data(), sizeof(int) * f->nnz);
+    if (e == cudaSuccess) e = up((void**)&f->d_kf, nullptr, sizeof(float) * f->nnz);
+    if (e == cudaSuccess) e = up((void**)&f->d_order, order.data(), sizeof(int) * n_rve);
+    if (e == cudaSuccess) e = up((void**)&f->d_queue, nullptr, sizeof(int));
+    if (e == cudaSuccess) e = up((void**)&f->d_Fbar, nullptr, sizeof(double) * 9 * n_rve);
+    if (e == cudaSuccess) e = up((void**)&f->d_w, nullptr, sizeof(double) * f->n_red);
+    if (e == cudaSuccess) e = up((void**)&f->d_u, nullptr, sizeof(double) * nd);
+    if (e == cudaSuccess) e = up((void**)&f->d_rhs, nullptr, sizeof(double) * f->n_red);
+    if (e == cudaSuccess) e = up((void**)&f->d_dx, nullptr, sizeof(double) * f->n_red);
+    if (e == cudaSuccess) e = up((void**)&f->d_r64, nullptr, sizeof(double) * f->n_red);
+    if (e == cudaSuccess) e = up((void**)&f->d_y64, nullptr, sizeof(double) * std::max(nd, (size_t)3 * f->n_red));
+    if (e == cudaSuccess) e = up((void**)&f->d_minv, nullptr, sizeof(float) * 9 * (size_t)(f->n_red / 3 + 1));
+    if (e == cudaSuccess) e = up((void**)&f->d_rnorm, nullptr, sizeof(double) * n_rve);
+    if (e == cudaSuccess) e = up((void**)&f->d_cg_iters, nullptr, sizeof(int) * n_rve);
+    if (e == cudaSuccess) e = up((void**)&f->d_active, ones.data(), sizeof(int) * n_rve);
+    if (e == cudaSuccess) e = up((void**)&f->d_P, nullptr, sizeof(double) * 9 * n_rve);
+    if (e == cudaSuccess) e = up((void**)&f->d_nn, nullptr, sizeof(double) * n_rve);
+    if (e == cudaSuccess) e = up((void**)&f->d_rve_of_elem, rve_of_elem.data(), sizeof(int) * rve_of_elem.size());
+    if (e == cudaSuccess) e = up((void**)&f->d_fail, nullptr, sizeof(int) * n_rve);
+    if (e == cudaSuccess) e = up((void**)&f->d_op, nullptr, sizeof(int) * n_rve);
+    if (e == cudaSuccess) e = up((void**)&f->d_wc, nullptr, sizeof(double) * f->n_red);
+    if (e == cudaSuccess) e = up((void**)&f->d_eta, nullptr, sizeof(double) * n_rve);
+    if (e != cudaSuccess) { delete f; return CEOS_E_CUDA; }
+    *handle = f;
+    return 0;
+}
+
+extern "C" int ceos_fe2_info(void* handle, int* n_nodes, int* n_elem, int* n_red, double* vf_actual) {
+    Fe2* f = static_cast<Fe2*>(handle);
+    if (!f) return CEOS_E_ARG;
+    if (n_nodes) *n_nodes = f->n_nodes;
+    if (n_elem) *n_elem = f->loop->n_elem;
+    if (n_red) *n_red = f->n_red;
+    if (vf_actual) std::copy(f->vf_actual.begin(), f->vf_actual.end(), vf_actual);
+    return 0;
+}
+
+extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int max_newton, double* P, double* A,
+                              int* newton_iters, int* cg_iters) {
+    Fe2* f = static_cast<Fe2*>(handle);
+    if (!f || !Fbar || !P || max_newton < 1 || !(tol > 0.0)) return CEOS_E_ARG;
+    Handle* h = f->loop;
+    cudaStream_t s = h->stream;
+    const int nr = f->n_rve;
+    CKF(cudaSetDevice(f->device));
+    CKF(cudaMemsetAsync(f->d_w, 0, sizeof(double) * f->n_red, s));
+    CKF(cudaMemsetAsync(f->d_wc, 0, sizeof(double) * f->n_red, s));
+    CKF(cudaMemsetAsync(f->d_dx, 0, sizeof(double) * f->n_red, s));
+    const bool verbose = std::getenv("CEOS_FE2_VERBOSE") != nullptr;
+    // Per-RVE load continuation Fbar(a) = I + a (Fbar - I): each RVE advances from its last
+    // converged level a_done towards 1 in steps da (1/n_sub at first).  A Newton step is accepted
+    // when no element folds and the residual grows by at most kGrowth; otherwise it is halved
+    // (backtracking line search) up to kMaxHalvings times.  A load step that still fails, or does
+    // not converge in max_newton iterations, is cut back: the RVE returns to its converged
+    // fluctuations and da shrinks by the golden ratio, as the reference's quasi-static driver
+    // cuts back its load steps (ModFEMAnalysis.f90:1136-1374).
+    constexpr int kMaxHalvings = 6, kMaxCutbacks = 16;
+    constexpr double kGrowth = 1.5;
+    const double golden = 0.6180339887498949;
+    enum { kNewton = 0, kDone = 1 };
+    std::vector<int> phase(nr, kNewton), nit(nr, 0), halv(nr, 0), cuts(nr, 0), its(nr, 0), cg_tot(nr, 0);
+    std::vector<int> op(nr), need(nr), fail(nr), cgi(nr);
+    std::vector<double> a_done(nr, 0.0), da(nr, 1.0 / std::max(1, f->n_sub)), a_try(nr), r0(nr, 1.0), racc(nr, 0.0),
+        rn(nr), eta(nr, 1.0), Fs(9 * (size_t)nr);
+    for (int r = 0; r < nr; ++r) a_try[r] = std::min(1.0, da[r]);
+    const int max_rounds = (max_newton + kMaxHalvings + 2) * (kMaxCutbacks + 2 * std::max(1, f->n_sub) + 2);
+    bool all_done = false;
+    for (int round = 0; round < max_rounds && !all_done; ++round) {
+        for (int r = 0; r < nr; ++r)
+            for (int k = 0; k < 9; ++k) {
+                const double I = (k % 4 == 0) ? 1.0 : 0.0;
+                Fs[9 * (size_t)r + k] = I + a_try[r] * (Fbar[9 * (size_t)r + k] - I);
+            }
+        CKF(cudaMemcpyAsync(f->d_Fbar, Fs.data(), sizeof(double) * Fs.size(), cudaMemcpyHostToDevice, s));
+        int rc = assemble(f);
+        if (rc) return rc;
+        const int st = ceos_status(h, nullptr);
+        if (st < 0) return st;
+        std::fill(fail.begin(), fail.end(), 0);
+        if (st) {
+            CKF(cudaMemsetAsync(f->d_fail, 0, sizeof(int) * nr, s));
+            rve_fail_kernel<<<(h->n_elem + 255) / 256, 256, 0, s>>>(h->n_elem, h->d_elem_status, f->d_rve_of_elem,
+                                                                    f->d_fail);
+            CKF(cudaGetLastError());
+            CKF(cudaMemcpyAsync(fail.data(), f->d_fail, sizeof(int) * nr, cudaMemcpyDeviceToHost, s));
+        }
+        rve_norm_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_rhs, f->d_nn);
+        CKF(cudaGetLastError());
+        CKF(cudaMemcpyAsync(rn.data(), f->d_nn, sizeof(double) * nr, cudaMemcpyDeviceToHost, s));
+        CKF(cudaStreamSynchronize(s));
+        all_done = true;
+        int n_need = 0, n_rej = 0, n_cut = 0;
+        double worst = 0.0;
+        for (int r = 0; r < nr; ++r) {
+            op[r] = kOpNone;
+            need[r] = 0;
+            if (phase[r] == kDone) continue;
+            all_done = false;
+            const bool ok = !fail[r] && std::isfinite(rn[r]);
+            bool cut = false, accepted = false;
+            if (nit[r] == 0) {  // start of a load step from the converged fluctuations
+                if (!ok) cut = true;
+                else { r0[r] = std::max(rn[r], 1e-300); accepted = true; }
+            } else if (ok && rn[r] <= kGrowth * racc[r]) {
+                accepted = true;
+            } else if (halv[r] >= kMaxHalvings) {
+                cut = true;
+            } else {
+                op[r] = kOpBacktrack;
+                ++halv[r];
+                ++n_rej;
+            }
+            if (accepted) {
+                racc[r] = rn[r];
+                halv[r] = 0;
+                if (rn[r] <= tol * r0[r] || rn[r] <= f->force_floor) {
+                    a_done[r] = a_try[r];
+                    op[r] = kOpSave;
+                    nit[r] = 0;
+                    if (a_done[r] >= 1.0) {
+                        phase[r] = kDone;
+                    } else {
+                        da[r] = std::min(2.0 * da[r], 1.0 - a_done[r]);  // grow after a converged step
+                        a_try[r] = 1.0 - (a_done[r] + da[r]) < 1e-12 ? 1.0 : a_done[r] + da[r];
+                    }
+                } else if (nit[r] >= max_newton) {
+                    cut = true;
+                } else {
+                    // Eisenstat-Walker forcing: quadratic convergence without over-solving
+                    const double rel = rn[r] / r0[r];
+                    eta[r] = std::min(1e-2, std::max(rel, 0.1 * tol / rel));
+                    need[r] = 1;
+                    ++nit[r];
+                    ++its[r];
+                    ++n_need;
+                    worst = std::max(worst, rel);
+                }
+            }
+            if (cut) {
+                if (++cuts[r] > kMaxCutbacks) {
+                    f->msg = "RVE " + std::to_string(r) + ": no convergence after " + std::to_string(kMaxCutbacks) +
+                             " load cut-backs (converged load level " + std::to_string(a_done[r]) + ")";
+                    return st ? st : 1;
+                }
+                op[r] = kOpRestore;
+                da[r] *= golden;
+                a_try[r] = a_done[r] + da[r];
+                nit[r] = 0;
+                halv[r] = 0;
+                ++n_cut;
+            }
+        }
+        if (verbose)
+            std::fprintf(stderr, "fe2: round %d solving %d max rel residual %.3e rejected %d cut back %d\n", round,
+                         n_need, worst, n_rej, n_cut);
+        if (all_done) break;
+        CKF(cudaMemcpyAsync(f->d_op, op.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+        rve_op_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_op, f->d_w, f->d_dx, f->d_wc);
+        CKF(cudaGetLastError());
+        if (n_need) {
+            CKF(cudaMemcpyAsync(f->d_active, need.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+            CKF(cudaMemcpyAsync(f->d_eta, eta.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, s));
+            rc = run_solver(f, 1, f->d_rhs, f->d_dx, 2000, 3);  // an inexact step is still a descent try
+            if (rc) return rc;
+            CKF(cudaMemcpyAsync(cgi.data(), f->d_cg_iters, sizeof(int) * nr, cudaMemcpyDeviceToHost, s));
+            rve_step_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_active, f->d_dx, f->d_w);
+            CKF(cudaGetLastError());
+            CKF(cudaStreamSynchronize(s));
+            for (int r = 0; r < nr; ++r)
+                if (need[r]) cg_tot[r] += cgi[r];
+        }
+    }
+    if (!all_done) {
+        f->msg = "load continuation did not finish";
+        return 1;
+    }
+    // converged state: K and f_int of the last assembly
+    homogenize_kernel<<<f->n_rve, 256, 0, s>>>(f->n_rve, f->d_node_off, h->d_X, h->d_fint, f->d_P, 1.0);
+    CKF(cudaGetLastError());
+    CKF(cudaMemcpyAsync(P, f->d_P, sizeof(double) * 9 * f->n_rve, cudaMemcpyDeviceToHost, s));
+    if (A) {
+        // static condensation with the 9 affine modes
+        const size_t nd = 3 * (size_t)f->n_nodes;
+        if (!f->d_Z) {
+            CKF(cudaMalloc(&f->d_A, sizeof(double) * 81 * f->n_rve));
+            CKF(cudaMalloc(&f->d_Z, sizeof(double) * 81 * f->n_rve));
+            CKF(cudaMalloc(&f->d_M, sizeof(double) * 9 * (size_t)f->n_red));
+            CKF(cudaMalloc(&f->d_X9, sizeof(double) * 9 * (size_t)f->n_red));
+        }
+        for (int kL = 0; kL < 9; ++kL) {
+            affine_mode_kernel<<<(int)((nd + 255) / 256), 256, 0, s>>>(f->n_nodes, h->d_X, kL, f->d_u);
+            CKF(cudaMemsetAsync(f->d_y64, 0, sizeof(double) * nd, s));
+            spmv_upper_kernel<<<(int)((nd * 32 + 255) / 256), 256, 0, s>>>((int)nd, h->d_rs, h->d_nup, f->d_col,
+                                                                         h->d_kval, f->d_u, f->d_y64);
+            zkz_kernel<<<f->n_rve, 256, 0, s>>>(f->n_rve, f->d_node_off, h->d_X, f->d_y64, kL, f->d_Z, 1.0);
+            CKF(cudaMemsetAsync(f->d_M + (size_t)kL * f->n_red, 0, sizeof(double) * f->n_red, s));
+            fold_kernel<<<(int)((nd + 255) / 256), 256, 0, s>>>((int)nd, f->d_fmap, f->d_y64, f->d_M + (size_t)kL * f->n_red,
+                                                               1.0);
+            CKF(cudaGetLastError());
+        }
+        std::vector<int> ones(f->n_rve, 1);
+        std::vector<double> eta_t(f->n_rve, 1e-8);
+        CKF(cudaMemcpyAsync(f->d_active, ones.data(), sizeof(int) * f->n_rve, cudaMemcpyHostToDevice, s));
+        CKF(cudaMemcpyAsync(f->d_eta, eta_t.data(), sizeof(double) * f->n_rve, cudaMemcpyHostToDevice, s));
+        int rc = run_solver(f, 9, f->d_M, f->d_X9, 4000, 8);
+        if (rc) return rc;
+        condense_kernel<<<f->n_rve, 256, 0, s>>>(f->n_rve, f->d_red_off, f->n_red, f->d_M, f->d_X9, f->d_Z, f->d_A, 1.0);
+        CKF(cudaGetLastError());
+        CKF(cudaMemcpyAsync(A, f->d_A, sizeof(double) * 81 * f->n_rve, cudaMemcpyDeviceToHost, s));
+    }
+    CKF(cudaStreamSynchronize(s));
+    if (newton_iters) std::copy(its.begin(), its.end(), newton_iters);
+    if (cg_iters) std::copy(cg_tot.begin(), cg_tot.end(), cg_iters);
+    return 0;
+}
+
+extern "C" int ceos_fe2_set_increments(void* handle, int n_sub) {
+    Fe2* f = static_cast<Fe2*>(handle);
+    if (!f || n_sub < 1) return CEOS_E_ARG;
+    f->n_sub = n_sub;
+    return 0;
+}
+
+extern "C" int ceos_fe2_message(void* handle, char* msg, int msg_len) {
+    Fe2* f = static_cast<Fe2*>(handle);
+    if (!f || !msg || msg_len < 1) return CEOS_E_ARG;
+    std::snprintf(msg, msg_len, "%s", f->msg.c_str());
+    return 0;
+}
+
+extern "C" void ceos_fe2_destroy(void* handle) { delete static_cast<Fe2*>(handle); }

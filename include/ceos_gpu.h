@@ -147,6 +147,30 @@ int ceos_cnh_assemble_noalloc(int n_nodes, int n_elem, const double* X_device, c
                               long long nnz, double mu, double lambda, double* fint_device,
                               double* kval_device, void* stream);
 
+/* ---- Batched FE^2 micro problems (no reference counterpart: CEOS solves one RVE at a time,
+ * MultiScale/ModMultiscaleAnalysis.f90:445-470) ------------------------------------------------
+ * n_rve periodic RVEs, RVE r a unit cube of n_cells[r]^3 Hexa8 cells with one cylindrical fibre
+ * along z of nominal volume fraction vf[r] (cells whose centroid lies strictly inside the fibre); both
+ * phases compressible Neo-Hookean (model 7), matrix shear modulus mu_matrix, fibre modulus
+ * stiff_ratio * mu_matrix, bulk modulus k_over_mu * mu in each phase. */
+int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, double mu_matrix, double stiff_ratio,
+                    double k_over_mu, int device, void** handle);
+/* Mesh sizes and the discretised fibre fraction of every RVE (any pointer may be NULL). */
+int ceos_fe2_info(void* handle, int* n_nodes, int* n_elem, int* n_red, double* vf_actual);
+/* Solve every RVE under its macro deformation gradient Fbar [n_rve][9] (row-major 3x3): Newton
+ * on the periodic fluctuations to ||T^T f_int|| <= tol * (its value at zero fluctuation), each
+ * linear system by block-Jacobi PCG (FP32) with FP64 refinement to 1e-8.  Outputs the homogenized
+ * first Piola stress P [n_rve][9] (row-major, the HomogenizeStress definition,
+ * ModMultiscaleAnalysis.f90:140-329) and, when A != NULL, the tangent dP/dFbar [n_rve][81]
+ * (row (iJ), column (kL), row-major pairs).  newton_iters / cg_iters [n_rve] may be NULL. */
+int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int max_newton, double* P, double* A,
+                   int* newton_iters, int* cg_iters);
+/* Apply Fbar in n_sub equal load increments per solve (default 1). */
+int ceos_fe2_set_increments(void* handle, int n_sub);
+/* Description of the last failure of ceos_fe2_solve (empty when none). */
+int ceos_fe2_message(void* handle, char* msg, int msg_len);
+void ceos_fe2_destroy(void* handle);
+
 /* ---- Host driver above the boundary (the Fortran host's role, restated in C++) ----------
  * Quasi-static analysis of one load case: QuasiStaticAnalysisFEM (ModFEMAnalysis.f90:1136-1374),
  * NewtonRaphsonFull_Solve (ModNewtonRaphsonFull.f90:44-168) and ApplyBoundaryConditionsNEW

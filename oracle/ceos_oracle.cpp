@@ -893,6 +893,48 @@ extern "C" int or_evaluate_sample(or_model* m, double time, const double* U, dou
     return status;
 }
 
+// HomogenizeStress (MultiScale/ModMultiscaleAnalysis.f90:140-329): Pbar = (1/V0) sum_e sum_gp
+// P w detJ_X with P = J sigma F^{-T} (StressTransformation Cauchy -> FirstPiola) of the Gauss-point
+// stresses of the last evaluation, F recomputed from U, V0 = sum of the element reference volumes.
+// P_out: row-major 3x3.
+extern "C" void or_homogenize(or_model* m, const double* U, double* P_out) {
+    double P[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    double V0 = 0.0;
+    ElemGeom g;
+    for (int e = 0; e < m->n_elem; ++e) {
+        gather(m, e, U, g);
+        for (int gp = 0; gp < 8; ++gp) {
+            double xi[3], w, dN[8][3], dNX[8][3];
+            hexa8_gp(gp, xi, &w);
+            hexa8_dN(xi, dN);
+            M3 JX, JXi;
+            jacobian(dN, g.Xe, JX);
+            const double detJX = det3(JX);
+            V0 += w * detJX;
+            inv3(JX, JXi);
+            global_derivs(JXi, dN, dNX);
+            M3 F, Fi, sg;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double s = 0.0;
+                    for (int n = 0; n < 8; ++n) s += dNX[n][j] * g.ue[3 * n + i];
+                    F[i][j] = s + (i == j ? 1.0 : 0.0);
+                }
+            inv3(F, Fi);
+            from_voigt(&m->sigma[((size_t)e * 8 + gp) * 6], sg);
+            const double J = det3(F);
+            for (int i = 0; i < 3; ++i)
+                for (int Jc = 0; Jc < 3; ++Jc) {
+                    double s = 0.0;
+                    for (int k = 0; k < 3; ++k) s += sg[i][k] * Fi[Jc][k];  // sigma F^{-T}
+                    P[i][Jc] += w * detJX * J * s;
+                }
+        }
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) P_out[3 * i + j] = P[i][j] / V0;
+}
+
 extern "C" void or_commit(or_model* m) {
     m->st_old = m->st_new;  // SwitchConvergedState (ModFEMAnalysis.f90:1349-1353)
 }

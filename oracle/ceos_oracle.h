@@ -83,6 +83,8 @@ int or_evaluate(or_model* m, double time, const double* U, double* fint, double*
 int or_evaluate_sample(or_model* m, double time, const double* U, double* fint, double* kval,
                        int n_eval, int threads);
 void or_commit(or_model* m);            /* SwitchConvergedState for every GP */
+/* HomogenizeStress (ModMultiscaleAnalysis.f90:140-329) of the last evaluation: P row-major 3x3. */
+void or_homogenize(or_model* m, const double* U, double* P_out);
 /* Gauss-point results of the last evaluation: sigma [n_elem*8*6], state [n_elem*8*nstate]. */
 void or_get_gp_stress(or_model* m, double* sigma);
 int  or_get_state(or_model* m, double* st, int which /*0 old, 1 new*/);

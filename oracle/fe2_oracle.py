@@ -1,0 +1,93 @@
+"""FP64 CPU oracle of one periodic RVE (TEST INFRASTRUCTURE ONLY).
+
+Restates the periodic micro problem the batched GPU solver handles: the reference's periodic
+multiscale model eliminates the slave DOFs with a matrix T and solves T^T K T du = -T^T R
+(FEM/Modules/ModMultiscalePeriodicFEMSoE.f90:77-182), then homogenizes the first Piola stress
+(HomogenizeStress, MultiScale/ModMultiscaleAnalysis.f90:140-329).  Here u = (Fbar - I) X + T w
+with w the periodic fluctuation of the independent nodes, one independent node held fixed, the
+element loop and HomogenizeStress taken from the C++ oracle and the reduced systems solved with
+scipy's sparse LU.  The tangent is checked by central finite differences of Pbar(Fbar).
+"""
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import oracle as O
+
+
+def rve_mesh(n, vf):
+    """Unit cube, n^3 cells, fibre along z through the centre (cells by centroid)."""
+    m = n + 1
+    k, j, i = np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij")
+    X = np.stack([i.ravel() / n, j.ravel() / n, k.ravel() / n], axis=1)
+    ke, je, ie = [a.ravel() for a in np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")]
+
+    def nid(a, b, c):
+        return (c * m + b) * m + a + 1
+
+    conn = np.stack([nid(ie, je, ke), nid(ie + 1, je, ke), nid(ie + 1, je + 1, ke), nid(ie, je + 1, ke),
+                     nid(ie, je, ke + 1), nid(ie + 1, je, ke + 1), nid(ie + 1, je + 1, ke + 1),
+                     nid(ie, je + 1, ke + 1)], axis=1).astype(np.int32)
+    xc, yc = (ie + 0.5) / n - 0.5, (je + 0.5) / n - 0.5
+    mat = (xc ** 2 + yc ** 2 < vf / np.pi).astype(np.int32)
+    ind = ((k % n) * n * n + (j % n) * n + (i % n)).ravel()
+    return X, conn, mat, ind
+
+
+class RVE:
+    def __init__(self, n, vf, mu_m=1.0, ratio=50.0, k_over_mu=100.0):
+        self.X, self.conn, self.mat, ind = rve_mesh(n, vf)
+        mu_f = ratio * mu_m
+        params = [[mu_m, k_over_mu * mu_m - 2 * mu_m / 3], [mu_f, k_over_mu * mu_f - 2 * mu_f / 3]]
+        self.model = O.Model(self.X, self.conn, [O.CNH, O.CNH], params, mat_id=self.mat)
+        self.rowmap, self.col = self.model.pattern()
+        nn = self.X.shape[0]
+        # T: full dof (3a+d) <- reduced dof 3(ind-1)+d, independent node 0 fixed
+        rows, cols = [], []
+        for a in range(nn):
+            if ind[a] == 0:
+                continue
+            for d in range(3):
+                rows.append(3 * a + d)
+                cols.append(3 * (ind[a] - 1) + d)
+        self.n_red = 3 * (n ** 3 - 1)
+        self.T = sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(3 * nn, self.n_red))
+        self.vf_actual = self.mat.mean()
+
+    def _K(self, kval):
+        n = 3 * self.X.shape[0]
+        r = np.repeat(np.arange(n), np.diff(self.rowmap))
+        c = self.col - 1
+        K = sp.csr_matrix((kval, (r, c)), shape=(n, n))
+        return (K + K.T - sp.diags(K.diagonal())).tocsr()
+
+    def solve(self, Fbar, tol=1e-10, itmax=25):
+        Fbar = np.asarray(Fbar, dtype=np.float64).reshape(3, 3)
+        w = np.zeros(self.n_red)
+        aff = (self.X @ (Fbar - np.eye(3)).T).reshape(-1)
+        r0 = None
+        for it in range(itmax):
+            U = aff + self.T @ w
+            fint, kval, rc, _ = self.model.evaluate(0.0, U)
+            assert rc == 0
+            R = self.T.T @ fint
+            nr = np.linalg.norm(R)
+            r0 = nr if r0 is None else r0
+            # relative to the first residual, with a floor at round-off of the internal forces
+            if nr <= tol * max(r0, 1e-300) or nr <= 1e-11 * np.linalg.norm(fint):
+                break
+            Kred = (self.T.T @ self._K(kval) @ self.T).tocsc()
+            w -= spla.spsolve(Kred, R)
+        self.U = U
+        self.iters = it
+        return self.model.homogenize(U)
+
+    def tangent_fd(self, Fbar, h=1e-6):
+        A = np.zeros((9, 9))
+        for kL in range(9):
+            dF = np.zeros(9)
+            dF[kL] = h
+            Pp = self.solve(np.asarray(Fbar).reshape(-1) + dF).reshape(-1)
+            Pm = self.solve(np.asarray(Fbar).reshape(-1) - dF).reshape(-1)
+            A[:, kL] = (Pp - Pm) / (2 * h)
+        return A

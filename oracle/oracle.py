@@ -52,6 +52,7 @@ def lib():
         L.or_evaluate_sample.restype = C.c_int
         L.or_evaluate_sample.argtypes = [P, C.c_double, dp, dp, P, C.c_int, C.c_int]
         L.or_commit.argtypes = [P]
+        L.or_homogenize.argtypes = [P, dp, dp]
         L.or_set_time_old.argtypes = [P, C.c_double]
         L.or_get_gp_stress.argtypes = [P, dp]
         L.or_get_state.restype = C.c_int
@@ -177,6 +178,11 @@ class Model:
 
     def commit(self):
         lib().or_commit(self._h)
+
+    def homogenize(self, U):
+        P = np.zeros(9)
+        lib().or_homogenize(self._h, _f64(U), P)
+        return P.reshape(3, 3)
 
     def set_time_old(self, t):
         lib().or_set_time_old(self._h, t)
