@@ -626,6 +626,18 @@ int assemble(Fe2* f) {
     return 0;
 }
 
+// Fibre area fraction of cell column (i, j) of an n^3 RVE: share of 16 x 16 sub-points of the
+// cell's cross-section strictly inside the fibre circle x^2 + y^2 < vf/pi about the RVE centre.
+double fibre_fraction(int n, int i, int j, double rad2) {
+    int inside = 0;
+    for (int b = 0; b < 16; ++b)
+        for (int a = 0; a < 16; ++a) {
+            const double x = (i + (a + 0.5) / 16.0) / n - 0.5, y = (j + (b + 0.5) / 16.0) / n - 0.5;
+            inside += (x * x + y * y < rad2) ? 1 : 0;
+        }
+    return inside / 256.0;
+}
+
 }  // namespace
 
 // -------------------------------------------------------------------------------------------------
@@ -642,7 +654,9 @@ extern "C" int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, 
     f->vf_nominal.assign(vf, vf + n_rve);
     // ---- union mesh: RVE r = unit cube, n^3 cells; fibre along z through the centre ----
     std::vector<double> X;
-    std::vector<int> conn, mat_id, fmap_host;
+    std::vector<int> conn, fmap_host;
+    std::vector<double> eparams;  // [n_elem][2] (Mu, Lambda) of each cell
+    const double mu_f = mu_matrix * stiff_ratio;
     f->node_off.assign(n_rve + 1, 0);
     f->red_off.assign(n_rve + 1, 0);
     f->nodes_of.assign(n_rve, 0);
@@ -667,7 +681,7 @@ extern "C" int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, 
                     for (int d = 0; d < 3; ++d) fmap_host.push_back(ind == 0 ? -1 : f->red_off[r] + 3 * (ind - 1) + d);
                 }
         const double rad2 = vf[r] / M_PI;
-        int nfib = 0;
+        double phisum = 0.0;
         for (int k = 0; k < n; ++k)
             for (int j = 0; j < n; ++j)
                 for (int i = 0; i < n; ++i) {
@@ -675,23 +689,22 @@ extern "C" int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, 
                     const int e[8] = {id(i, j, k), id(i + 1, j, k), id(i + 1, j + 1, k), id(i, j + 1, k),
                                       id(i, j, k + 1), id(i + 1, j, k + 1), id(i + 1, j + 1, k + 1), id(i, j + 1, k + 1)};
                     conn.insert(conn.end(), e, e + 8);
-                    const double xc = (i + 0.5) / n - 0.5, yc = (j + 0.5) / n - 0.5;
-                    const int fib = (xc * xc + yc * yc < rad2) ? 1 : 0;
-                    mat_id.push_back(fib);
-                    nfib += fib;
+                    const double phi = fibre_fraction(n, i, j, rad2);
+                    phisum += phi;
+                    const double mu_e = phi * mu_f + (1.0 - phi) * mu_matrix;
+                    const double k_e = phi * (k_over_mu * mu_f) + (1.0 - phi) * (k_over_mu * mu_matrix);
+                    eparams.push_back(mu_e);
+                    eparams.push_back(k_e - 2.0 * mu_e / 3.0);
                 }
-        f->vf_actual[r] = (double)nfib / (n * n * n);
+        f->vf_actual[r] = phisum / ((double)n * n * n);
     }
     f->n_nodes = f->node_off[n_rve];
     f->n_red = f->red_off[n_rve];
-    // ---- element loop: compressible Neo-Hookean phases (ModCompressibleNeoHookean.f90) ----
-    const double mu_m = mu_matrix, mu_f = mu_matrix * stiff_ratio;
-    const double pm[2] = {mu_m, k_over_mu * mu_m - 2.0 * mu_m / 3.0};
-    const double pf[2] = {mu_f, k_over_mu * mu_f - 2.0 * mu_f / 3.0};
-    ceos_material mats[2] = {{CEOS_CNH, 0, 2, pm}, {CEOS_CNH, 0, 2, pf}};
-    ceos_mesh mesh{f->n_nodes, (int)(conn.size() / 8), X.data(), conn.data(), mat_id.data()};
+    // ---- element loop: compressible Neo-Hookean cells (ModCompressibleNeoHookean.f90) ----
+    ceos_material mat{CEOS_CNH, 1, 2, eparams.data()};
+    ceos_mesh mesh{f->n_nodes, (int)(conn.size() / 8), X.data(), conn.data(), nullptr};
     void* lh = nullptr;
-    int rc = ceos_create(&mesh, mats, 2, CEOS_FP64, device, &lh);
+    int rc = ceos_create(&mesh, &mat, 1, CEOS_FP64, device, &lh);
     if (rc) { delete f; return rc; }
     f->loop = static_cast<Handle*>(lh);
     f->nnz = f->loop->nnz;

@@ -158,14 +158,17 @@ int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, double mu_m
 /* Mesh sizes and the discretised fibre fraction of every RVE (any pointer may be NULL). */
 int ceos_fe2_info(void* handle, int* n_nodes, int* n_elem, int* n_red, double* vf_actual);
 /* Solve every RVE under its macro deformation gradient Fbar [n_rve][9] (row-major 3x3): Newton
- * on the periodic fluctuations to ||T^T f_int|| <= tol * (its value at zero fluctuation), each
- * linear system by block-Jacobi PCG (FP32) with FP64 refinement to 1e-8.  Outputs the homogenized
+ * on the periodic fluctuations to ||T^T f_int|| <= tol * (its value at the start of the load
+ * step), per RVE load continuation with backtracking and golden-ratio cut-back, each linear system
+ * by block-Jacobi MINRES (FP32, SPD preconditioner; T^T K T may be indefinite when fibres buckle)
+ * with FP64 refinement to an Eisenstat-Walker tolerance (1e-8 for the tangent).  At most
+ * max_newton iterations per load step; n_cells <= 14.  Outputs the homogenized
  * first Piola stress P [n_rve][9] (row-major, the HomogenizeStress definition,
  * ModMultiscaleAnalysis.f90:140-329) and, when A != NULL, the tangent dP/dFbar [n_rve][81]
  * (row (iJ), column (kL), row-major pairs).  newton_iters / cg_iters [n_rve] may be NULL. */
 int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int max_newton, double* P, double* A,
                    int* newton_iters, int* cg_iters);
-/* Apply Fbar in n_sub equal load increments per solve (default 1). */
+/* First load step of every RVE = 1/n_sub of Fbar - I (default 1: the full load at once). */
 int ceos_fe2_set_increments(void* handle, int n_sub);
 /* Description of the last failure of ceos_fe2_solve (empty when none). */
 int ceos_fe2_message(void* handle, char* msg, int msg_len);

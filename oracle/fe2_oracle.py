@@ -1,6 +1,7 @@
 """FP64 CPU oracle of one periodic RVE (TEST INFRASTRUCTURE ONLY).
 
-Restates the periodic micro problem the batched GPU solver handles: the reference's periodic
+Restates the periodic micro problem the batched GPU solver handles (fibre cells with
+partial-volume moduli, mu_e = phi mu_f + (1 - phi) mu_m and likewise the bulk modulus): the reference's periodic
 multiscale model eliminates the slave DOFs with a matrix T and solves T^T K T du = -T^T R
 (FEM/Modules/ModMultiscalePeriodicFEMSoE.f90:77-182), then homogenizes the first Piola stress
 (HomogenizeStress, MultiScale/ModMultiscaleAnalysis.f90:140-329).  Here u = (Fbar - I) X + T w
@@ -15,8 +16,22 @@ import scipy.sparse.linalg as spla
 import oracle as O
 
 
+def fibre_fraction(n, rad2):
+    """[n][n] fibre area fraction of cell column (i, j): share of 16 x 16 sub-points of its
+    cross-section strictly inside x^2 + y^2 < rad2 about the RVE centre."""
+    sub = (np.arange(16) + 0.5) / 16.0
+    phi = np.zeros((n, n))
+    for j in range(n):
+        for i in range(n):
+            x = (i + sub[None, :]) / n - 0.5
+            y = (j + sub[:, None]) / n - 0.5
+            phi[j, i] = np.count_nonzero(x * x + y * y < rad2) / 256.0
+    return phi
+
+
 def rve_mesh(n, vf):
-    """Unit cube, n^3 cells, fibre along z through the centre (cells by centroid)."""
+    """Unit cube, n^3 cells, fibre along z through the centre; per-cell fibre fraction phi
+    (partial-volume cells)."""
     m = n + 1
     k, j, i = np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij")
     X = np.stack([i.ravel() / n, j.ravel() / n, k.ravel() / n], axis=1)
@@ -28,18 +43,20 @@ def rve_mesh(n, vf):
     conn = np.stack([nid(ie, je, ke), nid(ie + 1, je, ke), nid(ie + 1, je + 1, ke), nid(ie, je + 1, ke),
                      nid(ie, je, ke + 1), nid(ie + 1, je, ke + 1), nid(ie + 1, je + 1, ke + 1),
                      nid(ie, je + 1, ke + 1)], axis=1).astype(np.int32)
-    xc, yc = (ie + 0.5) / n - 0.5, (je + 0.5) / n - 0.5
-    mat = (xc ** 2 + yc ** 2 < vf / np.pi).astype(np.int32)
+    phi = fibre_fraction(n, vf / np.pi)[je, ie]
     ind = ((k % n) * n * n + (j % n) * n + (i % n)).ravel()
-    return X, conn, mat, ind
+    return X, conn, phi, ind
 
 
 class RVE:
     def __init__(self, n, vf, mu_m=1.0, ratio=50.0, k_over_mu=100.0):
-        self.X, self.conn, self.mat, ind = rve_mesh(n, vf)
+        self.X, self.conn, self.phi, ind = rve_mesh(n, vf)
         mu_f = ratio * mu_m
-        params = [[mu_m, k_over_mu * mu_m - 2 * mu_m / 3], [mu_f, k_over_mu * mu_f - 2 * mu_f / 3]]
-        self.model = O.Model(self.X, self.conn, [O.CNH, O.CNH], params, mat_id=self.mat)
+        # cell moduli mixed by fibre fraction (same operation order as the GPU set-up)
+        mu_e = self.phi * mu_f + (1.0 - self.phi) * mu_m
+        k_e = self.phi * (k_over_mu * mu_f) + (1.0 - self.phi) * (k_over_mu * mu_m)
+        params = np.stack([mu_e, k_e - 2.0 * mu_e / 3.0], axis=1)
+        self.model = O.Model(self.X, self.conn, [O.CNH], params, per_element=True)
         self.rowmap, self.col = self.model.pattern()
         nn = self.X.shape[0]
         # T: full dof (3a+d) <- reduced dof 3(ind-1)+d, independent node 0 fixed
@@ -52,7 +69,7 @@ class RVE:
                 cols.append(3 * (ind[a] - 1) + d)
         self.n_red = 3 * (n ** 3 - 1)
         self.T = sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(3 * nn, self.n_red))
-        self.vf_actual = self.mat.mean()
+        self.vf_actual = self.phi.mean()
 
     def _K(self, kval):
         n = 3 * self.X.shape[0]
