@@ -1,0 +1,227 @@
+"""Macro FE^2 on one GPU: a Hexa8 macro mesh whose Gauss points take their constitutive response
+from the learned surrogate (points outside its training box fall back to RVE solves) or from
+batched RVE solves everywhere (the direct method), with the macro Newton iteration, boundary
+conditions, element loop and linear solves on the device.
+
+The reference runs the macro problem with its FE^2 analysis (MultiScale/ModMultiscaleAnalysis.f90)
+and one RVE solve per macro Gauss point; the element loop here reads each point's Cauchy stress
+and spatial tangent from the external-material state (model 200) the material step writes.
+"""
+import ctypes as C
+import time
+
+import numpy as np
+import torch
+
+from . import FP64, CeosError, ElementLoop, _check, _ptr, lib, meshgen
+from . import fe2 as FE2
+
+EXTERNAL = 200
+_VI = [0, 1, 2, 0, 1, 0]
+_VJ = [0, 1, 2, 1, 2, 2]
+
+
+def _setup():
+    L = lib()
+    P, I, D = C.c_void_p, C.c_int, C.c_double
+    L.ceos_gp_deformation_device.argtypes = [P, P, P, P]
+    L.ceos_state_device.argtypes = [P, C.POINTER(P), C.POINTER(C.c_longlong), C.POINTER(I)]
+    L.ceos_pcg_create.argtypes = [P, C.POINTER(P)]
+    L.ceos_pcg_solve.argtypes = [P, P, P, P, P, D, I, C.POINTER(I), C.POINTER(D)]
+    L.ceos_pcg_destroy.argtypes = [P]
+    L.ceos_pcg_destroy.restype = None
+    L.ceos_state_scatter.argtypes = [P, I, P, P, I]
+    return L
+
+
+def spatial_from_PA(F, P, A):
+    """Cauchy stress [N,6] and spatial tangent [N,21] (upper Voigt entries, tensor components) from
+    the first Piola stress P [N,3,3] and its tangent A = dP/dF [N,9,9] (row (iJ), column (kL)):
+    sigma = P F^T / J and c_ijkl = F_jJ F_lL A_iJkL / J - delta_ik sigma_jl, minor-symmetrised."""
+    J = np.linalg.det(F)
+    sig = np.einsum("niJ,njJ->nij", P, F) / J[:, None, None]
+    A4 = A.reshape(-1, 3, 3, 3, 3)
+    c = np.einsum("njJ,nlL,niJkL->nijkl", F, F, A4) / J[:, None, None, None, None]
+    c -= np.einsum("ik,njl->nijkl", np.eye(3), sig)
+    c = 0.25 * (c + c.transpose(0, 2, 1, 3, 4) + c.transpose(0, 1, 2, 4, 3) + c.transpose(0, 2, 1, 4, 3))
+    s6 = np.stack([0.5 * (sig[:, i, j] + sig[:, j, i]) for i, j in zip(_VI, _VJ)], axis=1)
+    D = []
+    for p in range(6):
+        for q in range(p, 6):
+            D.append(c[:, _VI[p], _VJ[p], _VI[q], _VJ[q]])
+    return s6, np.stack(D, axis=1)
+
+
+def uniaxial_bc(X):
+    """Face x=0 fixed in x, corner (0,0,0) pinned, u_z = 0 at corner (0,1,0) (no rigid rotation about
+    x), face x=1 prescribed in x.  Returns (fixed 0-based dofs, prescribed x1-face dofs)."""
+    f = meshgen.node_grid_index(X)
+    fixed = set(3 * n for n in np.nonzero(f["x0"])[0])
+    c0 = np.nonzero(f["x0"] & f["y0"] & f["z0"])[0][0]
+    fixed.update(3 * c0 + d for d in range(3))
+    c1 = np.nonzero(f["x0"] & f["y1"] & f["z0"])[0][0]
+    fixed.add(3 * c1 + 2)
+    presc = np.array([3 * n for n in np.nonzero(f["x1"])[0]], np.int64)
+    return np.array(sorted(fixed), np.int64), presc
+
+
+class MacroFE2:
+    """Macro unit cube of nx^3 Hexa8 cells; element e carries fibre fraction vf_elem[e] and every
+    one of its Gauss points owns an n_cells^3 periodic RVE of that fraction."""
+
+    def __init__(self, nx, vf_elem, n_cells=6, surrogate=None, mu_matrix=1.0, stiff_ratio=50.0, k_over_mu=100.0,
+                 device=0):
+        self._L = _setup()
+        X, conn = meshgen.structured_box(nx, nx, nx, jitter=0.0)
+        self.X = X
+        self.loop = ElementLoop(X, conn, EXTERNAL, [[0.0]], precision=FP64, device=device)
+        self.n_elem = self.loop.n_elem
+        self.n_gp = 8 * self.n_elem
+        self.n_dof = self.loop.n_dof
+        self.vf_elem = np.ascontiguousarray(vf_elem, np.float64)
+        self.n_cells = n_cells
+        self.rve_args = dict(mu_matrix=mu_matrix, stiff_ratio=stiff_ratio, k_over_mu=k_over_mu, device=device)
+        self.sur = surrogate
+        dev = torch.device("cuda", device)
+        self.dev = dev
+        self.U = torch.zeros(self.n_dof, dtype=torch.float64, device=dev)
+        self.dU = torch.zeros_like(self.U)
+        self.fint = torch.zeros_like(self.U)
+        self.rhs = torch.zeros_like(self.U)
+        self.kval = torch.zeros(self.loop.nnz, dtype=torch.float64, device=dev)
+        self.F = torch.zeros(9 * self.n_gp, dtype=torch.float64, device=dev)
+        self.vf_dev = torch.as_tensor(self.vf_elem, device=dev)
+        self.flags = torch.zeros(self.n_gp, dtype=torch.int32, device=dev)
+        fixed, self.presc = uniaxial_bc(X)
+        mask = np.zeros(self.n_dof, np.uint8)
+        mask[fixed] = 1
+        mask[self.presc] = 1
+        self.fixed = fixed
+        self.mask = torch.as_tensor(mask, device=dev)
+        self.free = torch.as_tensor(mask == 0, device=dev)
+        st = C.c_void_p()
+        ld = C.c_longlong()
+        f32 = C.c_int()
+        _check(self._L.ceos_state_device(self.loop.handle, C.byref(st), C.byref(ld), C.byref(f32)))
+        self.state_ptr, self.ld, self.state_f32 = st.value, ld.value, f32.value
+        pcg = C.c_void_p()
+        _check(self._L.ceos_pcg_create(self.loop.handle, C.byref(pcg)))
+        self._pcg = pcg
+        self._direct = None
+        self.stats = {"material_s": 0.0, "loop_s": 0.0, "solve_s": 0.0, "fallback_points": 0, "pcg_iters": 0}
+
+    # ---- material step ------------------------------------------------------------------------
+    def _gp_F_host(self, idx=None):
+        F = self.F.view(9, self.n_gp).T
+        F = F if idx is None else F[torch.as_tensor(idx, device=self.dev)]
+        return F.cpu().numpy().reshape(-1, 3, 3)
+
+    def _rve_response(self, idx, batch):
+        """Solve the RVEs of points idx (Fbar from the current F) and write sigma, D into the state."""
+        Fh = self._gp_F_host(idx)
+        out = batch.solve(Fh, tangent=True)
+        sig, D = spatial_from_PA(Fh, out["P"], out["A"])
+        vals = np.ascontiguousarray(np.concatenate([sig, D], axis=1))
+        q = np.ascontiguousarray(idx, np.int32)
+        _check(self._L.ceos_state_scatter(self.loop.handle, len(q), _ptr(q), _ptr(vals), 27))
+        return out
+
+    def material(self, mode):
+        t0 = time.perf_counter()
+        _check(self._L.ceos_gp_deformation_device(self.loop.handle, C.c_void_p(self.U.data_ptr()),
+                                                  C.c_void_p(self.F.data_ptr()), None))
+        torch.cuda.synchronize(self.dev)
+        n_fb = 0
+        if mode == "surrogate":
+            self.sur.material_device(self.n_elem, C.c_void_p(self.F.data_ptr()), self.n_gp,
+                                     C.c_void_p(self.vf_dev.data_ptr()), C.c_void_p(self.state_ptr), self.state_f32,
+                                     self.ld, C.c_void_p(self.flags.data_ptr()))
+            torch.cuda.synchronize(self.dev)
+            idx = torch.nonzero(self.flags).flatten().cpu().numpy()
+            if idx.size:
+                n_fb = idx.size
+                vf = self.vf_elem[idx % self.n_elem]
+                b = FE2.BatchedRVE(np.full(idx.size, self.n_cells, np.int32), vf, **self.rve_args)
+                self._rve_response(idx, b)
+                b.close()
+        else:
+            if self._direct is None:
+                vf = np.tile(self.vf_elem, 8)  # point q = gp * n_elem + e
+                self._direct = FE2.BatchedRVE(np.full(self.n_gp, self.n_cells, np.int32), vf, **self.rve_args)
+            self._rve_response(np.arange(self.n_gp), self._direct)
+            n_fb = self.n_gp
+        torch.cuda.synchronize(self.dev)
+        self.stats["material_s"] += time.perf_counter() - t0
+        self.stats["fallback_points"] += n_fb if mode == "surrogate" else 0
+        return n_fb
+
+    # ---- Newton -------------------------------------------------------------------------------
+    def newton_step(self, ux_target, mode, tol=1e-6, max_newton=15, pcg_tol=1e-8):
+        """One load step: x1-face displacement ux_target; returns Newton iterations."""
+        self.U[torch.as_tensor(self.presc, device=self.dev)] = ux_target
+        r0 = None
+        for it in range(max_newton + 1):
+            self.material(mode)
+            t0 = time.perf_counter()
+            self.loop.evaluate_device(0.0, self.U, self.fint, self.kval)
+            torch.cuda.synchronize(self.dev)
+            rc, nf = self.loop.status()
+            if rc:
+                raise CeosError(rc, f"{nf} macro elements folded")
+            self.stats["loop_s"] += time.perf_counter() - t0
+            torch.neg(self.fint, out=self.rhs)
+            self.rhs[self.mask.bool()] = 0.0
+            rn = float(torch.linalg.vector_norm(self.rhs))
+            r0 = rn if r0 is None else r0
+            if rn <= tol * max(r0, 1e-300) or rn <= 1e-12:
+                return it
+            if it == max_newton:
+                break
+            t0 = time.perf_counter()
+            iters, rel = C.c_int(), C.c_double()
+            rc = self._L.ceos_pcg_solve(self._pcg, C.c_void_p(self.kval.data_ptr()), C.c_void_p(self.mask.data_ptr()),
+                                        C.c_void_p(self.rhs.data_ptr()), C.c_void_p(self.dU.data_ptr()), pcg_tol,
+                                        20000, C.byref(iters), C.byref(rel))
+            if rc and rel.value > 1e-4:
+                raise CeosError(rc, f"macro PCG stalled at relative residual {rel.value:.2e}")
+            self.stats["pcg_iters"] += iters.value
+            self.U += self.dU
+            torch.cuda.synchronize(self.dev)
+            self.stats["solve_s"] += time.perf_counter() - t0
+        raise CeosError(1, f"macro Newton did not converge (residual {rn:.3e}, first {r0:.3e})")
+
+    def run(self, stretch=1.2, n_steps=10, mode="surrogate", tol=1e-6, max_newton=15):
+        """Uniaxial stretch of the x1 face to `stretch` in n_steps increments.  Returns per-step wall
+        times (s), Newton iterations and fallback points."""
+        L = self.X[:, 0].max() - self.X[:, 0].min()
+        times, its, fbs = [], [], []
+        for k in range(1, n_steps + 1):
+            fb0 = self.stats["fallback_points"]
+            torch.cuda.synchronize(self.dev)
+            t0 = time.perf_counter()
+            its.append(self.newton_step((stretch - 1.0) * L * k / n_steps, mode, tol, max_newton))
+            torch.cuda.synchronize(self.dev)
+            times.append(time.perf_counter() - t0)
+            fbs.append(self.stats["fallback_points"] - fb0)
+        return {"step_s": np.array(times), "newton": np.array(its), "fallback_points": np.array(fbs)}
+
+    def gp_first_piola(self):
+        """First Piola stress at every Gauss point [n_gp,3,3] from the state (sigma) and F."""
+        st = self.loop.state(0)  # [n_elem, 8, 27]
+        sig6 = np.transpose(st[:, :, :6], (1, 0, 2)).reshape(self.n_gp, 6)
+        sig = np.zeros((self.n_gp, 3, 3))
+        for p, (i, j) in enumerate(zip(_VI, _VJ)):
+            sig[:, i, j] = sig6[:, p]
+            sig[:, j, i] = sig6[:, p]
+        F = self._gp_F_host()
+        J = np.linalg.det(F)
+        return J[:, None, None] * np.einsum("nij,nKj->niK", sig, np.linalg.inv(F))
+
+    def close(self):
+        if getattr(self, "_pcg", None):
+            self._L.ceos_pcg_destroy(self._pcg)
+            self._pcg = None
+        if self._direct is not None:
+            self._direct.close()
+            self._direct = None
+        self.loop.close()

@@ -39,6 +39,7 @@ int model_nparams(int model) {
         case M_VISCO_PRONY: return ModelInfo<M_VISCO_PRONY>::nparams;
         case M_J2_FINITE: return ModelInfo<M_J2_FINITE>::nparams;
         case M_VISCO_VAR: return ModelInfo<M_VISCO_VAR>::nparams;
+        case M_EXTERNAL: return ModelInfo<M_EXTERNAL>::nparams;
     }
     return -1;
 }
@@ -50,6 +51,7 @@ int model_nstate(int model) {
         case M_VISCO_PRONY: return ModelInfo<M_VISCO_PRONY>::nstate;
         case M_J2_FINITE: return ModelInfo<M_J2_FINITE>::nstate;
         case M_VISCO_VAR: return ModelInfo<M_VISCO_VAR>::nstate;
+        case M_EXTERNAL: return ModelInfo<M_EXTERNAL>::nstate;
     }
     return -1;
 }
@@ -135,6 +137,7 @@ int launch_elem(Handle* h, double dt, const double* dU, double* dfint, double* d
         case M_VISCO_PRONY: return launch_model<T, M_VISCO_PRONY>(h, dt, dU, dfint, dkval, s);
         case M_J2_FINITE: return launch_model<T, M_J2_FINITE>(h, dt, dU, dfint, dkval, s);
         case M_VISCO_VAR: return launch_model<T, M_VISCO_VAR>(h, dt, dU, dfint, dkval, s);
+        case M_EXTERNAL: return launch_model<T, M_EXTERNAL>(h, dt, dU, dfint, dkval, s);
     }
     return CEOS_E_MODEL;
 }
@@ -168,6 +171,10 @@ int occupancy_grid(Handle* h) {
         case M_VISCO_VAR:
             e = cudaFuncSetAttribute(element_loop_kernel<T, M_VISCO_VAR, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
             if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_VISCO_VAR, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
+            break;
+        case M_EXTERNAL:
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_EXTERNAL, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_EXTERNAL, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
             break;
     }
     if (e != cudaSuccess || per_sm < 1) per_sm = 1;
@@ -468,6 +475,55 @@ extern "C" int ceos_last_error(void* handle, int* elem_ids, int max_ids, char* m
         msg[msg_len - 1] = 0;
     }
     return n;
+}
+
+// Deformation gradient at every Gauss point from device displacements: F [9][8 n_elem] (row-major
+// components, point q = gp * n_elem + e), F = I + dU/dX with the Hexa8 shape functions.
+__global__ void gp_deformation_kernel(int n_elem, const double* X, const double* U, const int* conn0, double* F) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= 8LL * n_elem) return;
+    const int gp = (int)(q / n_elem), e = (int)(q - (long long)gp * n_elem);
+    double JX[3][3] = {}, Xn[8][3], Un[8][3];
+    for (int n = 0; n < 8; ++n) {
+        const int a = conn0[(size_t)8 * e + n];
+        for (int d = 0; d < 3; ++d) { Xn[n][d] = X[3 * (size_t)a + d]; Un[n][d] = U[3 * (size_t)a + d]; }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) JX[i][j] += c_dN[gp][n][i] * Xn[n][j];
+    }
+    const double det = det3(JX);
+    double Ji[3][3];
+    inv3(JX, det, Ji);
+    double Fm[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int n = 0; n < 8; ++n) {
+        double gX[3];
+        for (int j = 0; j < 3; ++j) gX[j] = Ji[j][0] * c_dN[gp][n][0] + Ji[j][1] * c_dN[gp][n][1] + Ji[j][2] * c_dN[gp][n][2];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) Fm[i][j] += Un[n][i] * gX[j];
+    }
+    const long long ld = 8LL * n_elem;
+    for (int k = 0; k < 9; ++k) F[k * ld + q] = Fm[k / 3][k % 3];
+}
+
+extern "C" int ceos_gp_deformation_device(void* handle, const double* dU, double* dF, void* stream) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !dU || !dF) return CEOS_E_ARG;
+    CK(cudaSetDevice(h->device));
+    const long long n = 8LL * h->n_elem;
+    gp_deformation_kernel<<<(unsigned)((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        h->n_elem, h->d_X, dU, h->d_conn, dF);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+// Device pointer of the committed Gauss-point state ([nvars][8][ld], FP64 or FP32 by precision
+// mode), e.g. for an external material to write the stress and tangent the loop reads.
+extern "C" int ceos_state_device(void* handle, void** ptr, long long* ld, int* is_f32) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !ptr) return CEOS_E_ARG;
+    *ptr = h->d_state[h->cur_old];
+    if (ld) *ld = h->ld;
+    if (is_f32) *is_f32 = h->precision == CEOS_MIXED ? 1 : 0;
+    return 0;
 }
 
 extern "C" int ceos_state_size(void* handle, int* nvars) {

@@ -127,6 +127,11 @@ CEOS_D int run_material(const T F[3][3], const T* p, const T* ebr, double dt, co
         svk_update<T>(F, p, sig, D);
     } else if constexpr (MODEL == M_VISCO_PRONY) {
         visco_prony_update<T>(F, p, ebr, io, sig, D);
+    } else if constexpr (MODEL == M_EXTERNAL) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sig[k] = io.ld(k);
+#pragma unroll
+        for (int k = 0; k < 21; ++k) D[k] = io.ld(6 + k);
     } else {
         T st[NS], stn[NS];
 #pragma unroll

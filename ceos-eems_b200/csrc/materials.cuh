@@ -10,7 +10,8 @@
 
 namespace ceos {
 
-enum : int { M_J2_SMALL = 2, M_SVK = 5, M_CNH = 7, M_VISCO_VAR = 12, M_VISCO_PRONY = 101, M_J2_FINITE = 102 };
+enum : int { M_J2_SMALL = 2, M_SVK = 5, M_CNH = 7, M_VISCO_VAR = 12, M_VISCO_PRONY = 101, M_J2_FINITE = 102,
+             M_EXTERNAL = 200 };
 
 template <int MODEL>
 struct ModelInfo;
@@ -26,6 +27,11 @@ template <>
 struct ModelInfo<M_J2_FINITE> { static constexpr int nstate = 7, nparams = 4; };
 template <>
 struct ModelInfo<M_VISCO_VAR> { static constexpr int nstate = 19, nparams = 6; };
+// External constitutive response: the "state" of each Gauss point holds its Cauchy stress (6)
+// and spatial tangent (21 upper entries), written by another kernel before the element loop
+// (the learned FE^2 surrogate, or RVE solves); one unused parameter.
+template <>
+struct ModelInfo<M_EXTERNAL> { static constexpr int nstate = 27, nparams = 1; };
 
 // ---------------------------------------------------------------------------------------
 // Compressible Neo-Hookean (ConstitutiveModelsLibrary/ModCompressibleNeoHookean.f90:422-546):

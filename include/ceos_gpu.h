@@ -46,7 +46,8 @@ enum ceos_precision {
 };
 
 enum ceos_error {
-    CEOS_E_ARG = -1, CEOS_E_CUDA = -2, CEOS_E_ALLOC = -3, CEOS_E_MESH = -4, CEOS_E_MODEL = -5
+    CEOS_E_ARG = -1, CEOS_E_CUDA = -2, CEOS_E_ALLOC = -3, CEOS_E_MESH = -4, CEOS_E_MODEL = -5,
+    CEOS_E_SOLVER = -6 /* iterative solver did not reach its tolerance */
 };
 
 /* Mesh as the reference holds it: CoordX interleaved [3*n_nodes] (ModNodes.f90:55),

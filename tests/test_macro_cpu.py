@@ -1,0 +1,40 @@
+"""CPU checks of the macro FE^2 host logic: the conversion of RVE outputs (first Piola stress and
+its tangent dP/dF) into the Cauchy stress and spatial tangent the element loop reads, against
+the compressible Neo-Hookean oracle, and the uniaxial boundary conditions."""
+import numpy as np
+
+import oracle as O
+from ceos_b200 import meshgen
+from ceos_b200.macro import spatial_from_PA, uniaxial_bc
+
+
+def _P(F, p):
+    s, _, _, _ = O.material_point(O.CNH, p, F)
+    S = np.array([[s[0], s[3], s[5]], [s[3], s[1], s[4]], [s[5], s[4], s[2]]])
+    return np.linalg.det(F) * S @ np.linalg.inv(F).T
+
+
+def test_spatial_tangent_from_first_piola_tangent():
+    rng = np.random.default_rng(0)
+    p = [1.0, 99.3]
+    for _ in range(3):
+        F = np.eye(3) + rng.uniform(-0.2, 0.2, (3, 3))
+        h = 1e-6
+        A = np.zeros((9, 9))
+        for k in range(9):
+            dF = np.zeros(9)
+            dF[k] = h
+            A[:, k] = ((_P(F + dF.reshape(3, 3), p) - _P(F - dF.reshape(3, 3), p)) / (2 * h)).reshape(-1)
+        sig, D = spatial_from_PA(F[None], _P(F, p)[None], A[None])
+        s, Dref, _, _ = O.material_point(O.CNH, p, F)
+        assert np.abs(sig[0] - s).max() <= 1e-12 * np.abs(s).max()
+        assert np.abs(D[0] - Dref[np.triu_indices(6)]).max() <= 1e-8 * np.abs(Dref).max()
+
+
+def test_uniaxial_bc_removes_rigid_motion():
+    X, _ = meshgen.structured_box(3, 3, 3, jitter=0.0)
+    fixed, presc = uniaxial_bc(X)
+    assert len(presc) == 16 and np.all(presc % 3 == 0)
+    assert len(set(fixed) & set(presc)) == 0
+    # x-face fixed in x (16 dofs) + pinned corner (y, z) + one z at corner (0,1,0)
+    assert len(fixed) == 16 + 2 + 1
