@@ -15,6 +15,8 @@ def _setup():
     L.ceos_fe2_solve.argtypes = [P, P, D, I, P, P, P, P]
     L.ceos_fe2_message.argtypes = [P, C.c_char_p, I]
     L.ceos_fe2_set_increments.argtypes = [P, I]
+    L.ceos_fe2_set_allow_failures.argtypes = [P, I]
+    L.ceos_fe2_set_fractions.argtypes = [P, P]
     L.ceos_fe2_destroy.argtypes = [P]
     L.ceos_fe2_destroy.restype = None
     return L
@@ -59,6 +61,18 @@ class BatchedRVE:
     def set_increments(self, n_sub):
         _check(lib().ceos_fe2_set_increments(self._h, n_sub))
 
+    def set_allow_failures(self, allow=True):
+        """RVEs that cannot converge come back as NaN (and newton_iters -1) instead of raising."""
+        _check(lib().ceos_fe2_set_allow_failures(self._h, 1 if allow else 0))
+        self._allow = allow
+
+    def set_fractions(self, vf):
+        """New fibre volume fractions for the same RVE sizes (mesh and pattern kept)."""
+        self.vf = np.ascontiguousarray(vf, dtype=np.float64)
+        assert self.vf.size == self.n_rve
+        _check(lib().ceos_fe2_set_fractions(self._h, _ptr(self.vf)))
+        _check(lib().ceos_fe2_info(self._h, None, None, None, _ptr(self.vf_actual)))
+
     def solve(self, Fbar, tangent=False, tol=1e-8, max_newton=20):
         Fbar = np.ascontiguousarray(np.asarray(Fbar, dtype=np.float64).reshape(self.n_rve, 9))
         P = np.zeros((self.n_rve, 9))
@@ -66,11 +80,11 @@ class BatchedRVE:
         nit = np.zeros(self.n_rve, np.int32)
         cgi = np.zeros(self.n_rve, np.int32)
         rc = lib().ceos_fe2_solve(self._h, _ptr(Fbar), tol, max_newton, _ptr(P), _ptr(A), _ptr(nit), _ptr(cgi))
-        if rc:
+        if rc and not (rc == 2 and getattr(self, "_allow", False)):
             buf = C.create_string_buffer(256)
             lib().ceos_fe2_message(self._h, buf, 256)
             raise CeosError(rc, buf.value.decode())
-        out = {"P": P.reshape(self.n_rve, 3, 3), "newton_iters": nit, "cg_iters": cgi}
+        out = {"P": P.reshape(self.n_rve, 3, 3), "newton_iters": nit, "cg_iters": cgi, "failed": nit < 0}
         if tangent:
             out["A"] = A.reshape(self.n_rve, 9, 9)
         return out

@@ -1,0 +1,142 @@
+"""Training data, fitting and error of the learned FE^2 surrogate, all on the GPU.
+
+Training pairs (C, vf) -> S come from the batched RVE solver itself (ceos_fe2_*): F = I + G with
+G_ij uniform in [-amp, amp] (det F > 0) and vf uniform in vf_range, one fixed RVE resolution
+n_cells (the homogenized response depends on the resolution, so the surrogate stands in for the
+RVE family of that resolution).  The RVE solver is also the judge of the surrogate's error."""
+import time
+
+import numpy as np
+
+from . import fe2 as FE2
+from .surrogate import Surrogate, init_params, training_targets, voigt_C
+
+
+def sample_points(n, seed, amp=0.15, vf_range=(0.1, 0.4)):
+    F = FE2.sample_macro_F(n, seed=seed, amp=amp)
+    vf = np.random.default_rng(seed + 7919).uniform(vf_range[0], vf_range[1], n)
+    return F, vf
+
+
+def rve_stresses(F, vf, n_cells=6, batch=4096, tangent=False, **rve_args):
+    """First Piola stress (and tangent) of the RVEs at (F, vf), solved in batches on the GPU.
+    RVEs that cannot converge come back as NaN.  Returns (P [n,3,3], A [n,9,9] or None, stats)."""
+    n = len(vf)
+    P = np.full((n, 3, 3), np.nan)
+    A = np.full((n, 9, 9), np.nan) if tangent else None
+    b = None
+    t0 = time.perf_counter()
+    newton, failed, minres = 0, 0, 0
+    for s0 in range(0, n, batch):
+        k = min(batch, n - s0)
+        if b is None or b.n_rve != k:
+            if b is not None:
+                b.close()
+            b = FE2.BatchedRVE(np.full(k, n_cells, np.int32), vf[s0:s0 + k], **rve_args)
+            b.set_allow_failures(True)
+        else:
+            b.set_fractions(vf[s0:s0 + k])
+        out = b.solve(F[s0:s0 + k], tangent=tangent)
+        P[s0:s0 + k] = out["P"]
+        if tangent:
+            A[s0:s0 + k] = out["A"]
+        newton += int(out["newton_iters"][out["newton_iters"] > 0].sum())
+        minres += int(out["cg_iters"].sum())
+        failed += int(out["failed"].sum())
+    if b is not None:
+        b.close()
+    secs = time.perf_counter() - t0
+    return P, A, {"seconds": secs, "rve_per_s": n / secs, "failed": failed, "newton_total": newton,
+                  "minres_total": minres}
+
+
+def fit(F, vf, P, epochs=150, batch=2048, lr0=3e-3, lr1=2e-5, seed=0, s_C=0.15, vf0=0.25, s_vf=0.15):
+    """Train a surrogate on the finite samples; the training box of the range check is the
+    component-wise extent of the training inputs.  Returns (Surrogate, loss history, seconds)."""
+    ok = np.all(np.isfinite(P.reshape(len(P), -1)), axis=1)
+    F, vf, P = F[ok], vf[ok], P[ok]
+    C6 = voigt_C(F)
+    S = np.linalg.solve(F, P)
+    s_scale = float(np.sqrt(np.mean(S ** 2)))
+    s_W = s_scale * s_C
+    sur = Surrogate(batch_max=batch)
+    sur.set_params(init_params(seed))
+    sur.set_scaling(s_C, s_W, vf0, s_vf)
+    x = sur.inputs(C6, vf)
+    sur.set_scaling(s_C, s_W, vf0, s_vf, lo=x.min(axis=0), hi=x.max(axis=0))
+    t, w = training_targets(F, P, s_C, s_W)
+    t0 = time.perf_counter()
+    hist = sur.train(x, t, w, epochs, batch, lr0, lr1, seed)
+    return sur, hist, time.perf_counter() - t0
+
+
+def predict_P(sur, F, vf):
+    """Surrogate first Piola stress [n,3,3] and out-of-range flags."""
+    S6, _, flags = sur.evaluate(voigt_C(F), vf)
+    S = np.zeros((len(vf), 3, 3))
+    for p, (i, j) in enumerate([(0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (0, 2)]):
+        S[:, i, j] = S6[:, p]
+        S[:, j, i] = S6[:, p]
+    return F @ S, flags
+
+
+def stress_errors(P_pred, P_ref):
+    """Relative stress errors: aggregate sqrt(sum |dP|^2 / sum |P|^2) and per-point |dP|/|P|."""
+    ok = np.all(np.isfinite(P_ref.reshape(len(P_ref), -1)), axis=1)
+    d = np.linalg.norm((P_pred - P_ref)[ok].reshape(ok.sum(), -1), axis=1)
+    r = np.linalg.norm(P_ref[ok].reshape(ok.sum(), -1), axis=1)
+    return {"aggregate": float(np.sqrt(np.sum(d ** 2) / np.sum(r ** 2))),
+            "median": float(np.median(d / r)), "p95": float(np.percentile(d / r, 95)),
+            "max": float(np.max(d / r)), "n": int(ok.sum())}
+
+
+def macro_compare(sur, nx=4, n_cells=6, stretch=1.2, n_steps=10, seed=11, tol=1e-6):
+    """Uniaxial macro stretch on an nx^3 mesh with the surrogate (RVE fallback outside its box)
+    and with RVE solves at every point; per-step wall times, Newton iterations, fallback points
+    and the relative error of the Gauss-point first Piola stresses of the surrogate run against
+    the direct run after every step."""
+    from . import macro as M
+    vf = np.random.default_rng(seed).uniform(0.1, 0.4, nx ** 3)
+    res, fields = {}, {}
+    for mode in ("direct", "surrogate"):
+        m = M.MacroFE2(nx, vf, n_cells=n_cells, surrogate=sur)
+        L = m.X[:, 0].max() - m.X[:, 0].min()
+        times, its, fbs, Ps = [], [], [], []
+        for k in range(1, n_steps + 1):
+            fb0 = m.stats["fallback_points"]
+            t0 = time.perf_counter()
+            its.append(m.newton_step((stretch - 1.0) * L * k / n_steps, mode, tol))
+            times.append(time.perf_counter() - t0)
+            fbs.append(m.stats["fallback_points"] - fb0)
+            Ps.append(m.gp_first_piola())
+        res[mode] = {"step_s": times, "newton": its, "fallback_points": fbs, "stats": dict(m.stats)}
+        fields[mode] = Ps
+        m.close()
+    res["stress_error_per_step"] = [stress_errors(Psu, Pd)["aggregate"]
+                                    for Pd, Psu in zip(fields["direct"], fields["surrogate"])]
+    return res
+
+
+def macro_surrogate_run(sur, nx=32, stretch=1.2, n_steps=10, seed=12, tol=1e-6, max_fallback=4096, n_cells=6):
+    """Surrogate macro run on nx^3 cells; stops at a step that would send more than max_fallback
+    points to RVE solves (FallbackLimit).  Returns per-step times and the steps done."""
+    from . import macro as M
+    vf = np.random.default_rng(seed).uniform(0.1, 0.4, nx ** 3)
+    m = M.MacroFE2(nx, vf, n_cells=n_cells, surrogate=sur)
+    m.max_fallback = max_fallback
+    L = m.X[:, 0].max() - m.X[:, 0].min()
+    times, its, fbs, stopped = [], [], [], None
+    for k in range(1, n_steps + 1):
+        fb0 = m.stats["fallback_points"]
+        t0 = time.perf_counter()
+        try:
+            its.append(m.newton_step((stretch - 1.0) * L * k / n_steps, "surrogate", tol))
+        except M.FallbackLimit as e:
+            stopped = {"step": k, "reason": str(e)}
+            break
+        times.append(time.perf_counter() - t0)
+        fbs.append(m.stats["fallback_points"] - fb0)
+    out = {"step_s": times, "newton": its, "fallback_points": fbs, "stopped": stopped, "n_gp": m.n_gp,
+           "stats": dict(m.stats)}
+    m.close()
+    return out

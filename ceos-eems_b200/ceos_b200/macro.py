@@ -65,6 +65,10 @@ def uniaxial_bc(X):
     return np.array(sorted(fixed), np.int64), presc
 
 
+class FallbackLimit(RuntimeError):
+    """More Gauss points left the surrogate's training box than the caller allows to solve."""
+
+
 class MacroFE2:
     """Macro unit cube of nx^3 Hexa8 cells; element e carries fibre fraction vf_elem[e] and every
     one of its Gauss points owns an n_cells^3 periodic RVE of that fraction."""
@@ -126,6 +130,8 @@ class MacroFE2:
         _check(self._L.ceos_state_scatter(self.loop.handle, len(q), _ptr(q), _ptr(vals), 27))
         return out
 
+    max_fallback = None  # cap on points sent back to RVE solves in one material step
+
     def material(self, mode):
         t0 = time.perf_counter()
         _check(self._L.ceos_gp_deformation_device(self.loop.handle, C.c_void_p(self.U.data_ptr()),
@@ -138,6 +144,8 @@ class MacroFE2:
                                      self.ld, C.c_void_p(self.flags.data_ptr()))
             torch.cuda.synchronize(self.dev)
             idx = torch.nonzero(self.flags).flatten().cpu().numpy()
+            if self.max_fallback is not None and idx.size > self.max_fallback:
+                raise FallbackLimit(f"{idx.size} of {self.n_gp} points outside the training box")
             if idx.size:
                 n_fb = idx.size
                 vf = self.vf_elem[idx % self.n_elem]

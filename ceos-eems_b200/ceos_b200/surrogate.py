@@ -137,3 +137,14 @@ def training_targets(F, P, s_C, s_W):
     S = voigt_S_from_P(F, P)
     t = S / (VOIGT_A * (s_W / s_C))
     return t, VOIGT_A ** 2
+
+
+def init_params(seed=0):
+    """He-style initial parameters (normal, std sqrt(2/fan_in); output layer sqrt(1/128); zero biases)."""
+    rng = np.random.default_rng(seed)
+    H = 128
+    parts = [rng.normal(0, np.sqrt(2.0 / 7), (H, 7)).ravel(), np.zeros(H)]
+    for _ in range(3):
+        parts += [rng.normal(0, np.sqrt(2.0 / H), (H, H)).ravel(), np.zeros(H)]
+    parts += [rng.normal(0, np.sqrt(1.0 / H), H), np.zeros(1)]
+    return np.concatenate(parts).astype(np.float32)

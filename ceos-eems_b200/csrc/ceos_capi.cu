@@ -515,6 +515,27 @@ extern "C" int ceos_gp_deformation_device(void* handle, const double* dU, double
     return 0;
 }
 
+// Replace the per-element parameters of a handle created with per_element materials:
+// params [n_elem][n_params] (element-major, as at creation).
+extern "C" int ceos_update_params(void* handle, const double* params) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !params || h->param_mode != 1) return CEOS_E_ARG;
+    CK(cudaSetDevice(h->device));
+    const size_t E = h->n_elem, np = h->n_params;
+    std::vector<double> P(np * E);
+    for (size_t e = 0; e < E; ++e)
+        for (size_t k = 0; k < np; ++k) P[k * E + e] = params[e * np + k];
+    h->host_params = P;
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->precision == CEOS_FP64) {
+        CK(cudaMemcpy(h->d_params, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(P.begin(), P.end());
+        CK(cudaMemcpy(h->d_params, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return 0;
+}
+
 // Device pointer of the committed Gauss-point state ([nvars][8][ld], FP64 or FP32 by precision
 // mode), e.g. for an external material to write the stress and tangent the loop reads.
 extern "C" int ceos_state_device(void* handle, void** ptr, long long* ld, int* is_f32) {

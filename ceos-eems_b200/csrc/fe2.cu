@@ -42,6 +42,8 @@ struct Fe2 {
     int n_rve = 0, device = 0;
     double force_floor = 0.0;            // residual norm below which an RVE counts as converged
     int n_sub = 1;                       // macro load sub-increments per solve
+    double mu_m = 1.0, mu_f = 50.0, k_over_mu = 100.0;
+    int allow_failures = 0;              // 1: RVEs that cannot converge are reported, not fatal
     std::vector<int> n;                  // cells per side of each RVE
     std::vector<double> vf_nominal, vf_actual;
     Handle* loop = nullptr;              // element loop over the union of all RVE meshes
@@ -650,6 +652,9 @@ extern "C" int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, 
     f->device = device;
     // round-off level of the nodal forces of a unit RVE with the stiffer phase
     f->force_floor = 1e-11 * mu_matrix * std::max(1.0, stiff_ratio);
+    f->mu_m = mu_matrix;
+    f->mu_f = mu_matrix * stiff_ratio;
+    f->k_over_mu = k_over_mu;
     f->n.assign(n_cells, n_cells + n_rve);
     f->vf_nominal.assign(vf, vf + n_rve);
     // ---- union mesh: RVE r = unit cube, n^3 cells; fibre along z through the centre ----
@@ -791,21 +796,25 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
     const bool verbose = std::getenv("CEOS_FE2_VERBOSE") != nullptr;
     // Per-RVE load continuation Fbar(a) = I + a (Fbar - I): each RVE advances from its last
     // converged level a_done towards 1 in steps da (1/n_sub at first).  A Newton step is accepted
-    // when no element folds and the residual grows by at most kGrowth; otherwise it is halved
+    // when no element folds and the residual grows by at most kGrowth (never beyond kDiverge x the
+    // residual at the start of the load step); otherwise it is halved
     // (backtracking line search) up to kMaxHalvings times.  A load step that still fails, or does
     // not converge in max_newton iterations, is cut back: the RVE returns to its converged
     // fluctuations and da shrinks by the golden ratio, as the reference's quasi-static driver
     // cuts back its load steps (ModFEMAnalysis.f90:1136-1374).
     constexpr int kMaxHalvings = 6, kMaxCutbacks = 16;
-    constexpr double kGrowth = 1.5;
+    // a looser growth test (4x) accepted steps whose linear solves then cost more in total
+    constexpr double kGrowth = 1.5, kDiverge = 1e3;
     const double golden = 0.6180339887498949;
-    enum { kNewton = 0, kDone = 1 };
+    enum { kNewton = 0, kDone = 1, kFailed = 2 };
     std::vector<int> phase(nr, kNewton), nit(nr, 0), halv(nr, 0), cuts(nr, 0), its(nr, 0), cg_tot(nr, 0);
     std::vector<int> op(nr), need(nr), fail(nr), cgi(nr);
     std::vector<double> a_done(nr, 0.0), da(nr, 1.0 / std::max(1, f->n_sub)), a_try(nr), r0(nr, 1.0), racc(nr, 0.0),
         rn(nr), eta(nr, 1.0), Fs(9 * (size_t)nr);
     for (int r = 0; r < nr; ++r) a_try[r] = std::min(1.0, da[r]);
-    const int max_rounds = (max_newton + kMaxHalvings + 2) * (kMaxCutbacks + 2 * std::max(1, f->n_sub) + 2);
+    // every round advances each active RVE by one Newton step, halving, cut-back or load step;
+    // a generous cap bounds the whole solve (RVEs still running then fail)
+    const int max_rounds = 4 * (max_newton + kMaxHalvings + 2) * (kMaxCutbacks + 2 * std::max(1, f->n_sub) + 8);
     bool all_done = false;
     for (int round = 0; round < max_rounds && !all_done; ++round) {
         for (int r = 0; r < nr; ++r)
@@ -836,14 +845,14 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
         for (int r = 0; r < nr; ++r) {
             op[r] = kOpNone;
             need[r] = 0;
-            if (phase[r] == kDone) continue;
+            if (phase[r] != kNewton) continue;
             all_done = false;
             const bool ok = !fail[r] && std::isfinite(rn[r]);
             bool cut = false, accepted = false;
             if (nit[r] == 0) {  // start of a load step from the converged fluctuations
                 if (!ok) cut = true;
                 else { r0[r] = std::max(rn[r], 1e-300); accepted = true; }
-            } else if (ok && rn[r] <= kGrowth * racc[r]) {
+            } else if (ok && rn[r] <= kGrowth * racc[r] && rn[r] <= kDiverge * r0[r]) {
                 accepted = true;
             } else if (halv[r] >= kMaxHalvings) {
                 cut = true;
@@ -882,7 +891,12 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
                 if (++cuts[r] > kMaxCutbacks) {
                     f->msg = "RVE " + std::to_string(r) + ": no convergence after " + std::to_string(kMaxCutbacks) +
                              " load cut-backs (converged load level " + std::to_string(a_done[r]) + ")";
-                    return st ? st : 1;
+                    if (!f->allow_failures) return st ? st : 1;
+                    // give up on this RVE: back to its last converged state, reported as failed
+                    phase[r] = kFailed;
+                    op[r] = kOpRestore;
+                    a_try[r] = a_done[r];
+                    continue;
                 }
                 op[r] = kOpRestore;
                 da[r] *= golden;
@@ -914,8 +928,17 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
     }
     if (!all_done) {
         f->msg = "load continuation did not finish";
-        return 1;
+        if (!f->allow_failures) return 1;
+        for (int r = 0; r < nr; ++r)
+            if (phase[r] == kNewton) phase[r] = kFailed;  // the last assembly is not at their converged state
     }
+    int n_failed = 0;
+    for (int r = 0; r < nr; ++r)
+        if (phase[r] == kFailed) {
+            ++n_failed;
+            its[r] = -1;
+        }
+    if (n_failed) f->msg = std::to_string(n_failed) + " RVE(s) did not converge";
     // converged state: K and f_int of the last assembly
     homogenize_kernel<<<f->n_rve, 256, 0, s>>>(f->n_rve, f->d_node_off, h->d_X, h->d_fint, f->d_P, 1.0);
     CKF(cudaGetLastError());
@@ -951,9 +974,50 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
         CKF(cudaMemcpyAsync(A, f->d_A, sizeof(double) * 81 * f->n_rve, cudaMemcpyDeviceToHost, s));
     }
     CKF(cudaStreamSynchronize(s));
+    for (int r = 0; r < nr; ++r)
+        if (phase[r] == kFailed) {
+            for (int k = 0; k < 9; ++k) P[9 * (size_t)r + k] = std::nan("");
+            if (A)
+                for (int k = 0; k < 81; ++k) A[81 * (size_t)r + k] = std::nan("");
+        }
     if (newton_iters) std::copy(its.begin(), its.end(), newton_iters);
     if (cg_iters) std::copy(cg_tot.begin(), cg_tot.end(), cg_iters);
+    return n_failed ? 2 : 0;
+}
+
+// Report RVEs that cannot converge (P and A set to NaN, newton_iters -1, return value 2) instead of
+// failing the whole solve.
+extern "C" int ceos_fe2_set_allow_failures(void* handle, int allow) {
+    Fe2* f = static_cast<Fe2*>(handle);
+    if (!f) return CEOS_E_ARG;
+    f->allow_failures = allow ? 1 : 0;
     return 0;
+}
+
+// New fibre volume fractions for the same RVE sizes (cell moduli recomputed, mesh kept).
+extern "C" int ceos_fe2_set_fractions(void* handle, const double* vf) {
+    Fe2* f = static_cast<Fe2*>(handle);
+    if (!f || !vf) return CEOS_E_ARG;
+    std::vector<double> eparams;
+    eparams.reserve(2 * (size_t)f->loop->n_elem);
+    for (int r = 0; r < f->n_rve; ++r) {
+        const int n = f->n[r];
+        const double rad2 = vf[r] / M_PI;
+        double phisum = 0.0;
+        for (int k = 0; k < n; ++k)
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                    const double phi = fibre_fraction(n, i, j, rad2);
+                    phisum += phi;
+                    const double mu_e = phi * f->mu_f + (1.0 - phi) * f->mu_m;
+                    const double k_e = phi * (f->k_over_mu * f->mu_f) + (1.0 - phi) * (f->k_over_mu * f->mu_m);
+                    eparams.push_back(mu_e);
+                    eparams.push_back(k_e - 2.0 * mu_e / 3.0);
+                }
+        f->vf_nominal[r] = vf[r];
+        f->vf_actual[r] = phisum / ((double)n * n * n);
+    }
+    return ceos_update_params(f->loop, eparams.data());
 }
 
 extern "C" int ceos_fe2_set_increments(void* handle, int n_sub) {

@@ -269,7 +269,7 @@ extern "C" int ceos_pcg_create(void* loop_handle, void** pcg) {
 // Solve K_ff x_f = b_f (x = 0 on dofs with fixed[i] != 0) for the element loop's upper CSR K
 // (device pointer, FP64), to ||r|| <= tol ||b_f||.  All pointers are device pointers.
 // iters / rel_res (host) receive the iteration count and the final relative residual.
-extern "C" int ceos_pcg_solve(void* pcg, const double* dK, const uint8_t* dfixed, const double* db, double* dx,
+extern "C" int ceos_pcg_solve(void* pcg, const double* dK, const unsigned char* dfixed, const double* db, double* dx,
                               double tol, int max_iter, int* iters, double* rel_res) {
     Pcg* g = static_cast<Pcg*>(pcg);
     if (!g || !dK || !dfixed || !db || !dx || max_iter < 1) return CEOS_E_ARG;

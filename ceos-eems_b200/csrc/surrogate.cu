@@ -1053,7 +1053,7 @@ extern "C" int ceos_sur_evaluate(void* handle, int n, const double* C6, const do
 extern "C" int ceos_sur_material_device(void* handle, int n_elem, const double* F, long long ldF, const double* vf,
                                         void* state, int state_f32, long long ld, int* flags, void* stream) {
     Sur* s = static_cast<Sur*>(handle);
-    if (!s || n_elem < 1 || !F || !vf || !state || ld < n_elem) return CEOS_E_ARG;
+    if (!s || n_elem < 1 || !F || ldF < 8LL * n_elem || !vf || !state || ld < n_elem) return CEOS_E_ARG;
     CKS(cudaSetDevice(s->device));
     InferArgs a{};
     a.n = 8 * n_elem;

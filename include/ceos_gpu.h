@@ -148,6 +148,61 @@ int ceos_cnh_assemble_noalloc(int n_nodes, int n_elem, const double* X_device, c
                               long long nnz, double mu, double lambda, double* fint_device,
                               double* kval_device, void* stream);
 
+/* ---- Device-side pieces for external materials and macro problems (no reference
+ * counterpart; the reference evaluates materials inside its element loop and solves with PARDISO)
+ * ---------------------------------------------------------------------------------------------- */
+/* Replace the per-element parameters of a handle created with per_element materials:
+ * params [n_elem][n_params] (element-major, as at creation). */
+int ceos_update_params(void* handle, const double* params);
+/* Deformation gradient at every Gauss point from device displacements U [3*n_nodes]:
+ * F [9][8*n_elem] (row-major components, point q = gp*n_elem + e), device pointers. */
+int ceos_gp_deformation_device(void* handle, const double* U_device, double* F_device, void* stream);
+/* Device pointer of the committed Gauss-point state [nvars][8][ld] (FP64, or FP32 in mixed mode).
+ * With model 200 (external material) each point's 27 state values are its Cauchy stress (Voigt
+ * 11,22,33,12,23,13) and the 21 upper entries of its spatial tangent, read by the element loop. */
+int ceos_state_device(void* handle, void** state, long long* ld, int* is_f32);
+/* Write nv values per point into the committed state: q [n_pts] point ids (gp*n_elem + e),
+ * vals [n_pts][nv] host arrays. */
+int ceos_state_scatter(void* handle, int n_pts, const int* q, const double* vals, int nv);
+/* Block-Jacobi preconditioned CG on the handle's symmetric upper CSR, on the device
+ * (replaces the PARDISO solve of ModNewtonRaphsonFull.f90:44-168 for device-resident Newton):
+ * solves K_ff x_f = b_f with x = 0 where fixed[i] != 0, to ||r|| <= tol ||b_f||.  K, fixed, b,
+ * x are device pointers; returns 0, or CEOS_E_SOLVER when max_iter is reached. */
+int ceos_pcg_create(void* handle, void** pcg);
+int ceos_pcg_solve(void* pcg, const double* K_device, const unsigned char* fixed_device, const double* b_device,
+                   double* x_device, double tol, int max_iter, int* iters, double* rel_res);
+void ceos_pcg_destroy(void* pcg);
+
+/* ---- Learned FE^2 surrogate (no reference counterpart) ---------------------------------------
+ * MLP energy e(x), x = [(C11-1, C22-1, C33-1, C12, C23, C13)/s_C, (vf - vf0)/s_vf], width 128,
+ * four softplus layers; S_k = a_k (s_W/s_C) de/dx_k (a = 2,2,2,1,1,1) and the material tangent
+ * a_p a_q (s_W/s_C^2) d2e/dx_p dx_q.  Parameters: flat FP32 vector (W1 [128][7], b1, W2, b2, W3,
+ * b3, W4, b4 [128][128] / [128], w5 [128], b5). */
+int ceos_sur_create(int batch_max, int device, void** handle);
+int ceos_sur_n_params(void);
+int ceos_sur_set_params(void* handle, const float* theta);
+int ceos_sur_get_params(void* handle, float* theta);
+/* scales = [s_C, s_W, vf0, s_vf]; lo/hi [7]: training box of x for the range check (may be NULL). */
+int ceos_sur_set_scaling(void* handle, const double* scales, const double* lo, const double* hi);
+/* Gradient of L = (1/n) sum w_k (de/dx_k - t_k)^2 (k < 6) over one batch (n <= batch_max):
+ * x [n][7], t [n][6], w [6] -> grad [n_params], loss.  BF16 tensor-core kernels, FP32 accumulation. */
+int ceos_sur_gradient(void* handle, int n, const float* x, const float* t, const float* w, float* grad,
+                      double* loss);
+/* Adam training, mini-batches of `batch` from a seeded per-epoch shuffle, learning rate decaying
+ * geometrically lr0 -> lr1; loss_hist [epochs]. */
+int ceos_sur_train(void* handle, int n, const float* x, const float* t, const float* w, int epochs, int batch,
+                   double lr0, double lr1, unsigned seed, double* loss_hist);
+/* C6 [n][6], vf [n] (host) -> S [n][6], material tangent [n][36], out_of_range [n] (any may be NULL). */
+int ceos_sur_evaluate(void* handle, int n, const double* C6, const double* vf, double* S, double* Cm,
+                      int* out_of_range);
+/* Device material step for an external-material element loop: F [9][ldF] (point q = gp*n_elem+e),
+ * vf [n_elem] -> Cauchy stress and spatial tangent into state[(v*8+gp)*ld + e] (FP32 when
+ * state_f32), flags [8*n_elem] = 1 outside the training box.  All device pointers. */
+int ceos_sur_material_device(void* handle, int n_elem, const double* F, long long ldF, const double* vf,
+                             void* state, int state_f32, long long ld, int* flags, void* stream);
+int ceos_sur_message(void* handle, char* msg, int msg_len);
+void ceos_sur_destroy(void* handle);
+
 /* ---- Batched FE^2 micro problems (no reference counterpart: CEOS solves one RVE at a time,
  * MultiScale/ModMultiscaleAnalysis.f90:445-470) ------------------------------------------------
  * n_rve periodic RVEs, RVE r a unit cube of n_cells[r]^3 Hexa8 cells with one cylindrical fibre
@@ -171,6 +226,11 @@ int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int max_newton,
                    int* newton_iters, int* cg_iters);
 /* First load step of every RVE = 1/n_sub of Fbar - I (default 1: the full load at once). */
 int ceos_fe2_set_increments(void* handle, int n_sub);
+/* allow != 0: an RVE that cannot converge gets NaN in P and A and newton_iters -1, and
+ * ceos_fe2_solve returns 2 after finishing the others (default 0: the solve fails). */
+int ceos_fe2_set_allow_failures(void* handle, int allow);
+/* New nominal fibre volume fractions vf [n_rve] for the same RVE sizes (cell moduli recomputed). */
+int ceos_fe2_set_fractions(void* handle, const double* vf);
 /* Description of the last failure of ceos_fe2_solve (empty when none). */
 int ceos_fe2_message(void* handle, char* msg, int msg_len);
 void ceos_fe2_destroy(void* handle);
