@@ -64,7 +64,9 @@ struct Fe2 {
     int* d_fmap = nullptr;      // [3*n_nodes] global reduced dof or -1
     int* d_col = nullptr;       // [nnz] 0-based column of the upper CSR
     int* d_rcol = nullptr;      // [nnz] column as RVE-local reduced dof, -1 on the fixed node
-    float* d_kf = nullptr;      // [nnz] FP32 copy of the CSR values
+    int* d_gcoord = nullptr;    // [n_nodes] grid coordinates of each node in its RVE (i | j<<8 | k<<16)
+    int* d_rve_of_blk = nullptr;  // [n_red/3] RVE of each independent node
+    float* d_kell = nullptr;    // [81 n_red] periodic ELL copy of T^T K T (FP32), slot-major per RVE
     int* d_order = nullptr;     // RVEs by decreasing size
     int* d_queue = nullptr;     // work-queue counter
     double* d_Fbar = nullptr;   // [n_rve*9] row-major
@@ -88,7 +90,7 @@ struct Fe2 {
     ~Fe2() {
         void* p[] = {d_node_off, d_red_off, d_ncell, d_rve_of_node, d_fmap, d_col, d_order, d_queue, d_Fbar, d_w,
                      d_u, d_rhs, d_dx, d_r64, d_y64, d_minv, d_rnorm, d_cg_iters, d_active, d_P, d_A, d_nn, d_Z, d_M, d_X9,
-                     d_rve_of_elem, d_fail, d_op, d_wc, d_eta, d_rcol, d_kf};
+                     d_rve_of_elem, d_fail, d_op, d_wc, d_eta, d_rcol, d_gcoord, d_rve_of_blk, d_kell};
         for (void* q : p)
             if (q) cudaFree(q);
         if (loop) ceos_destroy(loop);
@@ -128,31 +130,57 @@ __global__ void fold_kernel(int n_dof, const int* fmap, const double* f, double*
     if (q >= 0) atomicAdd(out + q, sgn * f[i]);
 }
 
-// Block-Jacobi: per independent node, the sum of the diagonal 3x3 blocks of the nodes mapped to
-// it (nodes n cells apart never share an element, so no off-diagonal block couples them).
-__global__ void diag_blocks_kernel(int n_nodes, const long long* rs, const int* nup, const double* K, const int* fmap,
-                                   double* acc /* [n_red/3][9] FP64 */) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= n_nodes) return;
-    const int q = fmap[3 * a];
-    if (q < 0) return;
-    const long long r0 = rs[a];
-    const int m = nup[a];
-    const long long r1 = r0 + 3 + 3LL * m, r2 = r1 + 2 + 3LL * m;
-    const double k00 = K[r0], k01 = K[r0 + 1], k02 = K[r0 + 2], k11 = K[r1], k12 = K[r1 + 1], k22 = K[r2];
-    double* b = acc + 3 * (size_t)q;  // q is a multiple of 3: block index q/3 -> offset 9*(q/3) = 3q
-    atomicAdd(b + 0, k00); atomicAdd(b + 1, k01); atomicAdd(b + 2, k02);
-    atomicAdd(b + 3, k01); atomicAdd(b + 4, k11); atomicAdd(b + 5, k12);
-    atomicAdd(b + 6, k02); atomicAdd(b + 7, k12); atomicAdd(b + 8, k22);
+// Periodic ELL copy of T^T K T: reduced row r (independent node ind = r/3 + 1, component r%3) of
+// an n^3 RVE couples with the 27 periodic neighbours of its node, so its entries sit in 81 slots
+// (neighbour offset nb = (di+1)*9 + (dj+1)*3 + (dk+1), column component dc): value of slot s of
+// row r at kell[81 q0 + s m + r] (m reduced dofs of the RVE, q0 its first).  The fold adds every
+// upper CSR entry (R, C) of the union mesh and its transpose; the offset comes from the nodes'
+// unwrapped grid coordinates (nodes of one element differ by at most one cell per axis), so it is
+// right for every n >= 2.
+__global__ void fold_ell_kernel(int n_dof, const long long* rs, const int* nup, const int* col0, const double* K,
+                                const int* fmap, const int* rve_of_node, const int* red_off, const int* gcoord,
+                                float* kell) {
+    const int lane = threadIdx.x & 31;
+    const int R = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (R >= n_dof) return;
+    const int r = fmap[R];
+    if (r < 0) return;  // warp-uniform: the fixed independent node
+    const int a = R / 3, k = R - 3 * a, m = nup[a];
+    const long long start = rs[a] + (k == 0 ? 0LL : (k == 1 ? 3LL + 3LL * m : 5LL + 6LL * m));
+    const int len = (3 - k) + 3 * m;
+    const int rve = rve_of_node[a], q0 = red_off[rve], mr = red_off[rve + 1] - q0;
+    float* base = kell + 81LL * q0;
+    const int ga = gcoord[a];
+    for (int t = lane; t < len; t += 32) {
+        const int C = col0[start + t];
+        const int c = fmap[C];
+        if (c < 0) continue;
+        const int b = C / 3, gb = gcoord[b];
+        const int di = (gb & 255) - (ga & 255), dj = ((gb >> 8) & 255) - ((ga >> 8) & 255),
+                  dk = (gb >> 16) - (ga >> 16);
+        const int nb = (di + 1) * 9 + (dj + 1) * 3 + (dk + 1);
+        const float v = (float)K[start + t];
+        atomicAdd(base + (size_t)(nb * 3 + (C - 3 * b)) * mr + (r - q0), v);
+        if (C != R) atomicAdd(base + (size_t)((26 - nb) * 3 + k) * mr + (c - q0), v);
+    }
 }
 
-// SPD block-Jacobi preconditioner: the inverse of each positive definite nodal block; a block
-// that is not positive definite (compressed stiff fibre, negative geometric stiffness) falls back
-// to the inverse of its |diagonal|, so the preconditioner stays symmetric positive definite.
-__global__ void invert_blocks_kernel(int n_blk, const double* acc, float* minv) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= n_blk) return;
-    const double* A = acc + 9 * (size_t)b;
+// SPD block-Jacobi preconditioner from the ELL self blocks (offset nb = 13): the inverse of each
+// positive definite nodal block; a block that is not positive definite (compressed stiff fibre,
+// negative geometric stiffness) falls back to the inverse of its |diagonal|, so the
+// preconditioner stays symmetric positive definite.
+__global__ void invert_blocks_kernel(int n_blk, const int* rve_of_blk, const int* red_off, const float* kell,
+                                     float* minv) {
+    const int bq = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bq >= n_blk) return;
+    const int rve = rve_of_blk[bq], q0 = red_off[rve], m = red_off[rve + 1] - q0;
+    const int r0 = 3 * bq - q0;
+    const float* base = kell + 81LL * q0;
+    double A[9];
+    for (int dr = 0; dr < 3; ++dr)
+        for (int dc = 0; dc < 3; ++dc) A[3 * dr + dc] = base[(size_t)(13 * 3 + dc) * m + r0 + dr];
+    for (int i = 0; i < 3; ++i)  // symmetrise the FP32 sums
+        for (int j = i + 1; j < 3; ++j) A[3 * i + j] = A[3 * j + i] = 0.5 * (A[3 * i + j] + A[3 * j + i]);
     double c[9];
     c[0] = A[4] * A[8] - A[5] * A[7];
     c[1] = A[2] * A[7] - A[1] * A[8];
@@ -166,23 +194,18 @@ __global__ void invert_blocks_kernel(int n_blk, const double* acc, float* minv) 
     const double det = A[0] * c[0] + A[1] * c[3] + A[2] * c[6];
     // leading principal minors, relative to the diagonal products
     const bool pd = A[0] > 0.0 && c[8] > 1e-6 * A[0] * A[4] && det > 1e-6 * A[0] * A[4] * A[8];
+    float* M = minv + 9 * (size_t)bq;
     if (pd) {
         const double r = 1.0 / det;
-        for (int k = 0; k < 9; ++k) minv[9 * (size_t)b + k] = (float)(c[k] * r);
+        for (int q = 0; q < 9; ++q) M[q] = (float)(c[q] * r);
     } else {
         const double amax = fmax(fabs(A[0]), fmax(fabs(A[4]), fabs(A[8])));
         const double fl = amax > 0.0 ? 1e-6 * amax : 1.0;
-        for (int k = 0; k < 9; ++k) minv[9 * (size_t)b + k] = 0.f;
-        minv[9 * (size_t)b + 0] = (float)(1.0 / fmax(fabs(A[0]), fl));
-        minv[9 * (size_t)b + 4] = (float)(1.0 / fmax(fabs(A[4]), fl));
-        minv[9 * (size_t)b + 8] = (float)(1.0 / fmax(fabs(A[8]), fl));
+        for (int q = 0; q < 9; ++q) M[q] = 0.f;
+        M[0] = (float)(1.0 / fmax(fabs(A[0]), fl));
+        M[4] = (float)(1.0 / fmax(fabs(A[4]), fl));
+        M[8] = (float)(1.0 / fmax(fabs(A[8]), fl));
     }
-}
-
-// FP32 copy of the CSR values for the inner iterations
-__global__ void to_f32_kernel(long long n, const double* a, float* b) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n) b[i] = (float)a[i];
 }
 
 // per-RVE Euclidean norm of a reduced vector (one CTA per RVE)
@@ -249,7 +272,8 @@ struct SolveArgs {
     const int* nup;
     const int* rcol;       // [nnz] column mapped to the RVE-local reduced dof, or -1
     const double* K;       // upper CSR values (FP64), refinement residuals
-    const float* Kf;       // the same values in FP32, inner iterations
+    const float* kell;     // periodic ELL copy in FP32, inner iterations
+    const int* ncell;      // [n_rve] cells per side
     const float* minv;     // SPD block-Jacobi inverse per independent node
     int nrhs;              // right-hand sides solved one after another
     const double* rhs;     // [nrhs][n_red]
@@ -322,6 +346,30 @@ __device__ void rve_spmv_red(int row0, int nrow, int q0, const int* fmap, const 
     }
 }
 
+// y = T^T K T x over one RVE from its periodic ELL copy: thread per reduced row, the 27 neighbour
+// nodes from the row's grid position (no index arrays, no atomics), slot-major coalesced values.
+__device__ __forceinline__ void ell_spmv(int m, int n, const float* __restrict__ kell, const float* x, float* y) {
+    const int nn = n * n;
+    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+        const int ind = r / 3 + 1;
+        const int i0 = ind % n, j0 = (ind / n) % n, k0 = ind / nn;
+        float acc = 0.f;
+#pragma unroll
+        for (int nb = 0; nb < 27; ++nb) {
+            int ii = i0 + nb / 9 - 1, jj = j0 + (nb / 3) % 3 - 1, kk = k0 + nb % 3 - 1;
+            ii += ii < 0 ? n : (ii >= n ? -n : 0);
+            jj += jj < 0 ? n : (jj >= n ? -n : 0);
+            kk += kk < 0 ? n : (kk >= n ? -n : 0);
+            const int ind2 = kk * nn + jj * n + ii;
+            if (ind2 == 0) continue;  // the fixed independent node
+            const int b = 3 * (ind2 - 1);
+            acc += __ldg(kell + (size_t)(nb * 3) * m + r) * x[b] + __ldg(kell + (size_t)(nb * 3 + 1) * m + r) * x[b + 1] +
+                   __ldg(kell + (size_t)(nb * 3 + 2) * m + r) * x[b + 2];
+        }
+        y[r] = acc;
+    }
+}
+
 __device__ __forceinline__ void apply_block(const float* Mb, const float r[3], float z[3]) {
     z[0] = Mb[0] * r[0] + Mb[1] * r[1] + Mb[2] * r[2];
     z[1] = Mb[3] * r[0] + Mb[4] * r[1] + Mb[5] * r[2];
@@ -348,6 +396,8 @@ __global__ void __launch_bounds__(kSolveThreads) fe2_minres_kernel(SolveArgs A) 
         const int q0 = A.red_off[rve], m = A.red_off[rve + 1] - q0, nb3 = m / 3;
         if (!A.active[rve]) continue;  // x of RVEs not solving is left as it is
         const float* Mr = A.minv + 3 * (size_t)q0;  // block of independent node j at Mr + 9 j
+        const float* kell = A.kell + 81LL * q0;
+        const int ncell = A.ncell[rve];
         // shared views: FP32 inner phase [xs][bufA][bufB][bufC][v][wa][wb] (m each);
         // FP64 refinement phase [xd][yd] (m each) over the same bytes
         float* xs = reinterpret_cast<float*>(smem);
@@ -402,9 +452,9 @@ __global__ void __launch_bounds__(kSolveThreads) fe2_minres_kernel(SolveArgs A) 
                 while (it < A.max_inner && beta > 0.f) {
                     // v = y / beta;  y = K_red v - (beta/oldb) r1
                     const float s = 1.f / beta;
-                    for (int i = tid; i < m; i += bs) { v[i] = s * y[i]; y[i] = 0.f; }
+                    for (int i = tid; i < m; i += bs) v[i] = s * y[i];
                     __syncthreads();
-                    rve_spmv_red<float, float>(dof0, nf, q0, A.fmap, A.rs, A.nup, A.rcol, A.Kf, v, y);
+                    ell_spmv(m, ncell, kell, v, y);
                     __syncthreads();
                     const float f1 = it > 0 ? beta / oldb : 0.f;
                     float al = 0.f;
@@ -587,7 +637,8 @@ int run_solver(Fe2* f, int nrhs, const double* rhs, double* x, int max_inner, in
     a.nup = h->d_nup;
     a.rcol = f->d_rcol;
     a.K = h->d_kval;
-    a.Kf = f->d_kf;
+    a.kell = f->d_kell;
+    a.ncell = f->d_ncell;
     a.minv = f->d_minv;
     a.nrhs = nrhs;
     a.rhs = rhs;
@@ -616,14 +667,12 @@ int assemble(Fe2* f) {
     fold_kernel<<<(nd + 255) / 256, 256, 0, h->stream>>>(nd, f->d_fmap, h->d_fint, f->d_rhs, -1.0);
     CKF(cudaGetLastError());
     const int n_blk = f->n_red / 3;
-    double* acc = f->d_y64;  // FP64 block accumulator: 9 n_red/3 doubles (d_y64 holds max(3 n_nodes, 3 n_red))
-    CKF(cudaMemsetAsync(acc, 0, sizeof(double) * 9 * (size_t)n_blk, h->stream));
-    diag_blocks_kernel<<<(f->n_nodes + 255) / 256, 256, 0, h->stream>>>(f->n_nodes, h->d_rs, h->d_nup, h->d_kval,
-                                                                        f->d_fmap, acc);
+    CKF(cudaMemsetAsync(f->d_kell, 0, sizeof(float) * 81 * (size_t)f->n_red, h->stream));
+    fold_ell_kernel<<<(unsigned)(((long long)nd * 32 + 255) / 256), 256, 0, h->stream>>>(
+        nd, h->d_rs, h->d_nup, f->d_col, h->d_kval, f->d_fmap, f->d_rve_of_node, f->d_red_off, f->d_gcoord, f->d_kell);
     CKF(cudaGetLastError());
-    invert_blocks_kernel<<<(n_blk + 255) / 256, 256, 0, h->stream>>>(n_blk, acc, f->d_minv);
-    CKF(cudaGetLastError());
-    to_f32_kernel<<<(unsigned)((f->nnz + 255) / 256), 256, 0, h->stream>>>(f->nnz, h->d_kval, f->d_kf);
+    invert_blocks_kernel<<<(n_blk + 255) / 256, 256, 0, h->stream>>>(n_blk, f->d_rve_of_blk, f->d_red_off, f->d_kell,
+                                                                      f->d_minv);
     CKF(cudaGetLastError());
     return 0;
 }
@@ -659,7 +708,7 @@ extern "C" int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, 
     f->vf_nominal.assign(vf, vf + n_rve);
     // ---- union mesh: RVE r = unit cube, n^3 cells; fibre along z through the centre ----
     std::vector<double> X;
-    std::vector<int> conn, fmap_host;
+    std::vector<int> conn, fmap_host, gcoord;
     std::vector<double> eparams;  // [n_elem][2] (Mu, Lambda) of each cell
     const double mu_f = mu_matrix * stiff_ratio;
     f->node_off.assign(n_rve + 1, 0);
@@ -682,6 +731,7 @@ extern "C" int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, 
                     X.push_back((double)i / n);
                     X.push_back((double)j / n);
                     X.push_back((double)k / n);
+                    gcoord.push_back(i | (j << 8) | (k << 16));
                     const int ind = (k % n) * n * n + (j % n) * n + (i % n);  // independent node
                     for (int d = 0; d < 3; ++d) fmap_host.push_back(ind == 0 ? -1 : f->red_off[r] + 3 * (ind - 1) + d);
                 }
@@ -746,7 +796,12 @@ extern "C" int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, 
     if (e == cudaSuccess) e = up((void**)&f->d_fmap, fmap_host.data(), sizeof(int) * nd);
     if (e == cudaSuccess) e = up((void**)&f->d_col, col.data(), sizeof(int) * f->nnz);
     if (e == cudaSuccess) e = up((void**)&f->d_rcol, rcol.data(), sizeof(int) * f->nnz);
-    if (e == cudaSuccess) e = up((void**)&f->d_kf, nullptr, sizeof(float) * f->nnz);
+    std::vector<int> rve_of_blk(f->n_red / 3);
+    for (int r = 0; r < n_rve; ++r)
+        for (int q = f->red_off[r] / 3; q < f->red_off[r + 1] / 3; ++q) rve_of_blk[q] = r;
+    if (e == cudaSuccess) e = up((void**)&f->d_gcoord, gcoord.data(), sizeof(int) * gcoord.size());
+    if (e == cudaSuccess) e = up((void**)&f->d_rve_of_blk, rve_of_blk.data(), sizeof(int) * rve_of_blk.size());
+    if (e == cudaSuccess) e = up((void**)&f->d_kell, nullptr, sizeof(float) * 81 * (size_t)f->n_red);
     if (e == cudaSuccess) e = up((void**)&f->d_order, order.data(), sizeof(int) * n_rve);
     if (e == cudaSuccess) e = up((void**)&f->d_queue, nullptr, sizeof(int));
     if (e == cudaSuccess) e = up((void**)&f->d_Fbar, nullptr, sizeof(double) * 9 * n_rve);
