@@ -158,8 +158,15 @@ def run_fe2_surrogate(args):
                        "loss_first_epoch": float(hist[0]), "loss_last_epoch": float(hist[-1])}
     rec["validation_stress_error"] = FS.stress_errors(Pp[~fl], Pv[~fl])
     rec["validation_out_of_range"] = int(fl.sum())
+    print(json.dumps({"partial": "training", "training": rec["training"],
+                      "validation": rec["validation_stress_error"]}), file=sys.stderr, flush=True)
     small = FS.macro_compare(sur, nx=4)
-    rec["macro_4cube"] = {k: small[k] for k in ("direct", "surrogate", "stress_error_per_step")}
+    rec["macro_4cube"] = {k: small[k] for k in ("direct", "surrogate", "stress_error_per_step",
+                                                "constitutive_error_per_step")}
+    rec["speedup_4cube_in_range_steps"] = [d / s for d, s, fb in zip(small["direct"]["step_s"], small["surrogate"]["step_s"],
+                                                                    small["surrogate"]["fallback_points"]) if fb == 0]
+    print(json.dumps({"partial": "4cube", "macro_4cube": rec["macro_4cube"],
+                      "speedup": rec["speedup_4cube_in_range_steps"]}), file=sys.stderr, flush=True)
     big = FS.macro_surrogate_run(sur, nx=32)
     evals = np.array(big["newton"]) + 1  # material evaluations per step
     st_b = big["stats"]
@@ -174,8 +181,7 @@ def run_fe2_surrogate(args):
     s32 = np.array(big["step_s"])
     rec["value"] = float(s32.mean()) if s32.size else None
     rec["speedup_32cube_estimated"] = float(np.mean(direct_est / s32)) if s32.size else None
-    rec["speedup_4cube_in_range_steps"] = [d / s for d, s, fb in zip(small["direct"]["step_s"], small["surrogate"]["step_s"],
-                                                                    small["surrogate"]["fallback_points"]) if fb == 0]
+
     rec["config"] = {"workload": "FE2 uniaxial stretch to 1.2 in 10 increments; macro 32^3 Hexa8 (262,144 GPs) and "
                                  "4^3 head-to-head; periodic fibre RVEs n=6, vf U[0.1,0.4], mu_f/mu_m=50, K/mu=100",
                      "surrogate": "MLP 7-128x4-1 softplus energy of (C, vf)"}

@@ -17,6 +17,8 @@ def _setup():
     L.ceos_fe2_set_increments.argtypes = [P, I]
     L.ceos_fe2_set_allow_failures.argtypes = [P, I]
     L.ceos_fe2_set_fractions.argtypes = [P, P]
+    L.ceos_fe2_set_warm_start.argtypes = [P, I]
+    L.ceos_fe2_set_solve_mask.argtypes = [P, P]
     L.ceos_fe2_destroy.argtypes = [P]
     L.ceos_fe2_destroy.restype = None
     return L
@@ -65,6 +67,15 @@ class BatchedRVE:
         """RVEs that cannot converge come back as NaN (and newton_iters -1) instead of raising."""
         _check(lib().ceos_fe2_set_allow_failures(self._h, 1 if allow else 0))
         self._allow = allow
+
+    def set_warm_start(self, on=True):
+        """Continue every RVE from its last converged state (macro load path) on the next solves."""
+        _check(lib().ceos_fe2_set_warm_start(self._h, 1 if on else 0))
+
+    def set_solve_mask(self, mask=None):
+        """Solve only the RVEs where mask != 0 on the next solves (None: all)."""
+        self._mask = None if mask is None else np.ascontiguousarray(mask, dtype=np.int32)
+        _check(lib().ceos_fe2_set_solve_mask(self._h, _ptr(self._mask) if self._mask is not None else None))
 
     def set_fractions(self, vf):
         """New fibre volume fractions for the same RVE sizes (mesh and pattern kept)."""

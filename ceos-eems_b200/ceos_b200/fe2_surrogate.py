@@ -50,9 +50,13 @@ def rve_stresses(F, vf, n_cells=6, batch=4096, tangent=False, **rve_args):
                   "minres_total": minres}
 
 
-def fit(F, vf, P, epochs=150, batch=2048, lr0=3e-3, lr1=2e-5, seed=0, s_C=0.15, vf0=0.25, s_vf=0.15):
+def fit(F, vf, P, epochs=150, batch=2048, lr0=3e-3, lr1=2e-5, seed=0, s_C=0.15, vf0=0.25, s_vf=0.15,
+        relative=0.2):
     """Train a surrogate on the finite samples; the training box of the range check is the
-    component-wise extent of the training inputs.  Returns (Surrogate, loss history, seconds)."""
+    component-wise extent of the training inputs.  relative > 0 weights every sample by
+    1 / (|S|^2 / mean|S|^2 + relative), so the loss measures relative stress error (small stresses of
+    nearly isochoric states count as much as the large volumetric ones) with a floor.
+    Returns (Surrogate, loss history, seconds)."""
     ok = np.all(np.isfinite(P.reshape(len(P), -1)), axis=1)
     F, vf, P = F[ok], vf[ok], P[ok]
     C6 = voigt_C(F)
@@ -65,8 +69,13 @@ def fit(F, vf, P, epochs=150, batch=2048, lr0=3e-3, lr1=2e-5, seed=0, s_C=0.15, 
     x = sur.inputs(C6, vf)
     sur.set_scaling(s_C, s_W, vf0, s_vf, lo=x.min(axis=0), hi=x.max(axis=0))
     t, w = training_targets(F, P, s_C, s_W)
+    sw = None
+    if relative > 0:
+        tn = np.sum(w * t * t, axis=1)
+        sw = 1.0 / (tn / tn.mean() + relative)
+        sw /= sw.mean()
     t0 = time.perf_counter()
-    hist = sur.train(x, t, w, epochs, batch, lr0, lr1, seed)
+    hist = sur.train(x, t, w, epochs, batch, lr0, lr1, seed, sw=sw)
     return sur, hist, time.perf_counter() - t0
 
 
@@ -95,25 +104,44 @@ def macro_compare(sur, nx=4, n_cells=6, stretch=1.2, n_steps=10, seed=11, tol=1e
     and with RVE solves at every point; per-step wall times, Newton iterations, fallback points
     and the relative error of the Gauss-point first Piola stresses of the surrogate run against
     the direct run after every step."""
+    import sys
+
+    from . import CeosError
     from . import macro as M
     vf = np.random.default_rng(seed).uniform(0.1, 0.4, nx ** 3)
-    res, fields = {}, {}
+    res, fields, const_err = {}, {}, []
     for mode in ("direct", "surrogate"):
         m = M.MacroFE2(nx, vf, n_cells=n_cells, surrogate=sur)
         L = m.X[:, 0].max() - m.X[:, 0].min()
-        times, its, fbs, Ps = [], [], [], []
+        times, its, fbs, Ps, failed = [], [], [], [], None
         for k in range(1, n_steps + 1):
             fb0 = m.stats["fallback_points"]
             t0 = time.perf_counter()
-            its.append(m.newton_step((stretch - 1.0) * L * k / n_steps, mode, tol))
+            try:
+                its.append(m.newton_step((stretch - 1.0) * L * k / n_steps, mode, tol))
+            except CeosError as e:  # an RVE (or the macro Newton) that cannot converge ends this run
+                failed = {"step": k, "stretch": 1.0 + (stretch - 1.0) * k / n_steps, "reason": str(e)}
+                print(f"macro {mode}: step {k} failed: {e}", file=sys.stderr, flush=True)
+                break
             times.append(time.perf_counter() - t0)
             fbs.append(m.stats["fallback_points"] - fb0)
             Ps.append(m.gp_first_piola())
-        res[mode] = {"step_s": times, "newton": its, "fallback_points": fbs, "stats": dict(m.stats)}
+            if mode == "direct":  # the surrogate's response at the direct run's own deformation
+                Fq = m._gp_F_host()
+                Pq, flq = predict_P(sur, Fq, np.tile(vf, 8))
+                const_err.append({"in_range": stress_errors(Pq[~flq], Ps[-1][~flq])["aggregate"] if (~flq).any()
+                                  else None, "out_of_range_points": int(flq.sum())})
+            print(f"macro {mode}: step {k} {times[-1]:.2f}s newton {its[-1]} fallback {fbs[-1]}", file=sys.stderr,
+                  flush=True)
+        res[mode] = {"step_s": times, "newton": its, "fallback_points": fbs, "stats": dict(m.stats),
+                     "failed": failed}
         fields[mode] = Ps
         m.close()
+    # field error: the two macro solutions differ wherever the constitutive responses do
     res["stress_error_per_step"] = [stress_errors(Psu, Pd)["aggregate"]
                                     for Pd, Psu in zip(fields["direct"], fields["surrogate"])]
+    # constitutive error: surrogate against RVE solves at the same deformation gradients
+    res["constitutive_error_per_step"] = const_err
     return res
 
 

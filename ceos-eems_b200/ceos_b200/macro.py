@@ -120,10 +120,22 @@ class MacroFE2:
         F = F if idx is None else F[torch.as_tensor(idx, device=self.dev)]
         return F.cpu().numpy().reshape(-1, 3, 3)
 
-    def _rve_response(self, idx, batch):
-        """Solve the RVEs of points idx (Fbar from the current F) and write sigma, D into the state."""
-        Fh = self._gp_F_host(idx)
+    def _point_batch(self):
+        """One RVE per macro Gauss point (point q = gp * n_elem + e), warm-started: every RVE follows
+        its point's macro load path from solve to solve."""
+        if self._direct is None:
+            vf = np.tile(self.vf_elem, 8)
+            self._direct = FE2.BatchedRVE(np.full(self.n_gp, self.n_cells, np.int32), vf, **self.rve_args)
+            self._direct.set_warm_start(True)
+        return self._direct
+
+    def _rve_response(self, idx, batch, all_points=False):
+        """Solve the RVEs of points idx (Fbar from the current F) and write sigma, D into the state;
+        with all_points the batch holds every point and idx selects the rows written."""
+        Fh = self._gp_F_host(None if all_points else idx)
         out = batch.solve(Fh, tangent=True)
+        if all_points:
+            Fh, out = Fh[idx], {"P": out["P"][idx], "A": out["A"][idx]}
         sig, D = spatial_from_PA(Fh, out["P"], out["A"])
         vals = np.ascontiguousarray(np.concatenate([sig, D], axis=1))
         q = np.ascontiguousarray(idx, np.int32)
@@ -131,6 +143,8 @@ class MacroFE2:
         return out
 
     max_fallback = None  # cap on points sent back to RVE solves in one material step
+    point_batch_limit = 16384  # meshes up to this many points keep one warm RVE per point
+    residual_floor = 1e-6      # Newton stops at |R| <= residual_floor |f_int| whatever the relative drop
 
     def material(self, mode):
         t0 = time.perf_counter()
@@ -148,15 +162,21 @@ class MacroFE2:
                 raise FallbackLimit(f"{idx.size} of {self.n_gp} points outside the training box")
             if idx.size:
                 n_fb = idx.size
-                vf = self.vf_elem[idx % self.n_elem]
-                b = FE2.BatchedRVE(np.full(idx.size, self.n_cells, np.int32), vf, **self.rve_args)
-                self._rve_response(idx, b)
-                b.close()
+                if self.n_gp <= self.point_batch_limit:
+                    b = self._point_batch()
+                    mask = np.zeros(self.n_gp, np.int32)
+                    mask[idx] = 1
+                    b.set_solve_mask(mask)
+                    self._rve_response(idx, b, all_points=True)
+                else:  # large meshes: a batch of just these points, each from the undeformed state
+                    b = FE2.BatchedRVE(np.full(idx.size, self.n_cells, np.int32), self.vf_elem[idx % self.n_elem],
+                                       **self.rve_args)
+                    self._rve_response(idx, b)
+                    b.close()
         else:
-            if self._direct is None:
-                vf = np.tile(self.vf_elem, 8)  # point q = gp * n_elem + e
-                self._direct = FE2.BatchedRVE(np.full(self.n_gp, self.n_cells, np.int32), vf, **self.rve_args)
-            self._rve_response(np.arange(self.n_gp), self._direct)
+            b = self._point_batch()
+            b.set_solve_mask(None)
+            self._rve_response(np.arange(self.n_gp), b, all_points=True)
             n_fb = self.n_gp
         torch.cuda.synchronize(self.dev)
         self.stats["material_s"] += time.perf_counter() - t0
@@ -164,9 +184,33 @@ class MacroFE2:
         return n_fb
 
     # ---- Newton -------------------------------------------------------------------------------
+    def predict(self, ux_target):
+        """Initial guess of a load step: the homogeneous uniaxial field u = (e x, -e y/2, -e z/2) for
+        the first step, then secant extrapolation of the last two converged fields (prescribing the
+        loaded face alone would put the whole increment into one element layer)."""
+        Xd = torch.as_tensor(self.X, device=self.dev)
+        L = float(self.X[:, 0].max() - self.X[:, 0].min())
+        if self._hist is None:
+            e = ux_target / L
+            U = torch.stack([e * Xd[:, 0], -0.5 * e * Xd[:, 1], -0.5 * e * Xd[:, 2]], dim=1).reshape(-1)
+        else:
+            (u1, U1), (u0, U0) = self._hist
+            U = U1 + (U1 - U0) * ((ux_target - u1) / (u1 - u0)) if u1 != u0 else U1.clone()
+        U[self.mask.bool()] = 0.0
+        self.U.copy_(U)
+
+    _hist = None  # (ux, U) of the last two converged steps
+
     def newton_step(self, ux_target, mode, tol=1e-6, max_newton=15, pcg_tol=1e-8):
         """One load step: x1-face displacement ux_target; returns Newton iterations."""
+        self.predict(ux_target)
         self.U[torch.as_tensor(self.presc, device=self.dev)] = ux_target
+        it = self._newton(mode, tol, max_newton, pcg_tol)
+        prev = self._hist[0] if self._hist is not None else (0.0, torch.zeros_like(self.U))
+        self._hist = ((ux_target, self.U.clone()), prev)
+        return it
+
+    def _newton(self, mode, tol, max_newton, pcg_tol):
         r0 = None
         for it in range(max_newton + 1):
             self.material(mode)
@@ -181,7 +225,9 @@ class MacroFE2:
             self.rhs[self.mask.bool()] = 0.0
             rn = float(torch.linalg.vector_norm(self.rhs))
             r0 = rn if r0 is None else r0
-            if rn <= tol * max(r0, 1e-300) or rn <= 1e-12:
+            # floor: the stresses of a surrogate point carry FP32 round-off (about 1e-7 relative)
+            floor = self.residual_floor * float(torch.linalg.vector_norm(self.fint))
+            if rn <= tol * max(r0, 1e-300) or rn <= max(floor, 1e-12):
                 return it
             if it == max_newton:
                 break

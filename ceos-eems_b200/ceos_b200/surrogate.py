@@ -20,8 +20,8 @@ def _setup():
     L.ceos_sur_set_params.argtypes = [P, P]
     L.ceos_sur_get_params.argtypes = [P, P]
     L.ceos_sur_set_scaling.argtypes = [P, P, P, P]
-    L.ceos_sur_gradient.argtypes = [P, I, P, P, P, P, P]
-    L.ceos_sur_train.argtypes = [P, I, P, P, P, I, I, D, D, C.c_uint, P]
+    L.ceos_sur_gradient.argtypes = [P, I, P, P, P, P, P, P]
+    L.ceos_sur_train.argtypes = [P, I, P, P, P, P, I, I, D, D, C.c_uint, P]
     L.ceos_sur_evaluate.argtypes = [P, I, P, P, P, P, P]
     L.ceos_sur_material_device.argtypes = [P, I, P, C.c_longlong, P, P, I, C.c_longlong, P, P]
     L.ceos_sur_message.argtypes = [P, C.c_char_p, I]
@@ -88,22 +88,25 @@ class Surrogate:
         x[:, 6] = (np.asarray(vf) - vf0) / s_vf
         return x
 
-    def gradient(self, x, t, w):
+    def gradient(self, x, t, w, sw=None):
         x = np.ascontiguousarray(x, np.float32)
         t = np.ascontiguousarray(t, np.float32)
         w = np.ascontiguousarray(w, np.float32)
+        sw = None if sw is None else np.ascontiguousarray(sw, np.float32)
         g = np.zeros(self.n_params, np.float32)
         loss = C.c_double()
-        self._check(self._L.ceos_sur_gradient(self._h, x.shape[0], _ptr(x), _ptr(t), _ptr(w), _ptr(g), C.byref(loss)))
+        self._check(self._L.ceos_sur_gradient(self._h, x.shape[0], _ptr(x), _ptr(t), _ptr(w), _ptr(sw), _ptr(g),
+                                              C.byref(loss)))
         return loss.value, g
 
-    def train(self, x, t, w, epochs, batch, lr0=2e-3, lr1=2e-5, seed=0):
+    def train(self, x, t, w, epochs, batch, lr0=2e-3, lr1=2e-5, seed=0, sw=None):
         x = np.ascontiguousarray(x, np.float32)
         t = np.ascontiguousarray(t, np.float32)
         w = np.ascontiguousarray(w, np.float32)
+        sw = None if sw is None else np.ascontiguousarray(sw, np.float32)
         hist = np.zeros(epochs)
-        self._check(self._L.ceos_sur_train(self._h, x.shape[0], _ptr(x), _ptr(t), _ptr(w), epochs, batch, lr0, lr1,
-                                           seed, _ptr(hist)))
+        self._check(self._L.ceos_sur_train(self._h, x.shape[0], _ptr(x), _ptr(t), _ptr(w), _ptr(sw), epochs, batch,
+                                           lr0, lr1, seed, _ptr(hist)))
         return hist
 
     def evaluate(self, C6, vf):

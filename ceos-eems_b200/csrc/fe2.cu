@@ -44,6 +44,9 @@ struct Fe2 {
     int n_sub = 1;                       // macro load sub-increments per solve
     double mu_m = 1.0, mu_f = 50.0, k_over_mu = 100.0;
     int allow_failures = 0;              // 1: RVEs that cannot converge are reported, not fatal
+    int warm = 0;                        // 1: continue every RVE from its last converged state
+    std::vector<double> F_prev;          // [n_rve][9] Fbar of the last converged state (warm start)
+    std::vector<int> solve_mask;         // [n_rve] 0: RVE skipped by the next solves (empty: all solved)
     std::vector<int> n;                  // cells per side of each RVE
     std::vector<double> vf_nominal, vf_actual;
     Handle* loop = nullptr;              // element loop over the union of all RVE meshes
@@ -845,11 +848,19 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
     cudaStream_t s = h->stream;
     const int nr = f->n_rve;
     CKF(cudaSetDevice(f->device));
-    CKF(cudaMemsetAsync(f->d_w, 0, sizeof(double) * f->n_red, s));
-    CKF(cudaMemsetAsync(f->d_wc, 0, sizeof(double) * f->n_red, s));
+    // Start of every RVE's path: Fbar = I with zero fluctuation, or (warm start) the Fbar and
+    // fluctuation of its last converged state, which d_w and d_wc both hold after a solve.
+    if (!f->warm || f->F_prev.size() != 9 * (size_t)nr) {
+        f->F_prev.assign(9 * (size_t)nr, 0.0);
+        for (int r = 0; r < nr; ++r) f->F_prev[9 * (size_t)r] = f->F_prev[9 * (size_t)r + 4] = f->F_prev[9 * (size_t)r + 8] = 1.0;
+        CKF(cudaMemsetAsync(f->d_w, 0, sizeof(double) * f->n_red, s));
+        CKF(cudaMemsetAsync(f->d_wc, 0, sizeof(double) * f->n_red, s));
+    }
+    const std::vector<double> Fp = f->F_prev;
     CKF(cudaMemsetAsync(f->d_dx, 0, sizeof(double) * f->n_red, s));
     const bool verbose = std::getenv("CEOS_FE2_VERBOSE") != nullptr;
-    // Per-RVE load continuation Fbar(a) = I + a (Fbar - I): each RVE advances from its last
+    // Per-RVE load continuation Fbar(a) = Fp + a (Fbar - Fp) (Fp = I, or the last converged Fbar
+    // with a warm start): each RVE advances from its last
     // converged level a_done towards 1 in steps da (1/n_sub at first).  A Newton step is accepted
     // when no element folds and the residual grows by at most kGrowth (never beyond kDiverge x the
     // residual at the start of the load step); otherwise it is halved
@@ -867,6 +878,11 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
     std::vector<double> a_done(nr, 0.0), da(nr, 1.0 / std::max(1, f->n_sub)), a_try(nr), r0(nr, 1.0), racc(nr, 0.0),
         rn(nr), eta(nr, 1.0), Fs(9 * (size_t)nr);
     for (int r = 0; r < nr; ++r) a_try[r] = std::min(1.0, da[r]);
+    for (int r = 0; r < nr && !f->solve_mask.empty(); ++r)
+        if (!f->solve_mask[r]) {  // skipped: stays at its current state
+            phase[r] = kDone;
+            a_try[r] = 0.0;
+        }
     // every round advances each active RVE by one Newton step, halving, cut-back or load step;
     // a generous cap bounds the whole solve (RVEs still running then fail)
     const int max_rounds = 4 * (max_newton + kMaxHalvings + 2) * (kMaxCutbacks + 2 * std::max(1, f->n_sub) + 8);
@@ -874,8 +890,8 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
     for (int round = 0; round < max_rounds && !all_done; ++round) {
         for (int r = 0; r < nr; ++r)
             for (int k = 0; k < 9; ++k) {
-                const double I = (k % 4 == 0) ? 1.0 : 0.0;
-                Fs[9 * (size_t)r + k] = I + a_try[r] * (Fbar[9 * (size_t)r + k] - I);
+                const size_t i = 9 * (size_t)r + k;
+                Fs[i] = Fp[i] + a_try[r] * (Fbar[i] - Fp[i]);
             }
         CKF(cudaMemcpyAsync(f->d_Fbar, Fs.data(), sizeof(double) * Fs.size(), cudaMemcpyHostToDevice, s));
         int rc = assemble(f);
@@ -988,11 +1004,16 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
             if (phase[r] == kNewton) phase[r] = kFailed;  // the last assembly is not at their converged state
     }
     int n_failed = 0;
-    for (int r = 0; r < nr; ++r)
+    for (int r = 0; r < nr; ++r) {
         if (phase[r] == kFailed) {
             ++n_failed;
             its[r] = -1;
         }
+        for (int k = 0; k < 9; ++k) {  // the converged state each RVE ends in (partial for failed ones)
+            const size_t i = 9 * (size_t)r + k;
+            f->F_prev[i] = Fp[i] + a_done[r] * (Fbar[i] - Fp[i]);
+        }
+    }
     if (n_failed) f->msg = std::to_string(n_failed) + " RVE(s) did not converge";
     // converged state: K and f_int of the last assembly
     homogenize_kernel<<<f->n_rve, 256, 0, s>>>(f->n_rve, f->d_node_off, h->d_X, h->d_fint, f->d_P, 1.0);
@@ -1040,6 +1061,26 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
     return n_failed ? 2 : 0;
 }
 
+// Warm start: every solve continues each RVE from the Fbar and fluctuation of its last converged
+// state (an FE^2 macro iteration moves Fbar a little; the RVE follows the macro load path instead
+// of restarting from the undeformed state).
+extern "C" int ceos_fe2_set_warm_start(void* handle, int on) {
+    Fe2* f = static_cast<Fe2*>(handle);
+    if (!f) return CEOS_E_ARG;
+    f->warm = on ? 1 : 0;
+    return 0;
+}
+
+// mask [n_rve]: 0 = leave the RVE out of the next solves (it keeps its state; its P and A are those
+// of that state); NULL = solve all.
+extern "C" int ceos_fe2_set_solve_mask(void* handle, const int* mask) {
+    Fe2* f = static_cast<Fe2*>(handle);
+    if (!f) return CEOS_E_ARG;
+    if (mask) f->solve_mask.assign(mask, mask + f->n_rve);
+    else f->solve_mask.clear();
+    return 0;
+}
+
 // Report RVEs that cannot converge (P and A set to NaN, newton_iters -1, return value 2) instead of
 // failing the whole solve.
 extern "C" int ceos_fe2_set_allow_failures(void* handle, int allow) {
@@ -1072,6 +1113,7 @@ extern "C" int ceos_fe2_set_fractions(void* handle, const double* vf) {
         f->vf_nominal[r] = vf[r];
         f->vf_actual[r] = phisum / ((double)n * n * n);
     }
+    f->F_prev.clear();  // new RVEs: the next solve starts from the undeformed state
     return ceos_update_params(f->loop, eparams.data());
 }
 

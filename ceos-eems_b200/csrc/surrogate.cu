@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(128) layer_gemm_kernel(LayerArgs A) {
 // loss and u = dL/dg (rounded into the padded BF16 tangent input).
 // ---------------------------------------------------------------------------------------------
 __global__ void seed_kernel(int n, const float* theta, const float* Z0, const float* G0, const float* T,
-                            const float* w6, float inv_n, __nv_bfloat16* U0, double* loss) {
+                            const float* w6, const float* sw, float inv_n, __nv_bfloat16* U0, double* loss) {
     __shared__ float W1s[kIn * kH];  // transposed: [k][m]
     __shared__ double red[8];
     for (int i = threadIdx.x; i < kIn * kH; i += blockDim.x) {
@@ -181,6 +181,7 @@ __global__ void seed_kernel(int n, const float* theta, const float* Z0, const fl
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double part = 0.0;
     if (s < n) {
+        const float ws = sw[s];  // per-sample weight
         float gk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         for (int m = 0; m < kH; ++m) {
             const float d = sigmoid_f(Z0[(size_t)s * kH + m]) * G0[(size_t)s * kH + m];
@@ -192,8 +193,8 @@ __global__ void seed_kernel(int n, const float* theta, const float* Z0, const fl
             float u = 0.f;
             if (k < 6) {
                 const float r = gk[k] - T[(size_t)s * 6 + k];
-                part += (double)w6[k] * r * r;
-                u = 2.f * w6[k] * r * inv_n;
+                part += (double)ws * w6[k] * r * r;
+                u = 2.f * ws * w6[k] * r * inv_n;
             }
             U0[(size_t)s * kInPad + k] = __float2bfloat16_rn(u);
         }
@@ -317,13 +318,14 @@ __global__ void step_kernel(int* ctr, float lr0, float decay, float b1, float b2
     hp[1] = 1.f / (1.f - powf(b1, (float)t));
     hp[2] = 1.f / (1.f - powf(b2, (float)t));
 }
-__global__ void gather_rows_kernel(int nb, int* ctr, const int* idx, const float* Xall, const float* Tall, float* X,
-                                   float* T) {
+__global__ void gather_rows_kernel(int nb, int* ctr, const int* idx, const float* Xall, const float* Tall,
+                                   const float* Swall, float* X, float* T, float* Sw) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nb) return;
     const int r = idx[ctr[1] + i];
     for (int k = 0; k < kIn; ++k) X[(size_t)i * kIn + k] = Xall[(size_t)r * kIn + k];
     for (int k = 0; k < 6; ++k) T[(size_t)i * 6 + k] = Tall[(size_t)r * 6 + k];
+    Sw[i] = Swall[r];
 }
 __global__ void advance_kernel(int* ctr, int nb) { ctr[1] += nb; }
 
@@ -653,11 +655,12 @@ struct Sur {
     // workspace for batches of cap samples
     __nv_bfloat16 *X0 = nullptr, *U0 = nullptr, *Hb = nullptr, *Hd = nullptr, *Db = nullptr, *Ab = nullptr;
     float *Z = nullptr, *Zd = nullptr, *G = nullptr, *Hd4 = nullptr, *T = nullptr, *w6 = nullptr;
+    float* Sw = nullptr;  // [cap] per-sample loss weights of the current batch
     __nv_bfloat16** Aptr = nullptr;  // device array of the 4 a_l pointers
     double* loss = nullptr;
     int* ctr = nullptr;  // [2] Adam step, batch offset
     ~Sur() {
-        void* p[] = {theta, grad, m1, m2, hp, WT, box, Wb1, Wb, WbT, X0, U0, Hb, Hd, Db, Ab, Z, Zd, G, Hd4, T, w6, Aptr, loss, ctr};
+        void* p[] = {theta, grad, m1, m2, hp, WT, box, Wb1, Wb, WbT, X0, U0, Hb, Hd, Db, Ab, Z, Zd, G, Hd4, T, w6, Aptr, loss, ctr, Sw};
         for (void* q : p)
             if (q) cudaFree(q);
         if (stream) cudaStreamDestroy(stream);
@@ -740,7 +743,8 @@ int grad_device(Sur* s, int n, const float* dX) {
         L.last = 0;
         layer_gemm_kernel<kH, kBwd><<<nb, 128, 0, st>>>(L);
     }
-    seed_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, s->theta, s->Z, s->G, s->T, s->w6, 1.f / n, s->U0, s->loss);
+    seed_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, s->theta, s->Z, s->G, s->T, s->w6, s->Sw, 1.f / n, s->U0,
+                                                 s->loss);
     // forward tangent
     for (int l = 0; l < 4; ++l) {
         L.Z = s->Z + l * BH;
@@ -831,6 +835,7 @@ extern "C" int ceos_sur_create(int batch_max, int device, void** handle) {
     al((void**)&s->G, sizeof(float) * 4 * BH);
     al((void**)&s->Hd4, sizeof(float) * BH);
     al((void**)&s->T, sizeof(float) * 6 * (size_t)s->cap);
+    al((void**)&s->Sw, sizeof(float) * (size_t)s->cap);
     al((void**)&s->w6, sizeof(float) * 6);
     al((void**)&s->Aptr, sizeof(void*) * 4);
     al((void**)&s->loss, sizeof(double));
@@ -887,9 +892,9 @@ extern "C" int ceos_sur_set_scaling(void* handle, const double* scales, const do
 }
 
 // Gradient of the Sobolev loss over one batch (x [n][7] normalised inputs, t [n][6] targets of
-// de/dx, w [6] weights): grad [n_params] and the loss.  Used to check the kernels.
-extern "C" int ceos_sur_gradient(void* handle, int n, const float* x, const float* t, const float* w, float* grad,
-                                 double* loss) {
+// de/dx, w [6] component weights, sw [n] sample weights or NULL): grad [n_params] and the loss.
+extern "C" int ceos_sur_gradient(void* handle, int n, const float* x, const float* t, const float* w, const float* sw,
+                                 float* grad, double* loss) {
     Sur* s = static_cast<Sur*>(handle);
     if (!s || n < 1 || n > s->cap || !x || !t || !w || !grad) return CEOS_E_ARG;
     CKS(cudaSetDevice(s->device));
@@ -898,6 +903,11 @@ extern "C" int ceos_sur_gradient(void* handle, int n, const float* x, const floa
     cudaMemcpyAsync(dX, x, sizeof(float) * kIn * (size_t)n, cudaMemcpyHostToDevice, s->stream);
     cudaMemcpyAsync(s->T, t, sizeof(float) * 6 * (size_t)n, cudaMemcpyHostToDevice, s->stream);
     cudaMemcpyAsync(s->w6, w, sizeof(float) * 6, cudaMemcpyHostToDevice, s->stream);
+    {
+        std::vector<float> ones;
+        if (!sw) ones.assign(n, 1.f);
+        cudaMemcpy(s->Sw, sw ? sw : ones.data(), sizeof(float) * (size_t)n, cudaMemcpyHostToDevice);
+    }
     cudaMemsetAsync(s->grad, 0, sizeof(float) * kNParams, s->stream);
     cudaMemsetAsync(s->loss, 0, sizeof(double), s->stream);
     int rc = grad_device(s, n, dX);
@@ -913,13 +923,14 @@ extern "C" int ceos_sur_gradient(void* handle, int n, const float* x, const floa
     return 0;
 }
 
-// Adam training on n samples (x [n][7], t [n][6], w [6]): epochs passes over a per-epoch
+// Adam training on n samples (x [n][7], t [n][6], w [6], sample weights sw [n] or NULL): epochs
+// passes over a per-epoch
 // shuffle (seeded), mini-batches of `batch` (<= capacity; the last partial batch of an epoch is
 // dropped), learning rate decaying geometrically from lr0 to lr1 over all steps.  One step
 // (batch gather, the four passes, weight gradients, Adam) is captured once into a CUDA graph
 // and replayed.  loss_hist[epochs] = mean batch loss of each epoch.
-extern "C" int ceos_sur_train(void* handle, int n, const float* x, const float* t, const float* w, int epochs,
-                              int batch, double lr0, double lr1, unsigned seed, double* loss_hist) {
+extern "C" int ceos_sur_train(void* handle, int n, const float* x, const float* t, const float* w, const float* sw,
+                              int epochs, int batch, double lr0, double lr1, unsigned seed, double* loss_hist) {
     Sur* s = static_cast<Sur*>(handle);
     if (!s || !x || !t || !w || epochs < 1 || batch < 1 || batch > s->cap || n < batch || !(lr0 > 0) || !(lr1 > 0))
         return CEOS_E_ARG;
@@ -927,7 +938,7 @@ extern "C" int ceos_sur_train(void* handle, int n, const float* x, const float* 
     cudaStream_t st = s->stream;
     const int nbatch = n / batch;
     const double decay = std::pow(lr1 / lr0, 1.0 / std::max(1, epochs * nbatch - 1));
-    float *dXall = nullptr, *dTall = nullptr, *dX = nullptr;
+    float *dXall = nullptr, *dTall = nullptr, *dX = nullptr, *dSw = nullptr;
     int* didx = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -939,18 +950,25 @@ extern "C" int ceos_sur_train(void* handle, int n, const float* x, const float* 
     if (cudaMalloc(&dXall, sizeof(float) * kIn * (size_t)n) != cudaSuccess ||
         cudaMalloc(&dTall, sizeof(float) * 6 * (size_t)n) != cudaSuccess ||
         cudaMalloc(&dX, sizeof(float) * kIn * (size_t)batch) != cudaSuccess ||
-        cudaMalloc(&didx, sizeof(int) * (size_t)n) != cudaSuccess)
+        cudaMalloc(&didx, sizeof(int) * (size_t)n) != cudaSuccess ||
+        cudaMalloc(&dSw, sizeof(float) * (size_t)n) != cudaSuccess)
         fail("training buffers");
     if (!rc) {
         cudaMemcpyAsync(dXall, x, sizeof(float) * kIn * (size_t)n, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(dTall, t, sizeof(float) * 6 * (size_t)n, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(s->w6, w, sizeof(float) * 6, cudaMemcpyHostToDevice, st);
+        {
+            std::vector<float> ones;
+            if (!sw) ones.assign(n, 1.f);
+            cudaMemcpy(dSw, sw ? sw : ones.data(), sizeof(float) * (size_t)n, cudaMemcpyHostToDevice);
+        }
         // capture one step
         if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             fail("begin capture");
         } else {
             step_kernel<<<1, 1, 0, st>>>(s->ctr, (float)lr0, (float)decay, 0.9f, 0.999f, s->hp);
-            gather_rows_kernel<<<(batch + 255) / 256, 256, 0, st>>>(batch, s->ctr, didx, dXall, dTall, dX, s->T);
+            gather_rows_kernel<<<(batch + 255) / 256, 256, 0, st>>>(batch, s->ctr, didx, dXall, dTall, dSw, dX, s->T,
+                                                                    s->Sw);
             const int r2 = grad_device(s, batch, dX);
             adam_kernel<<<(kNParams + 255) / 256, 256, 0, st>>>(s->theta, s->grad, s->m1, s->m2, s->hp, 0.9f, 0.999f,
                                                                 1e-8f, s->Wb1, s->Wb, s->WbT);
@@ -983,6 +1001,7 @@ extern "C" int ceos_sur_train(void* handle, int n, const float* x, const float* 
         if (cudaStreamSynchronize(st) != cudaSuccess) fail("transpose");
     }
     cudaFree(didx);
+    cudaFree(dSw);
     cudaFree(dX);
     cudaFree(dTall);
     cudaFree(dXall);

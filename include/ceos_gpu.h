@@ -184,14 +184,15 @@ int ceos_sur_set_params(void* handle, const float* theta);
 int ceos_sur_get_params(void* handle, float* theta);
 /* scales = [s_C, s_W, vf0, s_vf]; lo/hi [7]: training box of x for the range check (may be NULL). */
 int ceos_sur_set_scaling(void* handle, const double* scales, const double* lo, const double* hi);
-/* Gradient of L = (1/n) sum w_k (de/dx_k - t_k)^2 (k < 6) over one batch (n <= batch_max):
- * x [n][7], t [n][6], w [6] -> grad [n_params], loss.  BF16 tensor-core kernels, FP32 accumulation. */
-int ceos_sur_gradient(void* handle, int n, const float* x, const float* t, const float* w, float* grad,
-                      double* loss);
+/* Gradient of L = (1/n) sum_s sw_s sum_k w_k (de/dx_k - t_k)^2 (k < 6) over one batch (n <=
+ * batch_max): x [n][7], t [n][6], w [6], sw [n] (NULL: all 1) -> grad [n_params], loss.  BF16
+ * tensor-core kernels, FP32 accumulation. */
+int ceos_sur_gradient(void* handle, int n, const float* x, const float* t, const float* w, const float* sw,
+                      float* grad, double* loss);
 /* Adam training, mini-batches of `batch` from a seeded per-epoch shuffle, learning rate decaying
- * geometrically lr0 -> lr1; loss_hist [epochs]. */
-int ceos_sur_train(void* handle, int n, const float* x, const float* t, const float* w, int epochs, int batch,
-                   double lr0, double lr1, unsigned seed, double* loss_hist);
+ * geometrically lr0 -> lr1; sample weights sw [n] or NULL; loss_hist [epochs]. */
+int ceos_sur_train(void* handle, int n, const float* x, const float* t, const float* w, const float* sw, int epochs,
+                   int batch, double lr0, double lr1, unsigned seed, double* loss_hist);
 /* C6 [n][6], vf [n] (host) -> S [n][6], material tangent [n][36], out_of_range [n] (any may be NULL). */
 int ceos_sur_evaluate(void* handle, int n, const double* C6, const double* vf, double* S, double* Cm,
                       int* out_of_range);
@@ -229,6 +230,12 @@ int ceos_fe2_set_increments(void* handle, int n_sub);
 /* allow != 0: an RVE that cannot converge gets NaN in P and A and newton_iters -1, and
  * ceos_fe2_solve returns 2 after finishing the others (default 0: the solve fails). */
 int ceos_fe2_set_allow_failures(void* handle, int allow);
+/* on != 0: each solve continues every RVE from the Fbar and fluctuation of its last converged
+ * state (along the macro load path) instead of from Fbar = I (default 0). */
+int ceos_fe2_set_warm_start(void* handle, int on);
+/* mask [n_rve]: 0 leaves an RVE out of the next solves (it keeps its state; P and A are those of
+ * that state); NULL solves all (default). */
+int ceos_fe2_set_solve_mask(void* handle, const int* mask);
 /* New nominal fibre volume fractions vf [n_rve] for the same RVE sizes (cell moduli recomputed). */
 int ceos_fe2_set_fractions(void* handle, const double* vf);
 /* Description of the last failure of ceos_fe2_solve (empty when none). */

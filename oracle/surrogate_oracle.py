@@ -100,10 +100,11 @@ def energy_grad_hess(theta, x):
     return e, g, Hs
 
 
-def loss_and_grad(theta, x, t, w, bf=False):
+def loss_and_grad(theta, x, t, w, bf=False, sw=None):
     """Sobolev loss on the first 6 input derivatives and its parameter gradient.
 
-    x [N,7], t [N,6] targets of g[:, :6], w [6] component weights.  Returns (L, dL/dtheta).
+    x [N,7], t [N,6] targets of g[:, :6], w [6] component weights, sw [N] sample weights (None: 1).
+    Returns (L, dL/dtheta).
     bf=True rounds to bfloat16 where the GPU does: the BF16 weight copies of W1..W4, the padded
     inputs x and seeds u, the activations h_l, tangents hdot_l, adjoints delta_l (l >= 2) and a_l.
     """
@@ -136,9 +137,10 @@ def loss_and_grad(theta, x, t, w, bf=False):
     d1 = S[0] * G[0]                      # FP32 on the GPU, feeds the stress
     g = d1 @ W[0]                         # master FP32 W1
     res = g[:, :6] - t
-    L = float(np.sum(w * res * res) / N)
+    swv = np.ones(N) if sw is None else np.asarray(sw, np.float64)
+    L = float(np.sum(swv[:, None] * w * res * res) / N)
     u = np.zeros((N, NIN))
-    u[:, :6] = 2.0 * w * res / N
+    u[:, :6] = 2.0 * swv[:, None] * w * res / N
     U0 = r(u)
     # forward tangent
     Zd, Hd = [], []

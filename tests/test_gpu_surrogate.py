@@ -25,10 +25,11 @@ def test_training_gradient_matches_oracle():
     s = SG.Surrogate(batch_max=1024)
     s.set_params(th)
     th32 = s.params().astype(np.float64)
-    loss, g = s.gradient(x, t, w)
+    sw = np.random.default_rng(4).uniform(0.2, 3.0, len(x)).astype(np.float32)  # per-sample weights
+    loss, g = s.gradient(x, t, w, sw)
     Lb, gb = SO.loss_and_grad(th32, x.astype(np.float32).astype(np.float64), t.astype(np.float32).astype(np.float64),
-                              w, bf=True)
-    L64, g64 = SO.loss_and_grad(th32, x, t, w)
+                              w, bf=True, sw=sw)
+    L64, g64 = SO.loss_and_grad(th32, x, t, w, sw=sw)
     assert abs(loss - Lb) <= 1e-4 * Lb
     assert np.linalg.norm(g - gb) <= 2e-3 * np.linalg.norm(gb)
     assert np.linalg.norm(g - g64) <= 3e-2 * np.linalg.norm(g64)

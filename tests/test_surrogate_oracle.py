@@ -17,14 +17,15 @@ def _setup(seed=0, n=5):
 
 def test_loss_gradient_matches_finite_differences():
     th, x, t, w, rng = _setup()
-    _, gr = SO.loss_and_grad(th, x, t, w)
+    sw = rng.uniform(0.5, 2.0, len(x))
+    _, gr = SO.loss_and_grad(th, x, t, w, sw=sw)
     idx = rng.choice(SO.N_PARAMS, 40, replace=False)
     h = 1e-6
     fd = []
     for i in idx:
         e = np.zeros(SO.N_PARAMS)
         e[i] = h
-        fd.append((SO.loss_and_grad(th + e, x, t, w)[0] - SO.loss_and_grad(th - e, x, t, w)[0]) / (2 * h))
+        fd.append((SO.loss_and_grad(th + e, x, t, w, sw=sw)[0] - SO.loss_and_grad(th - e, x, t, w, sw=sw)[0]) / (2 * h))
     assert np.abs(np.array(fd) - gr[idx]).max() <= 1e-5 * np.abs(gr[idx]).max()
 
 
