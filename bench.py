@@ -143,7 +143,7 @@ def run_fe2_surrogate(args):
     from ceos_b200 import fe2_surrogate as FS
     rec = {"metric": "FE2 macro step time: surrogate vs direct", "unit": "s", "higher_is_better": False,
            "dtype": "bf16 training / f32 inference / f64 RVE", "data": "synthetic"}
-    F, vf = FS.sample_points(args.n_train, seed=1)
+    F, vf = FS.sample_points(args.n_train, seed=1, small_fraction=0.5)
     P, _, st = FS.rve_stresses(F, vf, batch=8192)
     Fv, vfv = FS.sample_points(4096, seed=99)
     Pv, _, _ = FS.rve_stresses(Fv, vfv, batch=4096)

@@ -12,9 +12,15 @@ from . import fe2 as FE2
 from .surrogate import Surrogate, init_params, training_targets, voigt_C
 
 
-def sample_points(n, seed, amp=0.15, vf_range=(0.1, 0.4)):
+def sample_points(n, seed, amp=0.15, vf_range=(0.1, 0.4), small_fraction=0.0):
+    """F = I + G, G_ij uniform in [-amp, amp] (det F > 0); a share small_fraction of the points has its
+    G scaled by a uniform factor in [0, 1] (more small strains, same range); vf uniform."""
     F = FE2.sample_macro_F(n, seed=seed, amp=amp)
-    vf = np.random.default_rng(seed + 7919).uniform(vf_range[0], vf_range[1], n)
+    rng = np.random.default_rng(seed + 7919)
+    vf = rng.uniform(vf_range[0], vf_range[1], n)
+    k = int(round(small_fraction * n))
+    if k:
+        F[:k] = np.eye(3) + rng.uniform(0.0, 1.0, (k, 1, 1)) * (F[:k] - np.eye(3))
     return F, vf
 
 
@@ -76,6 +82,7 @@ def fit(F, vf, P, epochs=150, batch=2048, lr0=3e-3, lr1=2e-5, seed=0, s_C=0.15, 
         sw /= sw.mean()
     t0 = time.perf_counter()
     hist = sur.train(x, t, w, epochs, batch, lr0, lr1, seed, sw=sw)
+    sur.set_reference(float(vf.min()), float(vf.max()))
     return sur, hist, time.perf_counter() - t0
 
 
@@ -147,7 +154,9 @@ def macro_compare(sur, nx=4, n_cells=6, stretch=1.2, n_steps=10, seed=11, tol=1e
 
 def macro_surrogate_run(sur, nx=32, stretch=1.2, n_steps=10, seed=12, tol=1e-6, max_fallback=4096, n_cells=6):
     """Surrogate macro run on nx^3 cells; stops at a step that would send more than max_fallback
-    points to RVE solves (FallbackLimit).  Returns per-step times and the steps done."""
+    points to RVE solves (FallbackLimit) or whose RVE or macro solve fails.  Returns per-step times
+    and the steps done."""
+    from . import CeosError
     from . import macro as M
     vf = np.random.default_rng(seed).uniform(0.1, 0.4, nx ** 3)
     m = M.MacroFE2(nx, vf, n_cells=n_cells, surrogate=sur)
@@ -159,7 +168,7 @@ def macro_surrogate_run(sur, nx=32, stretch=1.2, n_steps=10, seed=12, tol=1e-6, 
         t0 = time.perf_counter()
         try:
             its.append(m.newton_step((stretch - 1.0) * L * k / n_steps, "surrogate", tol))
-        except M.FallbackLimit as e:
+        except (M.FallbackLimit, CeosError) as e:
             stopped = {"step": k, "reason": str(e)}
             break
         times.append(time.perf_counter() - t0)

@@ -144,7 +144,7 @@ class MacroFE2:
 
     max_fallback = None  # cap on points sent back to RVE solves in one material step
     point_batch_limit = 16384  # meshes up to this many points keep one warm RVE per point
-    residual_floor = 1e-6      # Newton stops at |R| <= residual_floor |f_int| whatever the relative drop
+    stall_level = 1e-4         # relative residual below which a stalled Newton iteration counts as converged
 
     def material(self, mode):
         t0 = time.perf_counter()
@@ -158,6 +158,11 @@ class MacroFE2:
                                      self.ld, C.c_void_p(self.flags.data_ptr()))
             torch.cuda.synchronize(self.dev)
             idx = torch.nonzero(self.flags).flatten().cpu().numpy()
+            # a point sent to RVE solves stays there for the rest of the load step, so that no point
+            # switches between the two responses from one Newton iteration to the next
+            if self._sticky is not None:
+                idx = np.union1d(idx, self._sticky)
+            self._sticky = idx
             if self.max_fallback is not None and idx.size > self.max_fallback:
                 raise FallbackLimit(f"{idx.size} of {self.n_gp} points outside the training box")
             if idx.size:
@@ -200,10 +205,12 @@ class MacroFE2:
         self.U.copy_(U)
 
     _hist = None  # (ux, U) of the last two converged steps
+    _sticky = None  # points on RVE solves in the current load step
 
     def newton_step(self, ux_target, mode, tol=1e-6, max_newton=15, pcg_tol=1e-8):
         """One load step: x1-face displacement ux_target; returns Newton iterations."""
         self.predict(ux_target)
+        self._sticky = None
         self.U[torch.as_tensor(self.presc, device=self.dev)] = ux_target
         it = self._newton(mode, tol, max_newton, pcg_tol)
         prev = self._hist[0] if self._hist is not None else (0.0, torch.zeros_like(self.U))
@@ -212,6 +219,7 @@ class MacroFE2:
 
     def _newton(self, mode, tol, max_newton, pcg_tol):
         r0 = None
+        rprev = float("inf")
         for it in range(max_newton + 1):
             self.material(mode)
             t0 = time.perf_counter()
@@ -225,9 +233,12 @@ class MacroFE2:
             self.rhs[self.mask.bool()] = 0.0
             rn = float(torch.linalg.vector_norm(self.rhs))
             r0 = rn if r0 is None else r0
-            # floor: the stresses of a surrogate point carry FP32 round-off (about 1e-7 relative)
-            floor = self.residual_floor * float(torch.linalg.vector_norm(self.fint))
-            if rn <= tol * max(r0, 1e-300) or rn <= max(floor, 1e-12):
+            # The stresses of a surrogate point carry FP32 round-off (about 1e-7 relative), which puts a
+            # floor under the residual: below stall_level * r0, an iteration that no longer halves the
+            # residual has reached it and ends the step.
+            stalled = it >= 2 and rn <= self.stall_level * r0 and rn > 0.5 * rprev
+            rprev = rn
+            if rn <= tol * max(r0, 1e-300) or rn <= 1e-12 or stalled:
                 return it
             if it == max_newton:
                 break

@@ -24,6 +24,7 @@ def _setup():
     L.ceos_sur_train.argtypes = [P, I, P, P, P, P, I, I, D, D, C.c_uint, P]
     L.ceos_sur_evaluate.argtypes = [P, I, P, P, P, P, P]
     L.ceos_sur_material_device.argtypes = [P, I, P, C.c_longlong, P, P, I, C.c_longlong, P, P]
+    L.ceos_sur_set_reference.argtypes = [P, D, D]
     L.ceos_sur_message.argtypes = [P, C.c_char_p, I]
     L.ceos_sur_destroy.argtypes = [P]
     L.ceos_sur_destroy.restype = None
@@ -80,6 +81,10 @@ class Surrogate:
         hi = None if hi is None else np.ascontiguousarray(hi, np.float64)
         self._check(self._L.ceos_sur_set_scaling(self._h, _ptr(self.scales), _ptr(lo) if lo is not None else None,
                                                  _ptr(hi) if hi is not None else None))
+
+    def set_reference(self, vf_lo, vf_hi):
+        """Make C = I stress-free for vf in [vf_lo, vf_hi] (subtracts the tabulated S(I, vf))."""
+        self._check(self._L.ceos_sur_set_reference(self._h, vf_lo, vf_hi))
 
     def inputs(self, C6, vf):
         s_C, _, vf0, s_vf = self.scales

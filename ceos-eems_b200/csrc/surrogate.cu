@@ -46,6 +46,7 @@ __host__ __device__ constexpr int layer_b(int l) { return l == 0 ? oB1 : oB2 + (
 static_assert(layer_w(3) == oW4 && layer_b(3) == oB4, "parameter layout");
 constexpr int kTileN = 32;   // samples per CTA of the layer GEMMs
 constexpr int kChunk = 256;  // samples per CTA of the weight-gradient GEMMs
+constexpr int kTab = 513;    // vf grid of the reference-state stress table
 
 __device__ __forceinline__ float softplus_f(float z) { return fmaxf(z, 0.f) + log1pf(expf(-fabsf(z))); }
 __device__ __forceinline__ float sigmoid_f(float z) { return 0.5f * (1.f + tanhf(0.5f * z)); }
@@ -383,6 +384,11 @@ struct InferArgs {
     int state_f32;
     long long ld;
     int n_elem;
+    // reference-state correction: S(C = I, vf) tabulated over [tab_lo, tab_hi] (n_tab rows of 6),
+    // subtracted from every stress so that the undeformed state is stress-free (nullable)
+    const double* s0tab;
+    int n_tab;
+    double tab_lo, tab_hi;
 };
 
 __global__ void __launch_bounds__(256) infer_kernel(InferArgs A) {
@@ -581,6 +587,14 @@ __global__ void __launch_bounds__(256) infer_kernel(InferArgs A) {
                 const double av[6] = {2, 2, 2, 1, 1, 1};
                 double S[6], Cm[6][6];
                 for (int a = 0; a < 6; ++a) S[a] = av[a] * (A.sW / A.sC) * Gs[tid * 8 + a];
+                if (A.s0tab) {  // W - S0(vf):(C - I)/2 keeps the energy form and the tangent
+                    const double v = A.vf[q % A.vf_mod];
+                    double tpos = (v - A.tab_lo) / (A.tab_hi - A.tab_lo) * (A.n_tab - 1);
+                    tpos = fmin(fmax(tpos, 0.0), (double)(A.n_tab - 1));
+                    const int i0 = min((int)tpos, A.n_tab - 2);
+                    const double w = tpos - i0;
+                    for (int a = 0; a < 6; ++a) S[a] -= (1.0 - w) * A.s0tab[6 * i0 + a] + w * A.s0tab[6 * (i0 + 1) + a];
+                }
                 for (int a = 0; a < 6; ++a)
                     for (int b = a; b < 6; ++b) {
                         const double v = av[a] * av[b] * (A.sW / ((double)A.sC * A.sC)) * Hs[tid * 36 + a * 6 + b];
@@ -650,6 +664,9 @@ struct Sur {
     // parameters
     float *theta = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr, *hp = nullptr, *WT = nullptr;
     float *box = nullptr;  // [14] lo, hi
+    double* s0tab = nullptr;  // [kTab][6] reference-state stress over the vf range (when s0_on)
+    int s0_on = 0;
+    double tab_lo = 0.0, tab_hi = 1.0;
     __nv_bfloat16 *Wb1 = nullptr, *Wb = nullptr, *WbT = nullptr;
     int step = 0;
     // workspace for batches of cap samples
@@ -660,7 +677,7 @@ struct Sur {
     double* loss = nullptr;
     int* ctr = nullptr;  // [2] Adam step, batch offset
     ~Sur() {
-        void* p[] = {theta, grad, m1, m2, hp, WT, box, Wb1, Wb, WbT, X0, U0, Hb, Hd, Db, Ab, Z, Zd, G, Hd4, T, w6, Aptr, loss, ctr, Sw};
+        void* p[] = {theta, grad, m1, m2, hp, WT, box, Wb1, Wb, WbT, X0, U0, Hb, Hd, Db, Ab, Z, Zd, G, Hd4, T, w6, Aptr, loss, ctr, Sw, s0tab};
         for (void* q : p)
             if (q) cudaFree(q);
         if (stream) cudaStreamDestroy(stream);
@@ -1018,6 +1035,12 @@ int launch_infer(Sur* s, InferArgs& a, cudaStream_t st) {
     a.svf = s->scales[3];
     a.lo = s->box;
     a.hi = s->box + kIn;
+    if (s->s0_on) {
+        a.s0tab = s->s0tab;
+        a.n_tab = kTab;
+        a.tab_lo = s->tab_lo;
+        a.tab_hi = s->tab_hi;
+    }
     CKS(cudaFuncSetAttribute(infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInferSmem));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
@@ -1062,6 +1085,29 @@ extern "C" int ceos_sur_evaluate(void* handle, int n, const double* C6, const do
     cudaFree(dC); cudaFree(dv); cudaFree(dS); cudaFree(dCm); cudaFree(dfl);
     if (rc) return rc;
     CKS(e);
+    return 0;
+}
+
+// Make the undeformed state stress-free: tabulate the network's S at C = I for vf in [vf_lo, vf_hi]
+// and subtract it (linearly interpolated in vf) from every later stress.  This subtracts a term
+// linear in C from the energy, so the tangent is unchanged.  Call again after training.
+extern "C" int ceos_sur_set_reference(void* handle, double vf_lo, double vf_hi) {
+    Sur* s = static_cast<Sur*>(handle);
+    if (!s || !(vf_hi > vf_lo)) return CEOS_E_ARG;
+    CKS(cudaSetDevice(s->device));
+    s->s0_on = 0;
+    std::vector<double> C6(6 * kTab, 0.0), vf(kTab), S0(6 * kTab);
+    for (int i = 0; i < kTab; ++i) {
+        C6[6 * i] = C6[6 * i + 1] = C6[6 * i + 2] = 1.0;
+        vf[i] = vf_lo + (vf_hi - vf_lo) * i / (kTab - 1);
+    }
+    int rc = ceos_sur_evaluate(handle, kTab, C6.data(), vf.data(), S0.data(), nullptr, nullptr);
+    if (rc) return rc;
+    if (!s->s0tab) CKS(cudaMalloc(&s->s0tab, sizeof(double) * 6 * kTab));
+    CKS(cudaMemcpy(s->s0tab, S0.data(), sizeof(double) * 6 * kTab, cudaMemcpyHostToDevice));
+    s->tab_lo = vf_lo;
+    s->tab_hi = vf_hi;
+    s->s0_on = 1;
     return 0;
 }
 

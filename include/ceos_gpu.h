@@ -201,6 +201,9 @@ int ceos_sur_evaluate(void* handle, int n, const double* C6, const double* vf, d
  * state_f32), flags [8*n_elem] = 1 outside the training box.  All device pointers. */
 int ceos_sur_material_device(void* handle, int n_elem, const double* F, long long ldF, const double* vf,
                              void* state, int state_f32, long long ld, int* flags, void* stream);
+/* Subtract the network's stress at C = I (tabulated over vf in [vf_lo, vf_hi]) from every later
+ * stress: the undeformed state becomes stress-free, the tangent is unchanged. */
+int ceos_sur_set_reference(void* handle, double vf_lo, double vf_hi);
 int ceos_sur_message(void* handle, char* msg, int msg_len);
 void ceos_sur_destroy(void* handle);
 

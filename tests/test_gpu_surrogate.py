@@ -91,3 +91,23 @@ def test_training_fits_analytic_energy():
     err = np.linalg.norm(Sp - S6[:2000], axis=1) / np.linalg.norm(S6[:2000], axis=1).mean()
     assert np.median(err) < 0.03
     s.close()
+
+
+def test_reference_state_is_stress_free_and_tangent_unchanged():
+    th, _, _, _ = _problem()
+    s = SG.Surrogate(batch_max=256)
+    s.set_params(th)
+    s.set_scaling(0.15, 2.0, 0.25, 0.15)
+    rng = np.random.default_rng(2)
+    vf = rng.uniform(0.1, 0.4, 50)
+    F = np.eye(3) + rng.uniform(-0.1, 0.1, (50, 3, 3))
+    S_a, C_a, _ = s.evaluate(SG.voigt_C(F), vf)
+    I6 = np.tile([1.0, 1.0, 1.0, 0.0, 0.0, 0.0], (50, 1))
+    S_I, _, _ = s.evaluate(I6, vf)
+    s.set_reference(0.1, 0.4)
+    S_b, C_b, _ = s.evaluate(SG.voigt_C(F), vf)
+    S_I2, _, _ = s.evaluate(I6, vf)
+    assert np.abs(S_I2).max() <= 1e-4 * np.abs(S_I).max()          # table interpolation in vf
+    np.testing.assert_array_equal(C_a, C_b)                           # the tangent is untouched
+    assert np.abs((S_a - S_b) - S_I).max() <= 1e-4 * np.abs(S_I).max()
+    s.close()
