@@ -9,7 +9,8 @@ Newton evaluation of the whole mesh through the C ABI (the work the reference do
 SolveConstitutiveModel + InternalForce + TangentStiffnessMatrix per iteration).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-  python bench.py --workload fe2-surrogate [--n-train 200000] [--epochs 800]
+  python bench.py --workload fe2-surrogate [--n-train 200000] [--epochs 2000]
+  python bench.py --workload fe2-batch [--n-rve 4096]
 
 The second form runs the learned-surrogate experiment instead (training data from the batched
 RVE solver, training, validation error, a 4^3 macro head-to-head of surrogate and direct FE^2,
@@ -138,6 +139,35 @@ def algorithmic_bytes(n_nodes, n_elem, n_gp, n_dof, nnz, nb=3):
     return nodes + connectivity + state + fint + kval
 
 
+def run_fe2_batch(args):
+    """Batched FE^2: n_rve periodic fibre RVEs of uneven size n in {6..12}, vf U[0.1, 0.4], F = I + G
+    with |G_ij| <= 0.15, solved to 1e-8 with homogenized P and the 9x9 tangent, one batch on the GPU."""
+    import torch
+    from ceos_b200 import fe2
+    n, vf = fe2.sample_rve_family(args.n_rve, seed=4)
+    Fb = fe2.sample_macro_F(args.n_rve, seed=5)
+    t0 = time.perf_counter()
+    b = fe2.BatchedRVE(n, vf)
+    t_create = time.perf_counter() - t0
+    b.set_allow_failures(True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = b.solve(Fb, tangent=True)
+    torch.cuda.synchronize()
+    t_solve = time.perf_counter() - t0
+    ok = ~out["failed"]
+    rec = {"metric": "RVE solves/s (P and 9x9 tangent)", "value": float(args.n_rve / t_solve), "unit": "RVE/s",
+           "higher_is_better": True, "n_gpus": 1, "dtype": "f64 element loop / f32 MINRES with f64 refinement",
+           "data": "synthetic", "solve_s": t_solve, "setup_s": t_create, "failed_rves": int((~ok).sum()),
+           "newton_iters_mean": float(out["newton_iters"][ok].mean()), "newton_iters_max": int(out["newton_iters"].max()),
+           "minres_iters_mean": float(out["cg_iters"][ok].mean()),
+           "elements": int(b.n_elem), "reduced_dofs": int(b.n_red),
+           "config": {"workload": f"batched FE2: {args.n_rve} periodic fibre RVEs, n U{{6..12}}, vf U[0.1,0.4], "
+                                  "mu_f/mu_m=50, K/mu=100, F = I + G, |G_ij| <= 0.15, tol 1e-8, P + tangent"}}
+    print(json.dumps(rec), flush=True)
+    b.close()
+
+
 def run_fe2_surrogate(args):
     """Learned surrogate against direct batched FE^2 (all on the GPU, no oracle)."""
     from ceos_b200 import fe2_surrogate as FS
@@ -197,12 +227,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="element-loop", choices=["element-loop", "fe2-surrogate"])
+    ap.add_argument("--workload", default="element-loop", choices=["element-loop", "fe2-surrogate", "fe2-batch"])
+    ap.add_argument("--n-rve", type=int, default=4096)
     ap.add_argument("--n-train", type=int, default=200000)
-    ap.add_argument("--epochs", type=int, default=800)
+    ap.add_argument("--epochs", type=int, default=2000)
     args = ap.parse_args()
     if args.workload == "fe2-surrogate":
         return run_fe2_surrogate(args)
+    if args.workload == "fe2-batch":
+        return run_fe2_batch(args)
     warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
