@@ -1090,14 +1090,17 @@ extern "C" int ceos_fe2_set_allow_failures(void* handle, int allow) {
     return 0;
 }
 
-// New fibre volume fractions for the same RVE sizes (cell moduli recomputed, mesh kept).
+// New fibre volume fractions for the same RVE sizes (cell moduli recomputed, mesh kept); RVEs whose
+// fraction changes restart from the undeformed state at the next solve.
 extern "C" int ceos_fe2_set_fractions(void* handle, const double* vf) {
     Fe2* f = static_cast<Fe2*>(handle);
     if (!f || !vf) return CEOS_E_ARG;
     std::vector<double> eparams;
     eparams.reserve(2 * (size_t)f->loop->n_elem);
+    std::vector<int> changed(f->n_rve, 0);
     for (int r = 0; r < f->n_rve; ++r) {
         const int n = f->n[r];
+        changed[r] = vf[r] != f->vf_nominal[r];
         const double rad2 = vf[r] / M_PI;
         double phisum = 0.0;
         for (int k = 0; k < n; ++k)
@@ -1113,7 +1116,17 @@ extern "C" int ceos_fe2_set_fractions(void* handle, const double* vf) {
         f->vf_nominal[r] = vf[r];
         f->vf_actual[r] = phisum / ((double)n * n * n);
     }
-    f->F_prev.clear();  // new RVEs: the next solve starts from the undeformed state
+    // RVEs with a new fraction restart from the undeformed state; the others keep their warm state
+    if (f->F_prev.size() == 9 * (size_t)f->n_rve) {
+        Handle* h = f->loop;
+        for (int r = 0; r < f->n_rve; ++r) {
+            if (!changed[r]) continue;
+            for (int k = 0; k < 9; ++k) f->F_prev[9 * (size_t)r + k] = (k % 4 == 0) ? 1.0 : 0.0;
+            const size_t q0 = f->red_off[r], m = f->red_off[r + 1] - f->red_off[r];
+            CKF(cudaMemsetAsync(f->d_w + q0, 0, sizeof(double) * m, h->stream));
+            CKF(cudaMemsetAsync(f->d_wc + q0, 0, sizeof(double) * m, h->stream));
+        }
+    }
     return ceos_update_params(f->loop, eparams.data());
 }
 

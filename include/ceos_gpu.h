@@ -239,7 +239,8 @@ int ceos_fe2_set_warm_start(void* handle, int on);
 /* mask [n_rve]: 0 leaves an RVE out of the next solves (it keeps its state; P and A are those of
  * that state); NULL solves all (default). */
 int ceos_fe2_set_solve_mask(void* handle, const int* mask);
-/* New nominal fibre volume fractions vf [n_rve] for the same RVE sizes (cell moduli recomputed). */
+/* New nominal fibre volume fractions vf [n_rve] for the same RVE sizes (cell moduli recomputed);
+ * RVEs whose fraction changes restart from the undeformed state, the others keep a warm state. */
 int ceos_fe2_set_fractions(void* handle, const double* vf);
 /* Description of the last failure of ceos_fe2_solve (empty when none). */
 int ceos_fe2_message(void* handle, char* msg, int msg_len);
