@@ -53,14 +53,13 @@ def spatial_from_PA(F, P, A):
 
 
 def uniaxial_bc(X):
-    """Face x=0 fixed in x, corner (0,0,0) pinned, u_z = 0 at corner (0,1,0) (no rigid rotation about
-    x), face x=1 prescribed in x.  Returns (fixed 0-based dofs, prescribed x1-face dofs)."""
+    """Uniaxial stretch with symmetry planes: u_x = 0 on x = 0, u_y = 0 on y = 0, u_z = 0 on z = 0, face
+    x = 1 prescribed in x.  The planes remove the rigid modes without a point constraint (a pinned
+    corner concentrates strain in its elements).  Returns (fixed 0-based dofs, prescribed dofs)."""
     f = meshgen.node_grid_index(X)
     fixed = set(3 * n for n in np.nonzero(f["x0"])[0])
-    c0 = np.nonzero(f["x0"] & f["y0"] & f["z0"])[0][0]
-    fixed.update(3 * c0 + d for d in range(3))
-    c1 = np.nonzero(f["x0"] & f["y1"] & f["z0"])[0][0]
-    fixed.add(3 * c1 + 2)
+    fixed.update(3 * n + 1 for n in np.nonzero(f["y0"])[0])
+    fixed.update(3 * n + 2 for n in np.nonzero(f["z0"])[0])
     presc = np.array([3 * n for n in np.nonzero(f["x1"])[0]], np.int64)
     return np.array(sorted(fixed), np.int64), presc
 
@@ -162,7 +161,7 @@ class MacroFE2:
         _check(self._L.ceos_state_scatter(self.loop.handle, len(q), _ptr(q), _ptr(vals), 27))
 
     _pool = None
-    pool_size = 2048
+    pool_size = 512
 
     def _rve_response(self, idx, batch, all_points=False):
         """Solve the RVEs of points idx (Fbar from the current F) and write sigma, D into the state;

@@ -1039,7 +1039,8 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
                                                                1.0);
             CKF(cudaGetLastError());
         }
-        std::vector<int> ones(f->n_rve, 1);
+        std::vector<int> ones(f->n_rve, 1);  // masked-out RVEs need no new tangent either
+        if (!f->solve_mask.empty()) ones = f->solve_mask;
         std::vector<double> eta_t(f->n_rve, 1e-8);
         CKF(cudaMemcpyAsync(f->d_active, ones.data(), sizeof(int) * f->n_rve, cudaMemcpyHostToDevice, s));
         CKF(cudaMemcpyAsync(f->d_eta, eta_t.data(), sizeof(double) * f->n_rve, cudaMemcpyHostToDevice, s));
@@ -1071,8 +1072,8 @@ extern "C" int ceos_fe2_set_warm_start(void* handle, int on) {
     return 0;
 }
 
-// mask [n_rve]: 0 = leave the RVE out of the next solves (it keeps its state; its P and A are those
-// of that state); NULL = solve all.
+// mask [n_rve]: 0 = leave the RVE out of the next solves (it keeps its state, P is that of the state,
+// its tangent rows are not recomputed); NULL = solve all.
 extern "C" int ceos_fe2_set_solve_mask(void* handle, const int* mask) {
     Fe2* f = static_cast<Fe2*>(handle);
     if (!f) return CEOS_E_ARG;

@@ -36,5 +36,6 @@ def test_uniaxial_bc_removes_rigid_motion():
     fixed, presc = uniaxial_bc(X)
     assert len(presc) == 16 and np.all(presc % 3 == 0)
     assert len(set(fixed) & set(presc)) == 0
-    # x-face fixed in x (16 dofs) + pinned corner (y, z) + one z at corner (0,1,0)
-    assert len(fixed) == 16 + 2 + 1
+    # symmetry planes: x-dofs of x=0, y-dofs of y=0, z-dofs of z=0 (16 nodes each)
+    assert len(fixed) == 3 * 16
+    assert sorted(set(int(d) % 3 for d in fixed)) == [0, 1, 2]
