@@ -11,6 +11,7 @@ SolveConstitutiveModel + InternalForce + TangentStiffnessMatrix per iteration).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --workload fe2-surrogate [--n-train 200000] [--epochs 2000]
   python bench.py --workload fe2-batch [--n-rve 4096]
+  python bench.py --workload j2-plate
 
 The second form runs the learned-surrogate experiment instead (training data from the batched
 RVE solver, training, validation error, a 4^3 macro head-to-head of surrogate and direct FE^2,
@@ -139,6 +140,72 @@ def algorithmic_bytes(n_nodes, n_elem, n_gp, n_dof, nnz, nb=3):
     return nodes + connectivity + state + fint + kval
 
 
+def run_j2_plate(args):
+    """Finite-strain J2 plate: 96 x 96 x 48 Hexa8 (442,368 elements, 3.54 M Gauss points), jitter 5 %,
+    E = 200 GPa, nu = 0.3, sigma_y0 = 250 MPa, H = 1 GPa with E and sigma_y scaled per element by a
+    log-uniform factor in [0.9, 1.1]; uniaxial tension along x with lateral contraction, evaluated at
+    2.5 % strain from the committed state of 1.25 % (every point plastic).  One step = one evaluation
+    (return mapping, f_int, K) in mixed precision; GP updates/s, device-resident."""
+    import torch
+    import ceos_b200 as G
+    from ceos_b200 import meshgen
+    nx, ny, nz = 96, 96, 48
+    X, conn = meshgen.structured_box(nx, ny, nz, lx=2.0, ly=2.0, lz=1.0, jitter=0.05, seed=0)
+    rng = np.random.default_rng(3)
+    ne = conn.shape[0]
+    fac = np.exp(rng.uniform(np.log(0.9), np.log(1.1), (ne, 2)))
+    params = np.zeros((ne, 4))
+    params[:, 0] = 200e3 * fac[:, 0]   # MPa
+    params[:, 1] = 0.3
+    params[:, 2] = 250.0 * fac[:, 1]
+    params[:, 3] = 1e3
+    g = G.ElementLoop(X, conn, G.J2_FINITE, params, per_element=True, precision=G.MIXED)
+
+    def U_at(eps):
+        U = np.zeros_like(X)
+        U[:, 0] = eps * X[:, 0]
+        U[:, 1] = -0.5 * eps * X[:, 1]
+        U[:, 2] = -0.5 * eps * X[:, 2]
+        return U.reshape(-1)
+    _, _, rc, _ = g.evaluate(0.0, U_at(0.0125), tangent=False)
+    assert rc == 0, rc
+    g.commit()
+    dU = torch.tensor(U_at(0.025), dtype=torch.float64, device="cuda")
+    dfint = torch.zeros(g.n_dof, dtype=torch.float64, device="cuda")
+    dK = torch.zeros(g.nnz, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            g.evaluate_device(0.0, dU, dfint, dK, stream=sp)
+    torch.cuda.synchronize()
+    assert g.status()[0] == 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        g.evaluate_device(0.0, dU, dfint, dK, stream=sp)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    g.set_options(G.OPT_TIME_KERNELS)
+    g.evaluate_device(0.0, dU, dfint, dK, stream=sp)
+    k_ms, c_ms = g.kernel_time_ms()
+    g.set_options(0)
+    st = g.state(1)
+    n_gp = 8 * ne
+    alg = 48 * g.n_nodes + 32 * ne + 16 * ne + n_gp * 7 * 4 * 2 + 8 * g.n_dof + 8 * g.nnz
+    peak, kind = measured_peak_hbm()
+    rec = {"metric": "GP updates/s", "value": n_gp / (ms * 1e-3), "unit": "GP updates/s", "higher_is_better": True,
+           "n_gpus": 1, "steps": args.steps, "ms_per_step": ms, "dtype": "f32+f64", "data": "synthetic",
+           "plastic_points": int((st[:, :, 6] > 0).sum()), "gauss_points": n_gp,
+           "roofline": {"bound": "hbm", "achieved": alg / (k_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": alg / (k_ms * 1e-3) / 1e9 / peak, "peak_kind": kind, "kernel_ms": k_ms,
+                        "conversion_kernel_ms": c_ms, "algorithmic_bytes_per_launch": alg},
+           "config": {"workload": "finite-strain J2 plate 96x96x48 Hexa8 (442,368 elements, 3.54 M GPs), per-element "
+                                  "E and sigma_y x U_log[0.9,1.1], uniaxial tension at 2.5 % from 1.25 % committed"}}
+    print(json.dumps(rec), flush=True)
+
+
 def run_fe2_batch(args):
     """Batched FE^2: n_rve periodic fibre RVEs of uneven size n in {6..12}, vf U[0.1, 0.4], F = I + G
     with |G_ij| <= 0.15, solved to 1e-8 with homogenized P and the 9x9 tangent, one batch on the GPU."""
@@ -227,7 +294,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="element-loop", choices=["element-loop", "fe2-surrogate", "fe2-batch"])
+    ap.add_argument("--workload", default="element-loop",
+                    choices=["element-loop", "fe2-surrogate", "fe2-batch", "j2-plate"])
     ap.add_argument("--n-rve", type=int, default=4096)
     ap.add_argument("--n-train", type=int, default=200000)
     ap.add_argument("--epochs", type=int, default=2000)
@@ -236,6 +304,8 @@ def main():
         return run_fe2_surrogate(args)
     if args.workload == "fe2-batch":
         return run_fe2_batch(args)
+    if args.workload == "j2-plate":
+        return run_j2_plate(args)
     warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
