@@ -18,6 +18,7 @@ def _setup():
     L.ceos_fe2_set_allow_failures.argtypes = [P, I]
     L.ceos_fe2_set_fractions.argtypes = [P, P]
     L.ceos_fe2_set_warm_start.argtypes = [P, I]
+    L.ceos_fe2_set_solver_ctas.argtypes = [P, I]
     L.ceos_fe2_set_solve_mask.argtypes = [P, P]
     L.ceos_fe2_destroy.argtypes = [P]
     L.ceos_fe2_destroy.restype = None
@@ -67,6 +68,10 @@ class BatchedRVE:
         """RVEs that cannot converge come back as NaN (and newton_iters -1) instead of raising."""
         _check(lib().ceos_fe2_set_allow_failures(self._h, 1 if allow else 0))
         self._allow = allow
+
+    def set_solver_ctas(self, n=0):
+        """RVEs the MINRES kernel keeps in flight (0: as many as occupancy allows)."""
+        _check(lib().ceos_fe2_set_solver_ctas(self._h, n))
 
     def set_warm_start(self, on=True):
         """Continue every RVE from its last converged state (macro load path) on the next solves."""

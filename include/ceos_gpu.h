@@ -236,6 +236,8 @@ int ceos_fe2_set_allow_failures(void* handle, int allow);
 /* on != 0: each solve continues every RVE from the Fbar and fluctuation of its last converged
  * state (along the macro load path) instead of from Fbar = I (default 0). */
 int ceos_fe2_set_warm_start(void* handle, int on);
+/* RVEs the persistent solver keeps in flight (0: as many as occupancy allows). */
+int ceos_fe2_set_solver_ctas(void* handle, int n);
 /* mask [n_rve]: 0 leaves an RVE out of the next solves (it keeps its state and P is that of the
  * state; its rows of A are not recomputed and must not be used); NULL solves all (default). */
 int ceos_fe2_set_solve_mask(void* handle, const int* mask);
