@@ -143,7 +143,10 @@ class ElementLoop:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:  # at interpreter exit the library binding may already be gone
+            self.close()
+        except Exception:
+            pass
 
     @property
     def handle(self):

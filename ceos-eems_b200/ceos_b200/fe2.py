@@ -111,4 +111,7 @@ class BatchedRVE:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:  # at interpreter exit the library binding may already be gone
+            self.close()
+        except Exception:
+            pass

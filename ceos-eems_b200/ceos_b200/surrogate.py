@@ -136,7 +136,10 @@ class Surrogate:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:  # at interpreter exit the library binding may already be gone
+            self.close()
+        except Exception:
+            pass
 
 
 def training_targets(F, P, s_C, s_W):
