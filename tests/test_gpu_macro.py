@@ -97,3 +97,27 @@ def test_macro_element_with_rve_points_matches_oracle():
         Po = F2.RVE(3, 0.3).solve(F[q])
         assert np.abs(P[q] - Po).max() <= 1e-6 * np.abs(Po).max(), q
     m.close()
+
+
+def test_fallback_pool_reproduces_direct_rve_solves():
+    """A surrogate whose training box is empty sends every point to RVE solves; through the warm RVE
+    pool (the large-mesh path, forced here) and the sticky fallback the macro run must reproduce the
+    direct run's Gauss-point stresses."""
+    from ceos_b200 import surrogate as SG
+    sur = SG.Surrogate(batch_max=256)
+    sur.set_params(SG.init_params(0))
+    sur.set_scaling(0.15, 1.0, 0.25, 0.15, lo=np.full(7, 1e3), hi=np.full(7, 1e3 + 1))
+    vf = np.array([0.3])
+    fields = {}
+    for mode in ("direct", "surrogate"):
+        m = M.MacroFE2(1, vf, n_cells=3, surrogate=sur)
+        m.point_batch_limit = 0  # large-mesh path: slots in the warm pool
+        m.pool_size = 16
+        out = m.run(stretch=1.03, n_steps=2, mode=mode, tol=1e-8)
+        if mode == "surrogate":
+            assert out["fallback_points"].min() >= 8  # every point, every material evaluation
+        fields[mode] = m.gp_first_piola()
+        m.close()
+    Pd, Ps = fields["direct"], fields["surrogate"]
+    assert np.abs(Ps - Pd).max() <= 1e-6 * np.abs(Pd).max()
+    sur.close()

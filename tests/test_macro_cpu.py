@@ -39,3 +39,20 @@ def test_uniaxial_bc_removes_rigid_motion():
     # symmetry planes: x-dofs of x=0, y-dofs of y=0, z-dofs of z=0 (16 nodes each)
     assert len(fixed) == 3 * 16
     assert sorted(set(int(d) % 3 for d in fixed)) == [0, 1, 2]
+
+
+def test_stress_error_measures_and_sampling():
+    from ceos_b200 import fe2_surrogate as FS
+    rng = np.random.default_rng(0)
+    P = rng.normal(size=(50, 3, 3))
+    e = FS.stress_errors(P * 1.01, P)
+    assert abs(e["aggregate"] - 0.01) < 1e-12 and abs(e["median"] - 0.01) < 1e-12
+    P2 = P.copy()
+    P2[3] = np.nan  # unsolved reference points are ignored
+    assert FS.stress_errors(P, P2)["n"] == 49
+    F, vf = FS.sample_points(400, seed=2, small_fraction=0.5)
+    G = F - np.eye(3)
+    assert np.all(np.abs(G) <= 0.15 + 1e-12) and np.all(np.linalg.det(F) > 0)
+    assert np.all((vf >= 0.1) & (vf <= 0.4))
+    # the scaled half has smaller strains on average
+    assert np.abs(G[:200]).mean() < np.abs(G[200:]).mean()
