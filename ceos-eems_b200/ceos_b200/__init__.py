@@ -16,7 +16,7 @@ from . import meshgen  # noqa: F401
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "lib", "libceos_b200.so")
 
-J2_SMALL, SVK, CNH, VISCO_VAR, VISCO_PRONY, J2_FINITE = 2, 5, 7, 12, 101, 102
+J2_SMALL, NH_Q1P0, SVK, CNH, VISCO_VAR, VISCO_PRONY, J2_FINITE = 2, 4, 5, 7, 12, 101, 102
 FP64, MIXED = 0, 1
 OPT_STORE_STRESS = 1
 OPT_TIME_KERNELS = 2

@@ -34,6 +34,7 @@ void hexa8_dN_table(double out[8][8][3]) {
 int model_nparams(int model) {
     switch (model) {
         case M_CNH: return ModelInfo<M_CNH>::nparams;
+        case M_NH_Q1P0: return ModelInfo<M_NH_Q1P0>::nparams;
         case M_SVK: return ModelInfo<M_SVK>::nparams;
         case M_J2_SMALL: return ModelInfo<M_J2_SMALL>::nparams;
         case M_VISCO_PRONY: return ModelInfo<M_VISCO_PRONY>::nparams;
@@ -46,6 +47,7 @@ int model_nparams(int model) {
 int model_nstate(int model) {
     switch (model) {
         case M_CNH: return 0;
+        case M_NH_Q1P0: return 0;
         case M_SVK: return 0;
         case M_J2_SMALL: return ModelInfo<M_J2_SMALL>::nstate;
         case M_VISCO_PRONY: return ModelInfo<M_VISCO_PRONY>::nstate;
@@ -132,6 +134,7 @@ template <typename T>
 int launch_elem(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
     switch (h->model) {
         case M_CNH: return launch_model<T, M_CNH>(h, dt, dU, dfint, dkval, s);
+        case M_NH_Q1P0: return launch_model<T, M_NH_Q1P0>(h, dt, dU, dfint, dkval, s);
         case M_SVK: return launch_model<T, M_SVK>(h, dt, dU, dfint, dkval, s);
         case M_J2_SMALL: return launch_model<T, M_J2_SMALL>(h, dt, dU, dfint, dkval, s);
         case M_VISCO_PRONY: return launch_model<T, M_VISCO_PRONY>(h, dt, dU, dfint, dkval, s);
@@ -151,6 +154,10 @@ int occupancy_grid(Handle* h) {
         case M_CNH:
             e = cudaFuncSetAttribute(element_loop_kernel<T, M_CNH, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
             if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_CNH, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
+            break;
+        case M_NH_Q1P0:
+            e = cudaFuncSetAttribute(element_loop_kernel<T, M_NH_Q1P0, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_NH_Q1P0, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
             break;
         case M_SVK:
             e = cudaFuncSetAttribute(element_loop_kernel<T, M_SVK, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));

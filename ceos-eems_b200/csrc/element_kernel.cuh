@@ -72,7 +72,7 @@ struct ElemArgs {
 // prefetched with cp.async while the current tile computes (software pipeline).
 template <typename T>
 struct SmemLayout {
-    size_t g, ds, st, x, u, xf, rs, nup, node, ranks, status, total;
+    size_t g, ds, st, x, u, xf, rs, nup, node, ranks, status, kd, total;
     CEOS_HD explicit SmemLayout(int ns) {
         size_t o = 0;
         auto take = [&](size_t bytes) { size_t r = o; o += (bytes + 15) & ~size_t(15); return r; };
@@ -87,6 +87,7 @@ struct SmemLayout {
         node = take(sizeof(int) * 2 * 8 * kTileE);
         ranks = take(sizeof(uint32_t) * 2 * kTileE * 8); // [buf][e][8]
         status = take(sizeof(int) * kTileE);
+        kd = take(sizeof(double) * kTileE);              // [e] Mean Dilatation: d2psi/dJbar2 / V0
         total = o;
     }
 };
@@ -262,6 +263,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
     int* snode = reinterpret_cast<int*>(smem_raw + L.node);
     uint32_t* sranks = reinterpret_cast<uint32_t*>(smem_raw + L.ranks);
     int* sstatus = reinterpret_cast<int*>(smem_raw + L.status);
+    T* skd = reinterpret_cast<T*>(smem_raw + L.kd);
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int n_tiles = (a.e_end - a.e_begin + kTileE - 1) / kTileE;
@@ -377,6 +379,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                 StateIO<T> io{sst + gp * kTileE + el, a.st_new, (size_t)8 * a.ld, (size_t)gp * a.ld + e};
                 T sig[6], D[21];
                 if (status & 1) {
+                    if constexpr (MODEL == M_NH_Q1P0)
+                        if (gp == 0) skd[el] = T(0);
 #pragma unroll
                     for (int k = 0; k < 6; ++k) sig[k] = T(0);
 #pragma unroll
@@ -391,7 +395,49 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                         else
                             ebr[k] = a.ebr[k];
                     }
-                    status |= run_material<T, MODEL>(F, p, ebr, a.dt, io, sig, D);
+                    if constexpr (MODEL == M_NH_Q1P0) {
+                        // Jbar = V / V0 (ElementVolume, ModElement.f90:1313-1427): every Gauss-point
+                        // thread of the element sums the same 8 determinants (no barrier needed)
+                        double V = 0.0, V0 = 0.0;
+#pragma unroll 1
+                        for (int g2 = 0; g2 < 8; ++g2) {
+                            T JX2[3][3] = {}, Jc2[3][3] = {};
+#pragma unroll
+                            for (int n = 0; n < 8; ++n) {
+                                T X[3], x[3];
+                                if constexpr (sizeof(T) == 4) {
+                                    const float4* q = reinterpret_cast<const float4*>(sxf + (n * kTileE + el) * 8);
+                                    const float4 xv = q[0], uv = q[1];
+                                    X[0] = xv.x; X[1] = xv.y; X[2] = xv.z;
+                                    x[0] = xv.x + uv.x; x[1] = xv.y + uv.y; x[2] = xv.z + uv.z;
+                                } else {
+                                    const double* xp = sx + (n * kTileE + el) * 3;
+                                    const double* up = su + (n * kTileE + el) * 3;
+#pragma unroll
+                                    for (int d = 0; d < 3; ++d) {
+                                        X[d] = (T)xp[d];
+                                        x[d] = (T)(xp[d] + up[d]);
+                                    }
+                                }
+#pragma unroll
+                                for (int i = 0; i < 3; ++i) {
+                                    const T dn = (T)c_dN[g2][n][i];
+#pragma unroll
+                                    for (int j = 0; j < 3; ++j) {
+                                        JX2[i][j] += dn * X[j];
+                                        Jc2[i][j] += dn * x[j];
+                                    }
+                                }
+                            }
+                            V0 += (double)det3(JX2);
+                            V += (double)det3(Jc2);
+                        }
+                        const double Jbar = V / V0;
+                        nh_q1p0_update<T>(F, p, Jbar, sig, D);
+                        if (gp == 0) skd[el] = (T)(nh_q1p0_d2psi((double)p[1], Jbar) / V0);
+                    } else {
+                        status |= run_material<T, MODEL>(F, p, ebr, a.dt, io, sig, D);
+                    }
                 }
                 bool finite = true;
 #pragma unroll
@@ -407,7 +453,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                 for (int q = 0; q < 5; ++q)
                     st4<T>(dst + q * kTileE * 4, w * D[4 * q], w * D[4 * q + 1], w * D[4 * q + 2], w * D[4 * q + 3]);
                 st4<T>(dst + 5 * kTileE * 4, w * D[20], w * sig[0], w * sig[1], w * sig[2]);
-                st4<T>(dst + 6 * kTileE * 4, w * sig[3], w * sig[4], w * sig[5], T(0));
+                st4<T>(dst + 6 * kTileE * 4, w * sig[3], w * sig[4], w * sig[5], w);  // w: Mean Dilatation
                 if (status) atomicOr(&sstatus[el], status);
             }
         }
@@ -439,6 +485,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                 for (int o = 0; o < 4; ++o)
 #pragma unroll
                     for (int k = 0; k < 9; ++k) Ko[o][k] = T(0);
+                // Mean Dilatation: Bdiv of node b and of its partners, sum_gp w detJ grad N (current)
+                T bdb[3] = {T(0), T(0), T(0)}, bda[4][3] = {};
 #pragma unroll 1
                 for (int gp = 0; gp < 8; ++gp) {
                     const T* src = sds + (size_t)gp * 7 * kTileE * 4 + el * 4;
@@ -447,10 +495,16 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                     for (int q = 0; q < 5; ++q)
                         ld4<T>(src + q * kTileE * 4, Dm[4 * q], Dm[4 * q + 1], Dm[4 * q + 2], Dm[4 * q + 3]);
                     ld4<T>(src + 5 * kTileE * 4, Dm[20], s0, s1, s2);
-                    ld4<T>(src + 6 * kTileE * 4, s3, s4, s5, pad);
+                    T wgp;
+                    ld4<T>(src + 6 * kTileE * 4, s3, s4, s5, wgp);
                     const T* gsrc = sg + (size_t)gp * 8 * kTileE * 4 + el * 4;
                     T gx, gy, gz;
                     ld4<T>(gsrc + b * kTileE * 4, gx, gy, gz, pad);
+                    if constexpr (MODEL == M_NH_Q1P0) {
+                        bdb[0] += wgp * gx;
+                        bdb[1] += wgp * gy;
+                        bdb[2] += wgp * gz;
+                    }
                     // sigma g_b: the internal force of node b and the geometric term
                     const T q0 = s0 * gx + s3 * gy + s5 * gz;
                     const T q1 = s3 * gx + s1 * gy + s4 * gz;
@@ -487,6 +541,11 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                             T ax, ay, az;
                             ld4<T>(gsrc + an * kTileE * 4, ax, ay, az, pad);
                             const T geo = ax * q0 + ay * q1 + az * q2;
+                            if constexpr (MODEL == M_NH_Q1P0) {
+                                bda[o][0] += wgp * ax;
+                                bda[o][1] += wgp * ay;
+                                bda[o][2] += wgp * az;
+                            }
 #pragma unroll
                             for (int l = 0; l < 3; ++l) {
                                 Ko[o][0 * 3 + l] += ax * DB[0][l] + ay * DB[3][l] + az * DB[5][l];
@@ -496,6 +555,22 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                             Ko[o][0] += geo; Ko[o][4] += geo; Ko[o][8] += geo;
                         }
                     }
+                }
+                if constexpr (MODEL == M_NH_Q1P0) {  // Bdiv^T Bdiv d2psi/dJbar2 / V0 (ModElement.f90:463-466)
+                    const T kd = isfinite(skd[el]) ? skd[el] : T(0);  // failed elements have Bdiv = 0
+                    Kd[0] += kd * bdb[0] * bdb[0];
+                    Kd[1] += kd * bdb[0] * bdb[1];
+                    Kd[2] += kd * bdb[0] * bdb[2];
+                    Kd[3] += kd * bdb[1] * bdb[1];
+                    Kd[4] += kd * bdb[1] * bdb[2];
+                    Kd[5] += kd * bdb[2] * bdb[2];
+#pragma unroll
+                    for (int o = 0; o < 4; ++o)
+                        if (o < npair)
+#pragma unroll
+                            for (int k = 0; k < 3; ++k)
+#pragma unroll
+                                for (int l = 0; l < 3; ++l) Ko[o][k * 3 + l] += kd * bda[o][k] * bdb[l];
                 }
                 // ---- scatter ----
                 const int Bn = node_c[b * kTileE + el];

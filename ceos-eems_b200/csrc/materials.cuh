@@ -10,7 +10,7 @@
 
 namespace ceos {
 
-enum : int { M_J2_SMALL = 2, M_SVK = 5, M_CNH = 7, M_VISCO_VAR = 12, M_VISCO_PRONY = 101, M_J2_FINITE = 102,
+enum : int { M_J2_SMALL = 2, M_NH_Q1P0 = 4, M_SVK = 5, M_CNH = 7, M_VISCO_VAR = 12, M_VISCO_PRONY = 101, M_J2_FINITE = 102,
              M_EXTERNAL = 200 };
 
 template <int MODEL>
@@ -19,6 +19,8 @@ template <>
 struct ModelInfo<M_CNH> { static constexpr int nstate = 0, nparams = 2; };
 template <>
 struct ModelInfo<M_SVK> { static constexpr int nstate = 0, nparams = 2; };
+template <>
+struct ModelInfo<M_NH_Q1P0> { static constexpr int nstate = 0, nparams = 2; };
 template <>
 struct ModelInfo<M_J2_SMALL> { static constexpr int nstate = 7, nparams = 4; };
 template <>
@@ -53,6 +55,95 @@ CEOS_D void cnh_update(const T F[3][3], const T* p, T sig[6], T D[21]) {
     for (int i = 0; i < 6; ++i)
 #pragma unroll
         for (int j = i; j < 6; ++j) D[up21(i, j)] = l * (T)(delta6(i) * delta6(j)) + (i == j ? (i < 3 ? m : T(0.5) * m) : T(0));
+}
+
+// ---------------------------------------------------------------------------------------
+// Neo-Hookean of the Mean Dilatation element (ConstitutiveModelsLibrary/ModNeoHookeanQ1P0.f90):
+//   sigma = 2 C10 J^(-5/3) (b - tr(b)/3 I) + pbar I,  pbar = 3 K (Jbar^(1/3) - 1) / Jbar^(2/3)
+// (:429-484); tangent = push-forward of C_iso + C_p with C = F^T F (:540-613):
+//   C_iso = 2/3 J^(-2/3) (Sf:C) P - 2/3 (S_iso (x) C^-1 + C^-1 (x) S_iso),
+//   P = C^-1 [.] C^-1 - 1/3 C^-1 (x) C^-1,  C_p = J pbar (C^-1 (x) C^-1 - 2 C^-1 [.] C^-1),
+// with Sf = 2 C10 I, S_iso = J^(-2/3) (Sf - 1/3 (Sf:C) C^-1), [.] the minor-symmetric product
+// 1/4 (A_ik B_jl + A_il B_jk + A_jk B_il + A_jl B_ik) (Square_Voigt, ModMathRoutines.f90:581-625),
+// and the push-forward Q W Q^T / J (Push_Forward_Voigt, :254-311).  params [C10, BulkModulus];
+// Jbar = V / V0 of the element (SubSolveConstitutiveModel.f90:100).  Scalars in FP64.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+CEOS_D T sym_at(const T v[6], int i, int j) {  // entry (i, j) of a symmetric tensor in Voigt
+    return i == j ? v[i] : v[(i + j == 1) ? 3 : ((i + j == 3) ? 4 : 5)];
+}
+template <typename T>
+CEOS_D void nh_q1p0_update(const T F[3][3], const T* p, double Jbar, T sig[6], T D[21]) {
+    const double C10 = p[0], K = p[1];
+    T b[6], Cv[6];
+    ffT(F, b);
+    fTf(F, Cv);
+    const double J = det3_fp64(F);
+    const double jb13 = cbrt(Jbar);
+    const double pbar = 3.0 * K * (jb13 - 1.0) / (jb13 * jb13);
+    const double Jm23 = 1.0 / cbrt(J * J), Jm53 = Jm23 / J;
+    const T trb = b[0] + b[1] + b[2];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+        sig[k] = (T)(2.0 * C10 * Jm53) * (b[k] - (k < 3 ? trb / T(3) : T(0))) + (k < 3 ? (T)pbar : T(0));
+    // C^-1 (Voigt) by the adjugate
+    T Cm[3][3], Ci[3][3];
+    sym_to_mat(Cv, Cm);
+    inv3(Cm, det3(Cm), Ci);
+    const T civ[6] = {Ci[0][0], Ci[1][1], Ci[2][2], Ci[0][1], Ci[1][2], Ci[0][2]};
+    const T sc = T(2.0 * C10) * (Cv[0] + Cv[1] + Cv[2]);  // Sf : C
+    T siso[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) siso[k] = (T)Jm23 * ((k < 3 ? T(2.0 * C10) : T(0)) - sc / T(3) * civ[k]);
+    const int vi[6] = {0, 1, 2, 0, 1, 0}, vj[6] = {0, 1, 2, 1, 2, 2};
+    T Cb[6][6];
+#pragma unroll
+    for (int pp = 0; pp < 6; ++pp)
+#pragma unroll
+        for (int qq = 0; qq < 6; ++qq) {
+            const int i = vi[pp], j = vj[pp], k = vi[qq], l = vj[qq];
+            const T sq = T(0.25) * (sym_at(civ, i, k) * sym_at(civ, j, l) + sym_at(civ, i, l) * sym_at(civ, j, k) +
+                                    sym_at(civ, j, k) * sym_at(civ, i, l) + sym_at(civ, j, l) * sym_at(civ, i, k));
+            const T bl = civ[pp] * civ[qq];
+            const T ciso = T(2.0 / 3.0) * (T)Jm23 * sc * (sq - bl / T(3)) -
+                           T(2.0 / 3.0) * (siso[pp] * civ[qq] + civ[pp] * siso[qq]);
+            const T cp = (T)(J * pbar) * (bl - T(2) * sq);
+            Cb[pp][qq] = ciso + cp;
+        }
+    // push-forward: Q Cb Q^T / J, Q[p][r] = F_iI F_jJ (+ F_iJ F_jI for shear r)
+    T Q[6][6];
+#pragma unroll
+    for (int pp = 0; pp < 6; ++pp)
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+            const int i = vi[pp], j = vj[pp], I = vi[r], Jx = vj[r];
+            Q[pp][r] = F[i][I] * F[j][Jx] + (r >= 3 ? F[i][Jx] * F[j][I] : T(0));
+        }
+    T QC[6][6];
+#pragma unroll
+    for (int pp = 0; pp < 6; ++pp)
+#pragma unroll
+        for (int qq = 0; qq < 6; ++qq) {
+            T t = 0;
+#pragma unroll
+            for (int r = 0; r < 6; ++r) t += Q[pp][r] * Cb[r][qq];
+            QC[pp][qq] = t;
+        }
+    const T rJ = (T)(1.0 / J);
+#pragma unroll
+    for (int pp = 0; pp < 6; ++pp)
+#pragma unroll
+        for (int qq = pp; qq < 6; ++qq) {
+            T t = 0;
+#pragma unroll
+            for (int r = 0; r < 6; ++r) t += QC[pp][r] * Q[qq][r];
+            D[up21(pp, qq)] = t * rJ;
+        }
+}
+// SecondDerivativesOfPSI_Jbar_NeoHookeanQ1P0 (ModNeoHookeanQ1P0.f90:625-652)
+CEOS_D double nh_q1p0_d2psi(double K, double Jbar) {
+    const double jb13 = cbrt(Jbar);
+    return -(K * (jb13 - 2.0)) / (Jbar * jb13 * jb13);
 }
 
 // ---------------------------------------------------------------------------------------

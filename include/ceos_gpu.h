@@ -33,6 +33,8 @@ extern "C" {
  * ModConstitutiveModelLibrary.f90:39-56) and project-defined models (>= 101). */
 enum ceos_model_id {
     CEOS_J2_SMALL = 2,       /* ModJ2Plasticity.f90, params [E, nu, YieldStress, HardeningModulus]      */
+    CEOS_NH_Q1P0 = 4,        /* ModNeoHookeanQ1P0.f90 on the Mean Dilatation Hexa8 (Jbar = V/V0 per      */
+                             /* element, ModElement.f90:429-469), params [C10, BulkModulus]                */
     CEOS_SVK = 5,            /* ModStVenantKirchhoff.f90, params [YoungModulus, Poisson]                  */
     CEOS_CNH = 7,            /* ModCompressibleNeoHookean.f90, params [Mu, Lambda]                        */
     CEOS_VISCO_VAR = 12,     /* ModViscoelasticMatrix.f90, params [K_inf, Mu_inf, Lambda_inf, K_e, Mu_e, Ni_v] */

@@ -128,6 +128,98 @@ void cnh(const double* p, const M3 F, double sig[6], double D[36]) {
                            (2.0 / J) * (Mu - Lambda * std::log(J)) * (i == j ? kIsym[i] : 0.0);
 }
 
+// Voigt products of ModMathRoutines.f90 (tensor components, order 11,22,33,12,23,13):
+// Ball_Voigt (:532-577) A (x) B; Square_Voigt (:581-625), the minor-symmetric
+// 1/4 (A_ik B_jl + A_il B_jk + A_jk B_il + A_jl B_ik); Inner_Product_Voigt (:629-638).
+// (kVi, kVj: the Voigt index pairs above)
+double vget(const double a[6], int i, int j) {  // symmetric tensor entry from Voigt
+    for (int p = 0; p < 6; ++p)
+        if ((kVi[p] == i && kVj[p] == j) || (kVi[p] == j && kVj[p] == i)) return a[p];
+    return 0.0;
+}
+void ball_voigt(const double A[6], const double B[6], double T[36]) {
+    for (int p = 0; p < 6; ++p)
+        for (int q = 0; q < 6; ++q) T[p * 6 + q] = A[p] * B[q];
+}
+void square_voigt(const double A[6], const double B[6], double T[36]) {
+    for (int p = 0; p < 6; ++p)
+        for (int q = 0; q < 6; ++q) {
+            const int i = kVi[p], j = kVj[p], k = kVi[q], l = kVj[q];
+            T[p * 6 + q] = 0.25 * (vget(A, i, k) * vget(B, j, l) + vget(A, i, l) * vget(B, j, k) +
+                                   vget(A, j, k) * vget(B, i, l) + vget(A, j, l) * vget(B, i, k));
+        }
+}
+double inner_voigt(const double A[6], const double B[6]) {
+    return A[0] * B[0] + A[1] * B[1] + A[2] * B[2] + 2.0 * (A[3] * B[3] + A[4] * B[4] + A[5] * B[5]);
+}
+// Push_Forward_Voigt (:254-311): T = A W A^T / J, A the Voigt map of F (shear columns doubled)
+void push_forward_voigt(const double W[36], const M3 F, double T[36]) {
+    double A[6][6];
+    for (int p = 0; p < 6; ++p)
+        for (int r = 0; r < 6; ++r) {
+            const int i = kVi[p], j = kVj[p], I = kVi[r], Jx = kVj[r];
+            A[p][r] = F[i][I] * F[j][Jx] + (r >= 3 ? F[i][Jx] * F[j][I] : 0.0);
+        }
+    const double J = det3(F);
+    double AW[6][6];
+    for (int p = 0; p < 6; ++p)
+        for (int q = 0; q < 6; ++q) {
+            double t = 0.0;
+            for (int r = 0; r < 6; ++r) t += A[p][r] * (r <= q ? W[r * 6 + q] : W[q * 6 + r]);  // W upper
+            AW[p][q] = t;
+        }
+    for (int p = 0; p < 6; ++p)
+        for (int q = 0; q < 6; ++q) {
+            double t = 0.0;
+            for (int r = 0; r < 6; ++r) t += AW[p][r] * A[q][r];
+            T[p * 6 + q] = t / J;
+        }
+}
+
+// Neo-Hookean for the Mean Dilatation element (ModNeoHookeanQ1P0.f90): Cauchy stress
+// 2 C10 J^(-5/3) (b - tr(b)/3 I) + pbar I with pbar = 3 K (Jbar^(1/3) - 1) / Jbar^(2/3)
+// (:429-484); tangent = push-forward of C_iso + C_p (:540-613); params = [C10, BulkModulus].
+void nh_q1p0(const double* p, const M3 F, double Jbar, double sig[6], double D[36]) {
+    const double C10 = p[0], K = p[1];
+    M3 Ft, b, C, Ci;
+    transpose3(F, Ft);
+    matmul3(F, Ft, b);
+    matmul3(Ft, F, C);
+    inv3(C, Ci);
+    const double trb = b[0][0] + b[1][1] + b[2][2];
+    const double J = det3(F);
+    const double pbar = (3.0 * K * (std::pow(Jbar, 1.0 / 3.0) - 1.0)) / std::pow(Jbar, 2.0 / 3.0);
+    M3 S;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            S[i][j] = 2.0 * C10 * std::pow(J, -5.0 / 3.0) * (b[i][j] - (i == j ? trb / 3.0 : 0.0)) + (i == j ? pbar : 0.0);
+    to_voigt(S, sig);
+    double CV[6], CinvV[6], SfricV[6] = {2.0 * C10, 2.0 * C10, 2.0 * C10, 0, 0, 0}, devS[6], Siso[6];
+    to_voigt(C, CV);
+    to_voigt(Ci, CinvV);
+    const double sc = inner_voigt(SfricV, CV);
+    for (int k = 0; k < 6; ++k) {
+        devS[k] = SfricV[k] - (1.0 / 3.0) * sc * CinvV[k];
+        Siso[k] = std::pow(J, -2.0 / 3.0) * devS[k];
+    }
+    double SQ[36], BL[36], B1[36], B2[36], Cbar[36];
+    square_voigt(CinvV, CinvV, SQ);
+    ball_voigt(CinvV, CinvV, BL);
+    ball_voigt(Siso, CinvV, B1);
+    ball_voigt(CinvV, Siso, B2);
+    for (int k = 0; k < 36; ++k) {
+        const double Pm = SQ[k] - (1.0 / 3.0) * BL[k];
+        const double Ciso = (2.0 / 3.0) * std::pow(J, -2.0 / 3.0) * sc * Pm - (2.0 / 3.0) * (B1[k] + B2[k]);
+        const double Cp = J * pbar * (BL[k] - 2.0 * SQ[k]);
+        Cbar[k] = Ciso + Cp;
+    }
+    push_forward_voigt(Cbar, F, D);
+}
+// SecondDerivativesOfPSI_Jbar_NeoHookeanQ1P0 (:625-652)
+double nh_q1p0_d2psi(const double* p, double Jbar) {
+    return -(p[1] * (std::pow(Jbar, 1.0 / 3.0) - 2.0)) / std::pow(Jbar, 5.0 / 3.0);
+}
+
 // St Venant-Kirchhoff (ModStVenantKirchhoff.f90:643-780); params = [YoungModulus, Poisson],
 // Lambda/Mu from (:238-239).  The reference fills only the upper triangle of D (:751-756);
 // the full symmetric D is returned here (the element routine reads the upper triangle).
@@ -388,6 +480,7 @@ void j2_finite(const double* p, const M3 F, const double* st_old, double* st_new
 extern "C" int or_model_nparams(int model) {
     switch (model) {
         case OR_CNH: return 2;
+        case OR_NH_Q1P0: return 2;
         case OR_SVK: return 2;
         case OR_J2_SMALL: return 4;
         case OR_VISCO_VAR: return 6;
@@ -400,6 +493,7 @@ extern "C" int or_model_nparams(int model) {
 extern "C" int or_model_nstate(int model) {
     switch (model) {
         case OR_CNH: return 0;
+        case OR_NH_Q1P0: return 0;
         case OR_SVK: return 0;
         case OR_J2_SMALL: return 7;
         case OR_VISCO_VAR: return 19;
@@ -429,6 +523,7 @@ extern "C" int or_material_point(int model, const double* params, const double* 
         for (int j = 0; j < 3; ++j) F[i][j] = Fin[i * 3 + j];
     switch (model) {
         case OR_CNH: cnh(params, F, sigma, D); return 0;
+        case OR_NH_Q1P0: nh_q1p0(params, F, det3(F), sigma, D); return 0;  // single point: Jbar = J
         case OR_SVK: svk(params, F, sigma, D); return 0;
         case OR_J2_SMALL: j2_small(params, F, st_old, st_new, sigma, D); return 0;
         case OR_VISCO_PRONY: visco_prony(params, F, dt, st_old, st_new, sigma, D); return 0;
@@ -546,6 +641,7 @@ struct or_model {
     std::vector<double> sigma;            // [n_elem*8*6]
     std::vector<double> Dgp;              // [n_elem*8*36]
     std::vector<int> gp_status;
+    std::vector<double> jbar, vol0;       // [n_elem] Mean Dilatation: V/V0 and V0 of the last update
     double time_old = 0.0;
     const double* elem_params(int e) const {
         return per_element ? &params[(size_t)e * n_params_max] : &params[(size_t)mat_id[e] * n_params_max];
@@ -585,6 +681,8 @@ extern "C" or_model* or_create(int n_nodes, int n_elem, const double* X, const i
     m->sigma.assign(ngp * 6, 0.0);
     m->Dgp.assign(ngp * 36, 0.0);
     m->gp_status.assign(ngp, 0);
+    m->jbar.assign(n_elem, 1.0);
+    m->vol0.assign(n_elem, 1.0);
     return m;
 }
 
@@ -641,6 +739,22 @@ int element_update(or_model* m, int e, const ElemGeom& g, double dt) {
         if (det3(Jc) <= 1.0e-13) status = 1;
     }
     const int ns = m->nstate;
+    const bool q1p0 = m->elem_model(e) == OR_NH_Q1P0;
+    if (q1p0) {  // Jbar = Volume / VolumeX for every Gauss point (SubSolveConstitutiveModel.f90:65,100)
+        double V = 0.0, V0 = 0.0;
+        for (int gp = 0; gp < 8; ++gp) {
+            double xi[3], w, dN[8][3];
+            hexa8_gp(gp, xi, &w);
+            hexa8_dN(xi, dN);
+            M3 Jc, JX;
+            jacobian(dN, g.xe, Jc);
+            jacobian(dN, g.Xe, JX);
+            V0 += w * det3(JX);
+            V += w * det3(Jc);
+        }
+        m->jbar[e] = V / V0;
+        m->vol0[e] = V0;
+    }
     for (int gp = 0; gp < 8; ++gp) {
         double xi[3], w, dN[8][3], dNX[8][3];
         hexa8_gp(gp, xi, &w);
@@ -658,8 +772,15 @@ int element_update(or_model* m, int e, const ElemGeom& g, double dt) {
                 F[i * 3 + j] = s + (i == j ? 1.0 : 0.0);
             }
         const size_t q = (size_t)e * 8 + gp;
-        const int st = or_material_point(m->elem_model(e), m->elem_params(e), F, dt, &m->st_old[q * ns],
-                                         &m->st_new[q * ns], &m->sigma[q * 6], &m->Dgp[q * 36]);
+        int st = 0;
+        if (q1p0) {
+            M3 Fm;
+            for (int i = 0; i < 9; ++i) Fm[i / 3][i % 3] = F[i];
+            nh_q1p0(m->elem_params(e), Fm, m->jbar[e], &m->sigma[q * 6], &m->Dgp[q * 36]);
+        } else {
+            st = or_material_point(m->elem_model(e), m->elem_params(e), F, dt, &m->st_old[q * ns],
+                                   &m->st_new[q * ns], &m->sigma[q * 6], &m->Dgp[q * 36]);
+        }
         m->gp_status[q] = st;
         if (st && !status) status = st;
     }
@@ -713,11 +834,17 @@ int element_fint(const or_model* m, int e, const ElemGeom& g, double Fe[24]) {
 // ElementStiffnessMatrix, nonlinear full integration (ModElement.f90:310-348):
 // Ke += w detJ (B^T (D B) + G^T (S G)); D and S are read through their upper triangle
 // (dsymm 'L','U', ModMathRoutines.f90:975-1000); S = blockdiag(sigma) (ModConstitutiveModel.f90:292-314).
+// Mean Dilatation (ModElement.f90:429-469) adds Bdiv^T Bdiv d2psi/dJbar2 / VolumeX with
+// Bdiv = sum_gp w detJ (G(1,:) + G(5,:) + G(9,:)).
 void element_stiffness(const or_model* m, int e, const ElemGeom& g, double Ke[24][24]) {
     std::memset(Ke, 0, sizeof(double) * 576);
+    const bool q1p0 = m->elem_model(e) == OR_NH_Q1P0;
+    double Bdiv[24] = {0};
     for (int gp = 0; gp < 8; ++gp) {
         double B[6][24], G[9][24], detJ, w;
         if (!bg_matrices(g, gp, B, G, &detJ, &w)) continue;
+        if (q1p0)
+            for (int c = 0; c < 24; ++c) Bdiv[c] += (G[0][c] + G[4][c] + G[8][c]) * w * detJ;
         const double* Dg = &m->Dgp[((size_t)e * 8 + gp) * 36];
         const double* s = &m->sigma[((size_t)e * 8 + gp) * 6];
         double Ds[6][6], S[9][9];
@@ -755,6 +882,11 @@ void element_stiffness(const or_model* m, int e, const ElemGeom& g, double Ke[24
                 for (int k = 0; k < 9; ++k) t += G[k][i] * SG[k][j];
                 Ke[i][j] += a * t;
             }
+    }
+    if (q1p0) {
+        const double kd = nh_q1p0_d2psi(m->elem_params(e), m->jbar[e]) / m->vol0[e];
+        for (int i = 0; i < 24; ++i)
+            for (int j = 0; j < 24; ++j) Ke[i][j] += Bdiv[i] * Bdiv[j] * kd;
     }
 }
 

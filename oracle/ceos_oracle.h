@@ -25,6 +25,7 @@ extern "C" {
  * project-defined models with no reference implementation. */
 enum {
     OR_J2_SMALL = 2,     /* ModJ2Plasticity.f90 (small strain, reference)           */
+    OR_NH_Q1P0 = 4,      /* ModNeoHookeanQ1P0.f90 with the Mean Dilatation element  */
     OR_SVK = 5,          /* ModStVenantKirchhoff.f90                                 */
     OR_CNH = 7,          /* ModCompressibleNeoHookean.f90                            */
     OR_VISCO_VAR = 12,   /* ModViscoelasticMatrix.f90 (variational, one branch)      */

@@ -12,7 +12,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libceos_oracle.so")
 
-CNH, SVK, J2_SMALL, VISCO_VAR, VISCO_PRONY, J2_FINITE = 7, 5, 2, 12, 101, 102
+CNH, SVK, J2_SMALL, VISCO_VAR, VISCO_PRONY, J2_FINITE, NH_Q1P0 = 7, 5, 2, 12, 101, 102, 4
 
 _lib = None
 

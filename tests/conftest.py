@@ -17,3 +17,9 @@ def pytest_configure(config):
 def golden():
     with open(os.path.join(ROOT, "tests", "golden", "hexa8_svk.json")) as f:
         return json.load(f)
+
+
+@pytest.fixture(scope="session")
+def golden_nh():
+    with open(os.path.join(ROOT, "tests", "golden", "hexa8_nh_q1p0.json")) as f:
+        return json.load(f)

@@ -1,12 +1,15 @@
-"""Generate tests/golden/hexa8_svk.json from the reference's golden Checker case.
+"""Generate the golden fixtures tests/golden/hexa8_svk.json and tests/golden/hexa8_nh_q1p0.json from
+the reference's golden Checker cases.
 
-The reference ships exactly one case that pins the Hexa8 element loop, the upper-CSR
-assembly, the rearrangement boundary conditions and the Newton driver:
-Checker/Cases/NonLinear_FEA_3D_Hexa8_StVenant (96 Hexa8 elements, 195 nodes, St Venant-
-Kirchhoff, 50 load steps).  This script reads its input files (GiD-12 Mesh.dat, tables,
-time discretization) and its expected outputs (MARC displacement curves of node 11,
-NumOfIterRef.dat, the per-iteration NORM lines of Log_CEOS.txt) and writes them as one JSON
-fixture, so that the tests never read the reference tree at run time.
+Two reference cases pin the Hexa8 element loop, the upper-CSR assembly, the rearrangement boundary
+conditions and the Newton driver (96 Hexa8 elements, 195 nodes, 50 load steps, the same mesh):
+- Checker/Cases/NonLinear_FEA_3D_Hexa8_StVenant: St Venant-Kirchhoff, full integration;
+- Checker/Cases/NonLinear_FEA_3D_Hexa8_NeoHookean_Incompressible: Neo_Hookean (C10, Bulk
+  Modulus) with the Mean Dilatation element technology.
+This script reads their input files (GiD-12 Mesh.dat, tables, time discretization) and expected
+outputs (MARC displacement curves of node 11, NumOfIterRef.dat, the per-iteration NORM lines of
+Log_CEOS.txt) and writes them as JSON fixtures, so that the tests never read the reference tree
+at run time.
 
 Usage:  python tests/golden/make_golden.py /path/to/reference
 """
@@ -15,7 +18,12 @@ import os
 import re
 import sys
 
-CASE = "Checker/Cases/NonLinear_FEA_3D_Hexa8_StVenant"
+CASES = [
+    ("Checker/Cases/NonLinear_FEA_3D_Hexa8_StVenant", "hexa8_svk.json",
+     {"model": "St_Venant_Kirchhoff", "YoungModulus": 100.0e9, "Poisson": 0.3}),
+    ("Checker/Cases/NonLinear_FEA_3D_Hexa8_NeoHookean_Incompressible", "hexa8_nh_q1p0.json",
+     {"model": "Neo_Hookean", "C10": 5.0e10, "BulkModulus": 5.0e13, "element_technology": "Mean Dilatation"}),
+]
 
 
 def _lines(path):
@@ -118,31 +126,32 @@ def read_log_norms(path):
 
 
 def main(ref):
-    case = os.path.join(ref, CASE)
-    mesh = read_mesh(os.path.join(case, "Mesh.dat"))
-    fx = {
-        "source": CASE,
-        "material": {"model": "St_Venant_Kirchhoff", "YoungModulus": 100.0e9, "Poisson": 0.3},
-        "newton": {"tol": 1e-3, "itmax": 10, "max_cutbacks": 10},
-        "time": {"t0": 0.0, "t1": 1.0, "steps": 50},
-        "probe_node": 11,
-        "tables": {
-            "Table_Disp_Z": read_table(os.path.join(case, "Table_Disp_Z.tab")),
-            "Table_Load_Y": read_table(os.path.join(case, "Table_Load_Y.tab")),
-        },
-        "marc": {
-            "x": read_two_cols(os.path.join(case, "marc_disp_x.dat")),
-            "y": read_two_cols(os.path.join(case, "marc_disp_y.dat")),
-            "z": read_two_cols(os.path.join(case, "marc_disp_z.dat")),
-        },
-        "iterations_ref": read_two_cols(os.path.join(case, "NumOfIterRef.dat")),
-        "log_norms": read_log_norms(os.path.join(case, "Log_CEOS.txt")),
-    }
-    fx.update(mesh)
-    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hexa8_svk.json")
-    with open(out, "w") as f:
-        json.dump(fx, f, separators=(",", ":"))
-    print("wrote", out, "nodes", len(mesh["X"]) // 3, "elements", len(mesh["conn"]) // 8)
+    for case_rel, out_name, material in CASES:
+        case = os.path.join(ref, case_rel)
+        mesh = read_mesh(os.path.join(case, "Mesh.dat"))
+        fx = {
+            "source": case_rel,
+            "material": material,
+            "newton": {"tol": 1e-3, "itmax": 10, "max_cutbacks": 10},
+            "time": {"t0": 0.0, "t1": 1.0, "steps": 50},
+            "probe_node": 11,
+            "tables": {
+                "Table_Disp_Z": read_table(os.path.join(case, "Table_Disp_Z.tab")),
+                "Table_Load_Y": read_table(os.path.join(case, "Table_Load_Y.tab")),
+            },
+            "marc": {
+                "x": read_two_cols(os.path.join(case, "marc_disp_x.dat")),
+                "y": read_two_cols(os.path.join(case, "marc_disp_y.dat")),
+                "z": read_two_cols(os.path.join(case, "marc_disp_z.dat")),
+            },
+            "iterations_ref": read_two_cols(os.path.join(case, "NumOfIterRef.dat")),
+            "log_norms": read_log_norms(os.path.join(case, "Log_CEOS.txt")),
+        }
+        fx.update(mesh)
+        out = os.path.join(os.path.dirname(os.path.abspath(__file__)), out_name)
+        with open(out, "w") as f:
+            json.dump(fx, f, separators=(",", ":"))
+        print("wrote", out, "nodes", len(mesh["X"]) // 3, "elements", len(mesh["conn"]) // 8)
 
 
 if __name__ == "__main__":

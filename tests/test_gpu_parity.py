@@ -18,6 +18,7 @@ J2S_P = [200.0e3, 0.3, 250.0, 1000.0]
 J2F_P = [200.0e3, 0.3, 250.0, 1000.0]
 PRONY_P = [1.0, 100.0, 3, 0.3, 0.01, 0.2, 0.1, 0.1, 1.0, 0.0, 1.0]
 VV_P = [0.0, 1.0, 100.0 - 2.0 / 3.0, 0.0, 0.5, 0.2]   # K_inf, Mu_inf, Lambda_inf, K_e, Mu_e, Ni_v
+Q1P0_P = [0.5, 100.0]                                  # C10, BulkModulus (Mean Dilatation element)
 
 
 def smooth_u(X, amp, seed=1):
@@ -70,7 +71,8 @@ def _pair(model, params, X, conn, precision=G.FP64, per_element=False):
 
 @pytest.mark.parametrize("model,params,amp", [
     (G.CNH, CNH_P, 0.08), (G.SVK, SVK_P, 0.05), (G.J2_SMALL, J2S_P, 0.01),
-    (G.J2_FINITE, J2F_P, 0.01), (G.VISCO_PRONY, PRONY_P, 0.08), (G.VISCO_VAR, VV_P, 0.05)])
+    (G.J2_FINITE, J2F_P, 0.01), (G.VISCO_PRONY, PRONY_P, 0.08), (G.VISCO_VAR, VV_P, 0.05),
+    (G.NH_Q1P0, Q1P0_P, 0.08)])
 def test_evaluate_fp64(model, params, amp):
     X, conn = meshgen.structured_box(6, 5, 4, jitter=0.05, seed=2)
     g, o = _pair(model, params, X, conn)
@@ -94,7 +96,7 @@ def test_evaluate_fp64(model, params, amp):
 
 @pytest.mark.parametrize("model,params,amp,tol", [
     (G.CNH, CNH_P, 0.08, 2e-5), (G.VISCO_PRONY, PRONY_P, 0.08, 2e-5), (G.J2_FINITE, J2F_P, 0.01, 5e-5),
-    (G.VISCO_VAR, VV_P, 0.05, 2e-5)])
+    (G.VISCO_VAR, VV_P, 0.05, 2e-5), (G.NH_Q1P0, Q1P0_P, 0.08, 5e-5)])
 def test_evaluate_mixed(model, params, amp, tol):
     X, conn = meshgen.structured_box(6, 5, 4, jitter=0.05, seed=2)
     g, o = _pair(model, params, X, conn, precision=G.MIXED)
@@ -176,6 +178,27 @@ def test_golden_case_through_gpu(golden):
     np.testing.assert_array_equal(r["iters"], ref)
     log = np.array([v for s in golden["log_norms"] for v in s])
     big = log > 1e-2
+    np.testing.assert_allclose(r["norms"][big], log[big], rtol=1e-5)
+    g.close()
+
+
+def test_mean_dilatation_golden_case_through_gpu(golden_nh):
+    """The reference's Mean Dilatation golden case (Neo_Hookean, model 4) through the C ABI."""
+    X = np.array(golden_nh["X"]).reshape(-1, 3)
+    conn = np.array(golden_nh["conn"]).reshape(-1, 8)
+    bc = meshgen.golden_hexa8_svk_bc(golden_nh)
+    mat = golden_nh["material"]
+    g = G.ElementLoop(X, conn, G.NH_Q1P0, [mat["C10"], mat["BulkModulus"]])
+    node = golden_nh["probe_node"]
+    r = g.analysis(bc, tol=1e-3, itmax=10, norm_mode=1, probe_dofs=[3 * (node - 1) + d + 1 for d in range(3)])
+    assert r["rc"] == 0
+    for k, comp in enumerate("xyz"):
+        marc = np.array(golden_nh["marc"][comp])[1:, 1]
+        assert np.abs(r["probe"][k] - marc).max() <= 1e-4
+    ref = np.array([row[1] for row in golden_nh["iterations_ref"][1:]])
+    np.testing.assert_array_equal(r["iters"], ref)
+    log = np.array([v for s in golden_nh["log_norms"] for v in s])
+    big = log > 1.0
     np.testing.assert_allclose(r["norms"][big], log[big], rtol=1e-5)
     g.close()
 

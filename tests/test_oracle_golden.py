@@ -1,7 +1,10 @@
-"""Pins the FP64 oracle against the reference's only golden Hexa8 case
-(Checker/Cases/NonLinear_FEA_3D_Hexa8_StVenant): MARC displacement curves of node 11 with
-the Checker's absolute tolerance 1e-5 (Run_Checker.bat), Newton iteration counts per step
-(NumOfIterRef.dat, tolerance 1e-3) and the per-iteration residual norms of Log_CEOS.txt.
+"""Pins the FP64 oracle against the reference's golden Hexa8 cases:
+- Checker/Cases/NonLinear_FEA_3D_Hexa8_StVenant (full integration): MARC displacement curves of
+  node 11 within the Checker's absolute tolerance 1e-5 (its Run_Checker.bat), Newton iteration
+  counts per step (NumOfIterRef.dat) and the per-iteration residual norms of Log_CEOS.txt;
+- Checker/Cases/NonLinear_FEA_3D_Hexa8_NeoHookean_Incompressible (Mean Dilatation, model 4):
+  the same three records; that case's Run_Checker.bat compares the curves to MARC at 1e-3, the
+  oracle is held to 1e-4.
 The golden logs follow an absolute max-norm criterion ||R||_inf < Tol (norm_mode=1)."""
 import numpy as np
 
@@ -47,3 +50,31 @@ def test_relative_criterion_runs(golden):
     r = _run(golden, norm_mode=0)
     assert r["rc"] == 0
     assert int(r["iters"].sum()) < 162
+
+
+def _run_nh(golden_nh):
+    X = np.array(golden_nh["X"]).reshape(-1, 3)
+    conn = np.array(golden_nh["conn"]).reshape(-1, 8)
+    bc = meshgen.golden_hexa8_svk_bc(golden_nh)
+    mat = golden_nh["material"]
+    m = O.Model(X, conn, [O.NH_Q1P0], [[mat["C10"], mat["BulkModulus"]]])
+    node = golden_nh["probe_node"]
+    dofs = [3 * (node - 1) + d + 1 for d in range(3)]
+    return m.analysis(bc, tol=golden_nh["newton"]["tol"], itmax=golden_nh["newton"]["itmax"], norm_mode=1,
+                      probe_dofs=dofs)
+
+
+def test_golden_mean_dilatation_case(golden_nh):
+    r = _run_nh(golden_nh)
+    assert r["rc"] == 0
+    for k, comp in enumerate("xyz"):
+        marc = np.array(golden_nh["marc"][comp])[1:, 1]
+        assert np.abs(r["probe"][k] - marc).max() <= 1e-4, comp
+    ref = np.array([row[1] for row in golden_nh["iterations_ref"][1:]])
+    np.testing.assert_array_equal(r["iters"], ref)           # 206 iterations, step by step
+    log = np.array([v for s in golden_nh["log_norms"] for v in s])
+    ours = np.asarray(r["norms"])
+    assert ours.size == log.size == 256
+    big = log > 1.0            # the initial residuals are ~4e9: below 1 the norms are round-off
+    np.testing.assert_allclose(ours[big], log[big], rtol=1e-5)
+    np.testing.assert_array_equal(ours[~big] < 1e-3, log[~big] < 1e-3)

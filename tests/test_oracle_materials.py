@@ -167,3 +167,30 @@ def test_visco_var_relaxes_to_equilibrium_branch():
     s_eq, _, _, _ = O.material_point(O.VISCO_VAR, eq, F, 0.5, O.init_state(O.VISCO_VAR, eq))
     assert abs(s_first[0] - s_eq[0]) > 1e-3 * abs(s_eq[0])   # the branch carries stress at first
     assert np.allclose(sig, s_eq, rtol=1e-4, atol=1e-8)     # and has relaxed at the end
+
+
+def test_mean_dilatation_element_tangent_matches_finite_differences():
+    """The Mean Dilatation K (full-integration B^T D B + G^T S G with the Jbar pressure, plus
+    Bdiv^T Bdiv d2psi/dJbar2 / V0) is the derivative of its f_int: central differences of f_int
+    over the displacements of a jittered 2x2x2 mesh reproduce the assembled K."""
+    from ceos_b200 import meshgen
+    X, conn = meshgen.structured_box(2, 2, 2, jitter=0.05, seed=4)
+    m = O.Model(X, conn, [O.NH_Q1P0], [[1.0, 50.0]])
+    rng = np.random.default_rng(1)
+    U = 0.05 * (X @ rng.uniform(-1, 1, (3, 3)).T).reshape(-1) + 0.01 * rng.uniform(-1, 1, X.size)
+    f0, kval, rc, _ = m.evaluate(0.0, U)
+    assert rc == 0
+    rowmap, col = m.pattern()
+    n = X.size
+    K = np.zeros((n, n))
+    for r in range(n):
+        for p in range(rowmap[r] - 1, rowmap[r + 1] - 1):
+            K[r, col[p] - 1] = kval[p]
+            K[col[p] - 1, r] = kval[p]
+    h = 1e-7
+    for j in range(0, n, 5):
+        e = np.zeros(n)
+        e[j] = h
+        fp, _, _, _ = m.evaluate(0.0, U + e, tangent=False)
+        fm, _, _, _ = m.evaluate(0.0, U - e, tangent=False)
+        assert np.abs((fp - fm) / (2 * h) - K[:, j]).max() <= 1e-5 * np.abs(K).max(), j
