@@ -23,6 +23,11 @@ OPT_TIME_KERNELS = 2
 
 _lib = None
 
+# int (*)(void* user, double time, int load_case, int step, int cutback, int substep, int flag_end_step,
+#         int n_iterations, int n_dof, const double* U)
+STEP_CALLBACK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                            C.c_int, C.POINTER(C.c_double))
+
 
 class CeosError(RuntimeError):
     """Non-zero status of a C-ABI call (ClassStatus error convention)."""
@@ -74,6 +79,8 @@ def lib():
         L.ceos_destroy.restype = None
         L.ceos_analysis.argtypes = [P, I, P, P, I, P, I, P, P, P, I, P, P, P, D, I, I, I, I, P, P, I, P, P, I, P,
                                     ip, P]
+        L.ceos_analysis_set_callback.argtypes = [P, STEP_CALLBACK, P]
+        L.ceos_analysis_set_initial.argtypes = [P, P]
         _lib = L
     return _lib
 
@@ -227,7 +234,12 @@ class ElementLoop:
         _check(lib().ceos_gp_stress(self._h, _ptr(out)))
         return out.reshape(self.n_elem, 8, 6)
 
-    def analysis(self, bc, tol, itmax, norm_mode, norm_type=2, max_cutbacks=10, probe_dofs=(), max_log=100000):
+    def analysis(self, bc, tol, itmax, norm_mode, norm_type=2, max_cutbacks=10, probe_dofs=(), max_log=100000,
+                 on_step=None, U0=None):
+        """Quasi-static analysis of one load case through ceos_analysis.  on_step(time, load_case, step,
+        cutback, substep, flag_end_step, n_iterations, U) is called for every converged substep (the
+        WriteFEMResults call sites); a True return stops the analysis.  U0 starts from given
+        displacements (a restart) instead of zero."""
         n_steps = len(bc["t0"])
         iters = np.zeros(n_steps, np.int32)
         cuts = np.zeros(n_steps, np.int32)
@@ -245,6 +257,22 @@ class ElementLoop:
             keep.append(x)
             return _ptr(x)
 
+        cb = None
+        if on_step is not None:
+            def _cb(user, t, lc, st, cut, sub, flag, nit, ndof, U):
+                try:
+                    return 1 if on_step(t, lc, st, cut, sub, flag, nit, np.ctypeslib.as_array(U, (ndof,)).copy()) \
+                        else 0
+                except Exception:  # an exception cannot cross the C frame: stop the analysis instead
+                    import traceback
+                    traceback.print_exc()
+                    return 1
+            cb = STEP_CALLBACK(_cb)
+        _check(lib().ceos_analysis_set_callback(self._h, cb if cb is not None else STEP_CALLBACK(), None))
+        U0 = _f64(U0).reshape(-1) if U0 is not None else None
+        if U0 is not None and U0.size != self.n_dof:
+            raise ValueError(f"U0 has {U0.size} entries, the mesh {self.n_dof} dofs")
+        _check(lib().ceos_analysis_set_initial(self._h, _ptr(U0)))
         rc = lib().ceos_analysis(
             self._h, n_steps, arr(bc["t0"], np.float64), arr(bc["dt"], np.float64),
             len(bc["fixed"]), arr(bc["fixed"], np.int32),
@@ -254,6 +282,7 @@ class ElementLoop:
             arr(bc["force_final"], np.float64),
             tol, itmax, norm_mode, norm_type, max_cutbacks, _ptr(iters), _ptr(cuts), len(probe_dofs),
             _ptr(probe_dofs), _ptr(probe), max_log, _ptr(log), C.byref(nlog), _ptr(Uf))
+        lib().ceos_analysis_set_callback(self._h, STEP_CALLBACK(), None)
         return {"rc": rc, "iters": iters, "cutbacks": cuts, "probe": probe.reshape(len(probe_dofs), n_steps),
                 "norms": log[:min(nlog.value, max_log)], "U": Uf}
 

@@ -47,6 +47,10 @@ struct Handle {
     cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr, ev_k2 = nullptr;
     int grid_cap = 148, blocks_per_sm = 1;
     std::string msg;
+    // host analysis driver: per-substep result callback and the starting U of a restart
+    ceos_step_callback step_cb = nullptr;
+    void* step_user = nullptr;
+    std::vector<double> U_start;          // empty: start from U = 0
 
     size_t elem_bytes() const { return precision == CEOS_FP64 ? sizeof(double) : sizeof(float); }
     size_t state_bytes() const { return (size_t)nstate * 8 * ld * elem_bytes(); }

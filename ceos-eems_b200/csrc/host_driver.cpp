@@ -142,6 +142,24 @@ void symv_upper(int n, const int* rowmap, const int* col, const double* val, con
 
 }  // namespace
 
+extern "C" int ceos_analysis_set_callback(void* handle, ceos_step_callback cb, void* user) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h) return CEOS_E_ARG;
+    h->step_cb = cb;
+    h->step_user = cb ? user : nullptr;
+    return 0;
+}
+
+extern "C" int ceos_analysis_set_initial(void* handle, const double* U0) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h) return CEOS_E_ARG;
+    if (U0)
+        h->U_start.assign(U0, U0 + 3 * (size_t)h->n_nodes);
+    else
+        h->U_start.clear();
+    return 0;
+}
+
 extern "C" int ceos_analysis(void* handle, int n_steps, const double* step_t0, const double* step_dt, int n_fixed,
                              const int* fixed_dofs, int n_presc, const int* presc_dofs, const double* presc_init,
                              const double* presc_final, int n_force, const int* force_dofs, const double* force_init,
@@ -172,6 +190,11 @@ extern "C" int ceos_analysis(void* handle, int n_steps, const double* step_t0, c
     SkylineLDLT lin;
     lin.analyse(h);
     std::vector<double> U(n, 0.0), Uconv(n), Ubar(n), Ubar0(n), Fext(n), Fext0(n), dFext(n), dUp(n);
+    if (!h->U_start.empty()) {  // restart: U of the last converged step
+        if ((int)h->U_start.size() != n) return CEOS_E_ARG;
+        U = h->U_start;
+        h->U_start.clear();
+    }
     std::vector<double> X(n), R(n), fint(n), kval(nnz), DX(n), Ud(n), Rmod(n), mR(n);
     const double GR = (1.0 + std::sqrt(5.0)) / 2.0;
     int nl = 0;
@@ -192,7 +215,7 @@ extern "C" int ceos_analysis(void* handle, int n_steps, const double* step_t0, c
         Ubar0 = U;
         Uconv = U;
         double alpha = 1.0, alpha_min = 0.0, alpha_aux;
-        int CutBack = 0;
+        int CutBack = 0, SubStep = 0;
         while (true) {
             const double Time = step_t0[ST] + alpha * step_dt[ST];
             for (int i = 0; i < n; ++i) {
@@ -251,6 +274,7 @@ extern "C" int ceos_analysis(void* handle, int n_steps, const double* step_t0, c
             if (!converged) {
                 alpha = alpha_min + (1.0 - 1.0 / GR) * (alpha - alpha_min);
                 ++CutBack;
+                SubStep = 1;
                 if (CutBack > max_cutbacks) {
                     if (n_log) *n_log = nl;
                     return -10;
@@ -258,15 +282,24 @@ extern "C" int ceos_analysis(void* handle, int n_steps, const double* step_t0, c
                 continue;
             }
             U = X;
+            ++SubStep;
             if (alpha == 1.0) {
                 if (iters) iters[ST] = it;
                 if (cutbacks) cutbacks[ST] = CutBack;
+                if (h->step_cb && h->step_cb(h->step_user, Time, 1, ST + 1, CutBack, SubStep, 1, it, n, U.data())) {
+                    if (n_log) *n_log = nl;
+                    return CEOS_E_ABORTED;
+                }
                 break;
             }
             alpha_aux = alpha_min;
             alpha_min = alpha;
             alpha = std::min(alpha + GR * (alpha - alpha_aux), 1.0);
             Uconv = U;
+            if (h->step_cb && h->step_cb(h->step_user, Time, 1, ST + 1, CutBack, SubStep, 0, it, n, U.data())) {
+                if (n_log) *n_log = nl;
+                return CEOS_E_ABORTED;
+            }
         }
         // SwitchConvergedState; the evaluation time of the last converged iteration is committed
         rc = ceos_commit_state(handle);

@@ -49,7 +49,8 @@ enum ceos_precision {
 
 enum ceos_error {
     CEOS_E_ARG = -1, CEOS_E_CUDA = -2, CEOS_E_ALLOC = -3, CEOS_E_MESH = -4, CEOS_E_MODEL = -5,
-    CEOS_E_SOLVER = -6 /* iterative solver did not reach its tolerance */
+    CEOS_E_SOLVER = -6, /* iterative solver did not reach its tolerance */
+    CEOS_E_ABORTED = -7 /* a step callback asked the analysis driver to stop */
 };
 
 /* Mesh as the reference holds it: CoordX interleaved [3*n_nodes] (ModNodes.f90:55),
@@ -257,6 +258,22 @@ void ceos_fe2_destroy(void* handle);
  * sparse LDL^T in place of PARDISO.  Arrays as in the reference: dofs 1-based,
  * *_init/_final item-major [n_items*n_steps]; norm_mode 0 relative, 1 absolute;
  * norm_type 2 max-abs, 1 L2.  Outputs as documented for each array. */
+/* Result callback of ceos_analysis, the call sites of WriteFEMResults in QuasiStaticAnalysisFEM
+ * (ModFEMAnalysis.f90:1314-1337): called once per converged substep with the analysis time,
+ * the load case (1), the step (1-based among the steps of this call), the cut-back and substep
+ * counters as the reference keeps them (a cut back sets SubStep = 1, a converged substep adds
+ * 1), Flag_EndStep (1 when alpha = 1, the end of the step), the Newton iterations of that
+ * substep and U [n_dof] (host memory, valid during the call).  A nonzero return stops the
+ * analysis with CEOS_E_ABORTED. */
+typedef int (*ceos_step_callback)(void* user, double time, int load_case, int step, int cutback, int substep,
+                                  int flag_end_step, int n_iterations, int n_dof, const double* U);
+/* Installs (cb != NULL) or removes the result callback of this handle. */
+int ceos_analysis_set_callback(void* handle, ceos_step_callback cb, void* user);
+/* Starting displacements of the next ceos_analysis on this handle (RestartAnalysis,
+ * ModFEMAnalysis.f90:2827-2956: U of the last converged step read back from FEMAnalysis.result);
+ * U0 [n_dof] is copied, NULL clears it.  The next ceos_analysis consumes it. */
+int ceos_analysis_set_initial(void* handle, const double* U0);
+
 int ceos_analysis(void* handle, int n_steps, const double* step_t0, const double* step_dt,
                   int n_fixed, const int* fixed_dofs,
                   int n_presc, const int* presc_dofs, const double* presc_init, const double* presc_final,

@@ -9,7 +9,8 @@ conditions and the Newton driver (96 Hexa8 elements, 195 nodes, 50 load steps, t
 This script reads their input files (GiD-12 Mesh.dat, tables, time discretization) and expected
 outputs (MARC displacement curves of node 11, NumOfIterRef.dat, the per-iteration NORM lines of
 Log_CEOS.txt) and writes them as JSON fixtures, so that the tests never read the reference tree
-at run time.
+at run time.  It also copies each case's text files unchanged (line ends normalised) into
+tests/golden/cases/<case>/, the inputs of the case-file reader and of the Checker workflow.
 
 Usage:  python tests/golden/make_golden.py /path/to/reference
 """
@@ -17,6 +18,9 @@ import json
 import os
 import re
 import sys
+
+CASE_FILES = ["Settings.dat", "Mesh.dat", "Time_Discretization.dat", "Table_Disp_Z.tab", "Table_Load_Y.tab",
+              "Post_Processing.post", "marc_disp_x.dat", "marc_disp_y.dat", "marc_disp_z.dat", "NumOfIterRef.dat"]
 
 CASES = [
     ("Checker/Cases/NonLinear_FEA_3D_Hexa8_StVenant", "hexa8_svk.json",
@@ -148,7 +152,15 @@ def main(ref):
             "log_norms": read_log_norms(os.path.join(case, "Log_CEOS.txt")),
         }
         fx.update(mesh)
-        out = os.path.join(os.path.dirname(os.path.abspath(__file__)), out_name)
+        here = os.path.dirname(os.path.abspath(__file__))
+        cdir = os.path.join(here, "cases", out_name[:-5])
+        os.makedirs(cdir, exist_ok=True)
+        for name in CASE_FILES:
+            with open(os.path.join(case, name), "r", encoding="latin-1") as f:
+                text = f.read().replace("\r\n", "\n")
+            with open(os.path.join(cdir, name), "w", encoding="latin-1") as f:
+                f.write(text)
+        out = os.path.join(here, out_name)
         with open(out, "w") as f:
             json.dump(fx, f, separators=(",", ":"))
         print("wrote", out, "nodes", len(mesh["X"]) // 3, "elements", len(mesh["conn"]) // 8)
