@@ -481,12 +481,25 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                 T f0 = 0, f1 = 0, f2 = 0;
                 T Kd[6] = {0, 0, 0, 0, 0, 0};
                 T Ko[4][9];
-#pragma unroll
-                for (int o = 0; o < 4; ++o)
-#pragma unroll
-                    for (int k = 0; k < 9; ++k) Ko[o][k] = T(0);
                 // Mean Dilatation: Bdiv of node b and of its partners, sum_gp w detJ grad N (current)
                 T bdb[3] = {T(0), T(0), T(0)}, bda[4][3] = {};
+                // FP32: the 3x3 blocks accumulate two columns per packed FMA (sm_100 FFMA2).  Row 0
+                // pairs column 2 with the geometric term g_a . sigma g_b, which enters the diagonal
+                // of the block once after the Gauss-point loop.
+                float2 Pa[4][3], Pc[4], Da = {0.f, 0.f}, Dc = {0.f, 0.f};
+                float Pr[4][2], d11 = 0.f, d12 = 0.f, d22 = 0.f;
+                if constexpr (sizeof(T) == 4) {
+#pragma unroll
+                    for (int o = 0; o < 4; ++o) {
+                        Pa[o][0] = Pa[o][1] = Pa[o][2] = Pc[o] = make_float2(0.f, 0.f);
+                        Pr[o][0] = Pr[o][1] = 0.f;
+                    }
+                } else {
+#pragma unroll
+                    for (int o = 0; o < 4; ++o)
+#pragma unroll
+                        for (int k = 0; k < 9; ++k) Ko[o][k] = T(0);
+                }
 #pragma unroll 1
                 for (int gp = 0; gp < 8; ++gp) {
                     const T* src = sds + (size_t)gp * 7 * kTileE * 4 + el * 4;
@@ -524,36 +537,92 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                         DB[i][1] = d1 * gy + d3 * gx + d4 * gz;
                         DB[i][2] = d2 * gz + d4 * gy + d5 * gx;
                     }
-                    // diagonal block (b,b), upper 6
-                    {
-                        const T geo = gx * q0 + gy * q1 + gz * q2;
-                        Kd[0] += gx * DB[0][0] + gy * DB[3][0] + gz * DB[5][0] + geo;
-                        Kd[1] += gx * DB[0][1] + gy * DB[3][1] + gz * DB[5][1];
-                        Kd[2] += gx * DB[0][2] + gy * DB[3][2] + gz * DB[5][2];
-                        Kd[3] += gy * DB[1][1] + gx * DB[3][1] + gz * DB[4][1] + geo;
-                        Kd[4] += gy * DB[1][2] + gx * DB[3][2] + gz * DB[4][2];
-                        Kd[5] += gz * DB[2][2] + gy * DB[4][2] + gx * DB[5][2] + geo;
+                    if constexpr (sizeof(T) == 4) {
+                        float2 P[6];
+#pragma unroll
+                        for (int i = 0; i < 6; ++i) P[i] = make_float2(DB[i][0], DB[i][1]);
+                        const float2 z0 = make_float2(DB[0][2], q0), z3 = make_float2(DB[3][2], q1),
+                                     z5 = make_float2(DB[5][2], q2);
+                        {   // diagonal block (b,b), upper 6
+                            const float2 bx = make_float2(gx, gx), by = make_float2(gy, gy), bz = make_float2(gz, gz);
+                            Da = __ffma2_rn(bx, P[0], Da); Da = __ffma2_rn(by, P[3], Da); Da = __ffma2_rn(bz, P[5], Da);
+                            Dc = __ffma2_rn(bx, z0, Dc);   Dc = __ffma2_rn(by, z3, Dc);   Dc = __ffma2_rn(bz, z5, Dc);
+                            d11 += gy * P[1].y + gx * P[3].y + gz * P[4].y;
+                            d12 += gy * DB[1][2] + gx * DB[3][2] + gz * DB[4][2];
+                            d22 += gz * DB[2][2] + gy * DB[4][2] + gx * DB[5][2];
+                        }
+#pragma unroll
+                        for (int o = 0; o < 4; ++o) {
+                            if (o < npair) {
+                                const int an = (b + 1 + o) & 7;
+                                T ax, ay, az;
+                                ld4<T>(gsrc + an * kTileE * 4, ax, ay, az, pad);
+                                if constexpr (MODEL == M_NH_Q1P0) {
+                                    bda[o][0] += wgp * ax;
+                                    bda[o][1] += wgp * ay;
+                                    bda[o][2] += wgp * az;
+                                }
+                                const float2 bx = make_float2(ax, ax), by = make_float2(ay, ay), bz = make_float2(az, az);
+                                Pa[o][0] = __ffma2_rn(bx, P[0], Pa[o][0]);
+                                Pa[o][0] = __ffma2_rn(by, P[3], Pa[o][0]);
+                                Pa[o][0] = __ffma2_rn(bz, P[5], Pa[o][0]);
+                                Pc[o] = __ffma2_rn(bx, z0, Pc[o]);
+                                Pc[o] = __ffma2_rn(by, z3, Pc[o]);
+                                Pc[o] = __ffma2_rn(bz, z5, Pc[o]);
+                                Pa[o][1] = __ffma2_rn(by, P[1], Pa[o][1]);
+                                Pa[o][1] = __ffma2_rn(bx, P[3], Pa[o][1]);
+                                Pa[o][1] = __ffma2_rn(bz, P[4], Pa[o][1]);
+                                Pr[o][0] += ay * DB[1][2] + ax * DB[3][2] + az * DB[4][2];
+                                Pa[o][2] = __ffma2_rn(bz, P[2], Pa[o][2]);
+                                Pa[o][2] = __ffma2_rn(by, P[4], Pa[o][2]);
+                                Pa[o][2] = __ffma2_rn(bx, P[5], Pa[o][2]);
+                                Pr[o][1] += az * DB[2][2] + ay * DB[4][2] + ax * DB[5][2];
+                            }
+                        }
+                    } else {
+                        // diagonal block (b,b), upper 6
+                        {
+                            const T geo = gx * q0 + gy * q1 + gz * q2;
+                            Kd[0] += gx * DB[0][0] + gy * DB[3][0] + gz * DB[5][0] + geo;
+                            Kd[1] += gx * DB[0][1] + gy * DB[3][1] + gz * DB[5][1];
+                            Kd[2] += gx * DB[0][2] + gy * DB[3][2] + gz * DB[5][2];
+                            Kd[3] += gy * DB[1][1] + gx * DB[3][1] + gz * DB[4][1] + geo;
+                            Kd[4] += gy * DB[1][2] + gx * DB[3][2] + gz * DB[4][2];
+                            Kd[5] += gz * DB[2][2] + gy * DB[4][2] + gx * DB[5][2] + geo;
+                        }
+#pragma unroll
+                        for (int o = 0; o < 4; ++o) {
+                            if (o < npair) {
+                                const int an = (b + 1 + o) & 7;
+                                T ax, ay, az;
+                                ld4<T>(gsrc + an * kTileE * 4, ax, ay, az, pad);
+                                const T geo = ax * q0 + ay * q1 + az * q2;
+                                if constexpr (MODEL == M_NH_Q1P0) {
+                                    bda[o][0] += wgp * ax;
+                                    bda[o][1] += wgp * ay;
+                                    bda[o][2] += wgp * az;
+                                }
+#pragma unroll
+                                for (int l = 0; l < 3; ++l) {
+                                    Ko[o][0 * 3 + l] += ax * DB[0][l] + ay * DB[3][l] + az * DB[5][l];
+                                    Ko[o][1 * 3 + l] += ay * DB[1][l] + ax * DB[3][l] + az * DB[4][l];
+                                    Ko[o][2 * 3 + l] += az * DB[2][l] + ay * DB[4][l] + ax * DB[5][l];
+                                }
+                                Ko[o][0] += geo; Ko[o][4] += geo; Ko[o][8] += geo;
+                            }
+                        }
                     }
+                }
+                if constexpr (sizeof(T) == 4) {  // unpack the column pairs, add the geometric terms
+                    const float gb = Dc.y;
+                    Kd[0] = Da.x + gb; Kd[1] = Da.y; Kd[2] = Dc.x;
+                    Kd[3] = d11 + gb;  Kd[4] = d12;  Kd[5] = d22 + gb;
 #pragma unroll
                     for (int o = 0; o < 4; ++o) {
-                        if (o < npair) {
-                            const int an = (b + 1 + o) & 7;
-                            T ax, ay, az;
-                            ld4<T>(gsrc + an * kTileE * 4, ax, ay, az, pad);
-                            const T geo = ax * q0 + ay * q1 + az * q2;
-                            if constexpr (MODEL == M_NH_Q1P0) {
-                                bda[o][0] += wgp * ax;
-                                bda[o][1] += wgp * ay;
-                                bda[o][2] += wgp * az;
-                            }
-#pragma unroll
-                            for (int l = 0; l < 3; ++l) {
-                                Ko[o][0 * 3 + l] += ax * DB[0][l] + ay * DB[3][l] + az * DB[5][l];
-                                Ko[o][1 * 3 + l] += ay * DB[1][l] + ax * DB[3][l] + az * DB[4][l];
-                                Ko[o][2 * 3 + l] += az * DB[2][l] + ay * DB[4][l] + ax * DB[5][l];
-                            }
-                            Ko[o][0] += geo; Ko[o][4] += geo; Ko[o][8] += geo;
-                        }
+                        const float ga = Pc[o].y;
+                        Ko[o][0] = Pa[o][0].x + ga; Ko[o][1] = Pa[o][0].y; Ko[o][2] = Pc[o].x;
+                        Ko[o][3] = Pa[o][1].x;      Ko[o][4] = Pa[o][1].y + ga; Ko[o][5] = Pr[o][0];
+                        Ko[o][6] = Pa[o][2].x;      Ko[o][7] = Pa[o][2].y; Ko[o][8] = Pr[o][1] + ga;
                     }
                 }
                 if constexpr (MODEL == M_NH_Q1P0) {  // Bdiv^T Bdiv d2psi/dJbar2 / V0 (ModElement.f90:463-466)
