@@ -315,7 +315,9 @@ def main():
     from ceos_b200 import meshgen
     X, conn = meshgen.structured_box(args.nx, args.nx, args.nx, jitter=0.05, seed=0)
     n_elem, n_gp = conn.shape[0], 8 * conn.shape[0]
-    config = {"workload": WORKLOAD, "mesh": f"{args.nx}^3 Hexa8", "elements": int(n_elem), "gauss_points": int(n_gp),
+    workload = WORKLOAD if args.nx == 64 else (f"visco-Prony {args.nx}^3 Hexa8 ({int(n_elem)} elements, "
+                                               f"{int(n_gp)} GPs), cyclic simple shear")
+    config = {"workload": workload, "mesh": f"{args.nx}^3 Hexa8", "elements": int(n_elem), "gauss_points": int(n_gp),
               "material": "Neo-Hookean mu=1 K=100 + 3 Maxwell branches (0.3,0.01s),(0.2,0.1s),(0.1,1s)",
               "precision": "FP32 element arithmetic/state, FP64 detF/lnJ/K/f_int",
               "l2": "inputs larger than L2 (K 262 MB + state 403 MB per step)", "parallelism": f"replicas x{args.gpus}"}
