@@ -432,8 +432,8 @@ def main():
         t = torch.tensor([e2e_s], device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    # sanity: the device result equals the host result
-    assert torch.allclose(dfint.cpu(), f_pin, rtol=0, atol=0)
+    # sanity: the device result equals the host result (up to the summation order of the atomics)
+    assert torch.allclose(dfint.cpu(), f_pin, rtol=1e-10, atol=1e-12 * float(f_pin.abs().max()))
 
     ms_step = ms / args.steps
     value = world * n_gp * args.steps / (ms * 1e-3)

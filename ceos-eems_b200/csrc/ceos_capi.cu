@@ -76,12 +76,15 @@ void model_init_state(int model, double* st) {
 template <typename T>
 size_t elem_smem(const Handle* h) { return SmemLayout<T>(h->ns_used).total; }
 
+// One launch of the element loop over elements [e0, e1) and, in mixed mode with a tangent, the
+// conversion of the node row blocks [n0, n1) (final once every element touching them has run).
 template <typename T, int MODEL>
-int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
+int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s, int e0, int e1,
+                 int n0, int n1) {
     ElemArgs<T> a;
     a.n_elem = h->n_elem;
-    a.e_begin = 0;
-    a.e_end = h->n_elem;
+    a.e_begin = e0;
+    a.e_end = e1;
     for (int k = 0; k < 12; ++k) a.pu[k] = T(0);
     if (h->param_mode == 0)
         for (int k = 0; k < h->n_params && k < 12; ++k) a.pu[k] = (T)h->host_params[k];
@@ -117,13 +120,15 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
     int grid = std::min(n_tiles, h->grid_cap);
     const bool timed = (h->options & CEOS_OPT_TIME_KERNELS) && h->ev_k0;
     if (timed) CK(cudaEventRecord(h->ev_k0, s));
-    element_loop_kernel<T, MODEL, (sizeof(T) == 4)><<<grid, kThreads, smem, s>>>(a);
-    CK(cudaGetLastError());
+    if (n_tiles > 0) {
+        element_loop_kernel<T, MODEL, (sizeof(T) == 4)><<<grid, kThreads, smem, s>>>(a);
+        CK(cudaGetLastError());
+    }
     if (timed) CK(cudaEventRecord(h->ev_k1, s));
-    if (sizeof(T) == 4 && dkval) {
+    if (sizeof(T) == 4 && dkval && n1 > n0) {
         // FP32 node-pair blocks -> FP64 CSR (every K entry written once), scratch re-zeroed
-        const int cgrid = h->grid_cap > 0 ? 148 * 8 : 1184;
-        kblock_to_csr_kernel<<<cgrid, 256, 0, s>>>(h->n_nodes, h->d_rs, h->d_nup, h->d_kblk, dkval);
+        const int cgrid = std::min(h->grid_cap > 0 ? 148 * 8 : 1184, (n1 - n0 + 7) / 8);
+        kblock_to_csr_kernel<<<cgrid, 256, 0, s>>>(n0, n1, h->d_rs, h->d_nup, h->d_kblk, dkval);
         CK(cudaGetLastError());
     }
     if (timed) CK(cudaEventRecord(h->ev_k2, s));
@@ -131,16 +136,17 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
 }
 
 template <typename T>
-int launch_elem(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
+int launch_elem(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s, int e0, int e1,
+                int n0, int n1) {
     switch (h->model) {
-        case M_CNH: return launch_model<T, M_CNH>(h, dt, dU, dfint, dkval, s);
-        case M_NH_Q1P0: return launch_model<T, M_NH_Q1P0>(h, dt, dU, dfint, dkval, s);
-        case M_SVK: return launch_model<T, M_SVK>(h, dt, dU, dfint, dkval, s);
-        case M_J2_SMALL: return launch_model<T, M_J2_SMALL>(h, dt, dU, dfint, dkval, s);
-        case M_VISCO_PRONY: return launch_model<T, M_VISCO_PRONY>(h, dt, dU, dfint, dkval, s);
-        case M_J2_FINITE: return launch_model<T, M_J2_FINITE>(h, dt, dU, dfint, dkval, s);
-        case M_VISCO_VAR: return launch_model<T, M_VISCO_VAR>(h, dt, dU, dfint, dkval, s);
-        case M_EXTERNAL: return launch_model<T, M_EXTERNAL>(h, dt, dU, dfint, dkval, s);
+        case M_CNH: return launch_model<T, M_CNH>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
+        case M_NH_Q1P0: return launch_model<T, M_NH_Q1P0>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
+        case M_SVK: return launch_model<T, M_SVK>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
+        case M_J2_SMALL: return launch_model<T, M_J2_SMALL>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
+        case M_VISCO_PRONY: return launch_model<T, M_VISCO_PRONY>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
+        case M_J2_FINITE: return launch_model<T, M_J2_FINITE>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
+        case M_VISCO_VAR: return launch_model<T, M_VISCO_VAR>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
+        case M_EXTERNAL: return launch_model<T, M_EXTERNAL>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
     }
     return CEOS_E_MODEL;
 }
@@ -377,19 +383,65 @@ extern "C" int ceos_slot_map(void* handle, long long* out) {
 }
 
 namespace ceos {
-int evaluate_device(Handle* h, double time, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
+// Clears the accumulators of one evaluation on stream s.
+static int evaluate_prologue(Handle* h, double time, double* dfint, double* dkval, cudaStream_t s) {
     CK(cudaSetDevice(h->device));
-    const double dt = time - h->time_old;
     h->time_eval = time;
     CK(cudaMemsetAsync(h->d_status_count, 0, sizeof(int), s));
     CK(cudaMemsetAsync(dfint, 0, sizeof(double) * 3 * (size_t)h->n_nodes, s));
     // FP64 mode accumulates straight into K (zeroed here); the mixed mode writes every K entry
     // from its FP32 block scratch, so K needs no clearing.
     if (dkval && h->precision == CEOS_FP64) CK(cudaMemsetAsync(dkval, 0, sizeof(double) * (size_t)h->nnz, s));
-    int rc = (h->precision == CEOS_FP64) ? launch_elem<double>(h, dt, dU, dfint, dkval, s)
-                                         : launch_elem<float>(h, dt, dU, dfint, dkval, s);
+    return 0;
+}
+
+static int evaluate_range(Handle* h, double time, const double* dU, double* dfint, double* dkval, cudaStream_t s,
+                          int e0, int e1, int n0, int n1) {
+    const double dt = time - h->time_old;
+    return (h->precision == CEOS_FP64) ? launch_elem<double>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1)
+                                       : launch_elem<float>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
+}
+
+int evaluate_device(Handle* h, double time, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
+    int rc = evaluate_prologue(h, time, dfint, dkval, s);
+    if (rc) return rc;
+    rc = evaluate_range(h, time, dU, dfint, dkval, s, 0, h->n_elem, 0, h->n_nodes);
     if (rc) return rc;
     h->evaluated = true;
+    return 0;
+}
+
+// Slab plan of the host-buffer evaluation: n_slabs element ranges; after slab c every node whose
+// elements all lie in slabs <= c is final, and the final nodes form the prefix [0, slab_node_end[c])
+// of the row order (a running maximum over the nodes of the last slab touching them).  Meshes whose
+// numbering follows a sweep (structured or banded) finish a growing prefix after every slab; any
+// other numbering simply leaves the copies to the end.
+static int plan_slabs(Handle* h) {
+    const int kMinElemPerSlab = 16384;
+    int ns = std::min(4, h->n_elem / kMinElemPerSlab);
+    if (ns < 1) ns = 1;
+    // boundaries on whole tiles of kTileE elements: the kernel stages state rows with 16-byte copies
+    // from st_old + e_begin + 32 t, which must stay 16-byte aligned
+    h->slab_e.assign(ns + 1, 0);
+    for (int c = 1; c < ns; ++c) h->slab_e[c] = (int)((long long)h->n_elem * c / ns / kTileE * kTileE);
+    h->slab_e[ns] = h->n_elem;
+    std::vector<int> last(h->n_nodes, 0);
+    for (int c = 0; c < ns; ++c)
+        for (int e = h->slab_e[c]; e < h->slab_e[c + 1]; ++e)
+            for (int k = 0; k < 8; ++k) last[h->conn0[(size_t)8 * e + k]] = c;
+    h->slab_node_end.assign(ns, 0);
+    int run = 0, n = 0;
+    for (int c = 0; c < ns; ++c) {
+        while (n < h->n_nodes && std::max(run, last[n]) <= c) run = std::max(run, last[n++]);
+        h->slab_node_end[c] = n;
+    }
+    h->slab_node_end[ns - 1] = h->n_nodes;
+    if (ns > 1) {
+        CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+        h->slab_ev.assign(ns, nullptr);
+        for (auto& ev : h->slab_ev) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    h->n_slabs = ns;
     return 0;
 }
 }  // namespace ceos
@@ -424,11 +476,43 @@ extern "C" int ceos_evaluate(void* handle, double time, const double* U, double*
     CK(cudaSetDevice(h->device));
     cudaStream_t s = h->stream;
     const size_t nd = 3 * (size_t)h->n_nodes;
+    if (h->n_slabs == 0) {
+        const int rc = plan_slabs(h);
+        if (rc) return rc;
+    }
     CK(cudaMemcpyAsync(h->d_U, U, nd * sizeof(double), cudaMemcpyHostToDevice, s));
-    int rc = evaluate_device(h, time, h->d_U, h->d_fint, kval ? h->d_kval : nullptr, s);
+    double* dk = kval ? h->d_kval : nullptr;
+    int rc = evaluate_prologue(h, time, h->d_fint, dk, s);
     if (rc) return rc;
-    CK(cudaMemcpyAsync(fint, h->d_fint, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (kval) CK(cudaMemcpyAsync(kval, h->d_kval, (size_t)h->nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->n_slabs == 1) {
+        rc = evaluate_range(h, time, h->d_U, h->d_fint, dk, s, 0, h->n_elem, 0, h->n_nodes);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(fint, h->d_fint, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (kval) CK(cudaMemcpyAsync(kval, h->d_kval, (size_t)h->nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
+    } else {
+        // slab c computes on s; the rows it finished travel to the host on copy_stream meanwhile
+        int n_done = 0;
+        for (int c = 0; c < h->n_slabs; ++c) {
+            const int n_end = h->slab_node_end[c];
+            rc = evaluate_range(h, time, h->d_U, h->d_fint, dk, s, h->slab_e[c], h->slab_e[c + 1], n_done, n_end);
+            if (rc) return rc;
+            if (n_end > n_done) {
+                CK(cudaEventRecord(h->slab_ev[c], s));
+                CK(cudaStreamWaitEvent(h->copy_stream, h->slab_ev[c], 0));
+                CK(cudaMemcpyAsync(fint + 3 * (size_t)n_done, h->d_fint + 3 * (size_t)n_done,
+                                   3 * (size_t)(n_end - n_done) * sizeof(double), cudaMemcpyDeviceToHost,
+                                   h->copy_stream));
+                if (kval) {
+                    const long long k0 = h->rs[n_done], k1 = n_end < h->n_nodes ? h->rs[n_end] : h->nnz;
+                    CK(cudaMemcpyAsync(kval + k0, h->d_kval + k0, (size_t)(k1 - k0) * sizeof(double),
+                                       cudaMemcpyDeviceToHost, h->copy_stream));
+                }
+            }
+            n_done = n_end;
+        }
+        CK(cudaStreamSynchronize(h->copy_stream));
+    }
+    h->evaluated = true;
     CK(cudaStreamSynchronize(s));
     return ceos_status(handle, n_failed);
 }
@@ -775,6 +859,9 @@ Handle::~Handle() {
     if (ev_k0) cudaEventDestroy(ev_k0);
     if (ev_k1) cudaEventDestroy(ev_k1);
     if (ev_k2) cudaEventDestroy(ev_k2);
+    for (cudaEvent_t ev : slab_ev)
+        if (ev) cudaEventDestroy(ev);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     if (stream) cudaStreamDestroy(stream);
 }
 

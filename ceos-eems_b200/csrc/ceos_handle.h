@@ -45,6 +45,13 @@ struct Handle {
     double time_old = 0.0, time_eval = 0.0;
     int options = 0;
     cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr, ev_k2 = nullptr;
+    // host-buffer evaluation in element slabs: after slab c the node rows [0, slab_node_end[c]) are final
+    // and go to the host on copy_stream while the next slabs compute
+    int n_slabs = 0;                      // 0: plan not built yet
+    std::vector<int> slab_e;              // [n_slabs + 1] element boundaries
+    std::vector<int> slab_node_end;       // [n_slabs] final node-row prefix after each slab
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> slab_ev;
     int grid_cap = 148, blocks_per_sm = 1;
     std::string msg;
     // host analysis driver: per-substep result callback and the starting U of a restart

@@ -239,11 +239,11 @@ CEOS_D void finalize_row_block(int node, long long rs, int m, float* kblk, doubl
 }
 
 // Block scratch -> FP64 CSR values of K, one warp per node row block; leaves the scratch zero.
-__global__ void __launch_bounds__(256) kblock_to_csr_kernel(int n_nodes, const long long* __restrict__ rs,
+__global__ void __launch_bounds__(256) kblock_to_csr_kernel(int n_begin, int n_end, const long long* __restrict__ rs,
                                                             const int* __restrict__ nup, float* kblk, double* K) {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; n < n_nodes; n += warps)
+    for (int n = n_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); n < n_end; n += warps)
         finalize_row_block(n, __ldg(rs + n), __ldg(nup + n), kblk, K, lane);
 }
 
