@@ -309,22 +309,25 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
             const int gp = warp, el = lane, e = e0 + el;
             if (e < a.e_end) {
                 int status = 0;
-                T JX[3][3] = {}, Jc[3][3] = {};
+                // J_X = sum dN/dxi (x) X and J_u = sum dN/dxi (x) u; the current Jacobian is J_X + J_u, and
+                // F = I + (J_X^-1 J_u)^T equals DeformationGradient's I + sum u (x) grad_X N with the
+                // displacement gradient formed from small numbers (no I + O(1) cancellation in FP32)
+                T JX[3][3] = {}, Ju[3][3] = {};
 #pragma unroll
                 for (int n = 0; n < 8; ++n) {
-                    T X[3], x[3];
+                    T X[3], u[3];
                     if constexpr (sizeof(T) == 4) {
                         const float4* q = reinterpret_cast<const float4*>(sxf + (n * kTileE + el) * 8);
                         const float4 xv = q[0], uv = q[1];
                         X[0] = xv.x; X[1] = xv.y; X[2] = xv.z;
-                        x[0] = xv.x + uv.x; x[1] = xv.y + uv.y; x[2] = xv.z + uv.z;
+                        u[0] = uv.x; u[1] = uv.y; u[2] = uv.z;
                     } else {
                         const double* xp = sx + (n * kTileE + el) * 3;
                         const double* up = su + (n * kTileE + el) * 3;
 #pragma unroll
                         for (int d = 0; d < 3; ++d) {
                             X[d] = (T)xp[d];
-                            x[d] = (T)(xp[d] + up[d]);
+                            u[d] = (T)up[d];
                         }
                     }
 #pragma unroll
@@ -333,40 +336,37 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
 #pragma unroll
                         for (int j = 0; j < 3; ++j) {
                             JX[i][j] += dn * X[j];
-                            Jc[i][j] += dn * x[j];
+                            Ju[i][j] += dn * u[j];
                         }
                     }
                 }
+                T Jc[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) Jc[i][j] = JX[i][j] + Ju[i][j];
                 const T detJX = det3(JX);
                 const T detJ = det3(Jc);
                 if (!(detJX > T(1.0e-13)) || !(detJ > T(1.0e-13))) status |= 1;
                 T JXi[3][3], Jci[3][3];
                 inv3(JX, detJX, JXi);
                 inv3(Jc, detJ, Jci);
-                T F[3][3] = {{T(1), T(0), T(0)}, {T(0), T(1), T(0)}, {T(0), T(0), T(1)}};
+                // F[i][j] = delta_ij + sum_k JXi[j][k] Ju[k][i]
+                T F[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        F[i][j] = (i == j ? T(1) : T(0)) + (JXi[j][0] * Ju[0][i] + JXi[j][1] * Ju[1][i] + JXi[j][2] * Ju[2][i]);
+                // current gradients grad_x N of the 8 nodes for phase B
 #pragma unroll
                 for (int n = 0; n < 8; ++n) {
                     const T d0 = (T)c_dN[gp][n][0], d1 = (T)c_dN[gp][n][1], d2 = (T)c_dN[gp][n][2];
-                    T gX[3], gx[3];
+                    T gx[3];
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        gX[j] = JXi[j][0] * d0 + JXi[j][1] * d1 + JXi[j][2] * d2;
+                    for (int j = 0; j < 3; ++j)
                         gx[j] = (status & 1) ? T(0) : Jci[j][0] * d0 + Jci[j][1] * d1 + Jci[j][2] * d2;
-                    }
                     st4<T>(sg + ((gp * 8 + n) * kTileE + el) * 4, gx[0], gx[1], gx[2], T(0));
-                    T uu[3];
-                    if constexpr (sizeof(T) == 4) {
-                        const float4 uv = reinterpret_cast<const float4*>(sxf + (n * kTileE + el) * 8)[1];
-                        uu[0] = uv.x; uu[1] = uv.y; uu[2] = uv.z;
-                    } else {
-                        const double* up = su + (n * kTileE + el) * 3;
-                        uu[0] = (T)up[0]; uu[1] = (T)up[1]; uu[2] = (T)up[2];
-                    }
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) F[i][j] += uu[i] * gX[j];
-                    }
                 }
                 // constitutive update
                 T p[NP];
