@@ -77,7 +77,7 @@ def run_cpu_sample(X, conn, threads, nz_layers=4, reps=1):
         dt = time.perf_counter() - t0
         best = dt if best is None else min(best, dt)
     n_gp = 8 * cs.shape[0]
-    return n_gp / best, n_gp, best
+    return n_gp / best, n_gp, best, m
 
 
 def clocks_sampler_start(path):
@@ -327,7 +327,7 @@ def main():
             return
         threads = os.cpu_count() or 1
         reps = max(1, min(args.steps, 3))
-        rate, n_sample, secs = run_cpu_sample(X, conn, threads, nz_layers=args.nx, reps=reps)
+        rate, n_sample, secs, _ = run_cpu_sample(X, conn, threads, nz_layers=args.nx, reps=reps)
         sample = f"whole mesh ({n_sample // 8} elements, {n_sample} GPs) per step, FP64, best of {reps}"
         line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": warmup, "ms_per_step": secs * 1e3 * n_gp / n_sample,
@@ -455,10 +455,23 @@ def main():
             "clocks": clocks}
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        rate, n_sample, secs = run_cpu_sample(X, conn, threads, nz_layers=args.nx)
+        rate, n_sample, secs, m = run_cpu_sample(X, conn, threads, nz_layers=args.nx)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"one evaluation of the whole mesh ({n_sample // 8} elements), FP64 "
                                           f"oracle on {threads} threads, {secs:.2f} s"}
+        # error of the measured evaluation against the FP64 oracle at the same state: the oracle has
+        # the same history (increments at DT and 2 DT committed) and evaluates the timed U at 3 DT
+        m.commit()
+        m.set_time_old(2 * DT)
+        f_o, k_o, rc_o, _ = m.evaluate(t_eval, U_host)
+        if rc_o == 0:
+            f_g, k_g = f_pin.numpy(), K_pin.numpy()
+            line["error_vs_fp64_oracle"] = {
+                "f_int_rel": float(np.abs(f_g - f_o).max() / np.abs(f_o).max()),
+                "K_rel": float(np.abs(k_g - k_o).max() / np.abs(k_o).max()),
+                "K_rel_fro": float(np.linalg.norm(k_g - k_o) / np.linalg.norm(k_o)),
+                "what": "max |GPU - oracle| / max |oracle| over all f_int and K entries of the timed evaluation "
+                        f"(mixed precision GPU vs FP64 oracle, {args.nx}^3 mesh, same Gauss-point history)"}
     if rank == 0:
         print(json.dumps(line))
     g.close()

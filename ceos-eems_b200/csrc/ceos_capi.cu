@@ -93,7 +93,6 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
         for (int k = 0; k < 4 && k < (int)h->host_params[2]; ++k)
             a.ebr[k] = (T)std::exp(-dt / (2.0 * h->host_params[4 + 2 * k]));
     a.X = h->d_X;
-    a.Xf = h->d_Xf;
     a.U = dU;
     a.conn = h->d_conn;
     a.rs = h->d_rs;
@@ -759,13 +758,6 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     CK(cudaMalloc(&d_X, 3 * N * sizeof(double)));
     CK(cudaMemcpy(d_X, mesh->X, 3 * N * sizeof(double), cudaMemcpyHostToDevice));
-    if (precision == CEOS_MIXED) {
-        std::vector<float> xf(4 * N, 0.f);
-        for (size_t n = 0; n < N; ++n)
-            for (int d = 0; d < 3; ++d) xf[4 * n + d] = (float)mesh->X[3 * n + d];
-        CK(cudaMalloc(&d_Xf, 4 * N * sizeof(float)));
-        CK(cudaMemcpy(d_Xf, xf.data(), 4 * N * sizeof(float), cudaMemcpyHostToDevice));
-    }
     CK(cudaMalloc(&d_U, 3 * N * sizeof(double)));
     CK(cudaMemset(d_U, 0, 3 * N * sizeof(double)));
     CK(cudaMalloc(&d_fint, 3 * N * sizeof(double)));
@@ -853,7 +845,7 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
 Handle::~Handle() {
     if (stream) cudaStreamSynchronize(stream);
     void* ptrs[] = {d_X, d_U, d_fint, d_kval, d_conn, d_rs, d_nup, d_ranks, d_elem_status, d_status_count,
-                    d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress, d_kblk, d_Xf};
+                    d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress, d_kblk};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (ev_k0) cudaEventDestroy(ev_k0);

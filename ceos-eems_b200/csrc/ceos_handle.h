@@ -27,7 +27,6 @@ struct Handle {
     // device buffers
     cudaStream_t stream = nullptr;
     double *d_X = nullptr, *d_U = nullptr, *d_fint = nullptr, *d_kval = nullptr;
-    float4* d_Xf = nullptr;               // mixed mode: reference coordinates in FP32
     int* d_conn = nullptr;
     long long* d_rs = nullptr;
     int* d_nup = nullptr;

@@ -39,7 +39,6 @@ struct ElemArgs {
     int n_elem;
     int e_begin, e_end;     // element range of this launch
     const double* X;        // [3*n_nodes] reference coordinates (CoordX)
-    const float4* Xf;       // [n_nodes] reference coordinates in FP32 (CEOS_MIXED)
     const double* U;        // [3*n_nodes] displacements, DOF 3n+d
     const int* conn;        // [n_elem*8] 0-based node ids
     const long long* rs;    // [n_nodes] CSR position of the first entry of row 3n (0-based)
@@ -79,9 +78,12 @@ struct SmemLayout {
         g = take(sizeof(T) * 8 * 8 * kTileE * 4);        // [gp][node][e][4]: grad N (current)
         ds = take(sizeof(T) * 8 * 7 * kTileE * 4);       // [gp][quad][e][4]: w detJ (D upper 21, sigma 6)
         st = take(sizeof(T) * (size_t)(ns > 0 ? ns : 1) * 8 * kTileE);  // [v][gp][e]: committed state
-        x = take(sizeof(T) == 4 ? 16 : sizeof(double) * 8 * kTileE * 3);  // [node][e][3] (FP64 mode)
-        u = take(sizeof(double) * 8 * kTileE * 3);
-        xf = take(sizeof(T) == 4 ? sizeof(float) * 8 * kTileE * 8 : 16);  // [node][e][X 4 | U 4] in FP32
+        x = take(sizeof(double) * 8 * kTileE * 3);     // [node][e][3] staged X (FP64)
+        u = take(sizeof(double) * 8 * kTileE * 3);     // [node][e][3] staged U (FP64)
+        // FP32 mode: [node][e][dX 4 | dU 4], element-local differences in FP32.  It overlays the
+        // FP64 staging of x and u (12 KB >= 8 KB, contiguous): the staging of a tile is converted
+        // before the tile computes, and the next tile is staged only after phase A stopped reading.
+        xf = sizeof(T) == 4 ? x : take(16);
         rs = take(sizeof(long long) * 2 * 8 * kTileE);  // double-buffered [buf][node][e]
         nup = take(sizeof(int) * 2 * 8 * kTileE);
         node = take(sizeof(int) * 2 * 8 * kTileE);
@@ -187,9 +189,7 @@ CEOS_D void prefetch_nodes_state(const ElemArgs<T>& a, int e0, const int* node_s
         const int node = node_s[n * kTileE + lane];
         const double* Up = a.U + 3 * (size_t)node;
         double* ud = us + (n * kTileE + lane) * 3;
-        if constexpr (sizeof(T) == 4) {
-            cp_async16(xf + (n * kTileE + lane) * 8, a.Xf + node);
-        } else {
+        {
             const double* Xp = a.X + 3 * (size_t)node;
             double* xd = xs + (n * kTileE + lane) * 3;
 #pragma unroll
@@ -296,11 +296,23 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
             cp_commit();
         }
         if constexpr (sizeof(T) == 4) {
-            // one FP64 -> FP32 conversion per (node, element) instead of one per Gauss point
+            // One FP64 -> FP32 conversion per (node, element), of the differences to the element's
+            // node 0: X_n - X_0 and u_n - u_0 are formed in FP64, so the FP32 values keep their
+            // relative precision at the element scale (absolute coordinates rounded to FP32 would
+            // perturb an element of size h by ~6e-8 / h, which the bulk modulus of a nearly
+            // incompressible material amplifies in f_int).  J_X and J_u are unchanged by the shift
+            // because sum_n dN_n/dxi = 0.
             const int n = warp, el = lane;
+            const double* xp = sx + (n * kTileE + el) * 3;
             const double* up = su + (n * kTileE + el) * 3;
+            const double* x0 = sx + el * 3;
+            const double* u0 = su + el * 3;
+            const float4 dx = make_float4((float)(xp[0] - x0[0]), (float)(xp[1] - x0[1]), (float)(xp[2] - x0[2]), 0.f);
+            const float4 du = make_float4((float)(up[0] - u0[0]), (float)(up[1] - u0[1]), (float)(up[2] - u0[2]), 0.f);
+            __syncthreads();  // every thread has read the FP64 staging that the FP32 tile overlays
             float4* dst = reinterpret_cast<float4*>(sxf + (n * kTileE + el) * 8);
-            dst[1] = make_float4((float)up[0], (float)up[1], (float)up[2], 0.f);
+            dst[0] = dx;
+            dst[1] = du;
             __syncthreads();
         }
 
