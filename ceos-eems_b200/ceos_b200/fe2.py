@@ -20,6 +20,7 @@ def _setup():
     L.ceos_fe2_set_warm_start.argtypes = [P, I]
     L.ceos_fe2_set_solver_ctas.argtypes = [P, I]
     L.ceos_fe2_set_solve_mask.argtypes = [P, P]
+    L.ceos_fe2_autotune.argtypes = [P, P, P, P, P, I]
     L.ceos_fe2_destroy.argtypes = [P]
     L.ceos_fe2_destroy.restype = None
     return L
@@ -72,6 +73,22 @@ class BatchedRVE:
     def set_solver_ctas(self, n=0):
         """RVEs the MINRES kernel keeps in flight (0: as many as occupancy allows)."""
         _check(lib().ceos_fe2_set_solver_ctas(self._h, n))
+
+    def autotune(self, Fbar):
+        """Time the MINRES launch shapes (threads per RVE x RVEs in flight) on the first Newton system of
+        every RVE at Fbar and keep the fastest for the following solves.  Returns {"threads", "ctas"
+        (0: occupancy limit), "ms": {(threads, in_flight): ms}}."""
+        Fbar = np.ascontiguousarray(np.asarray(Fbar, dtype=np.float64).reshape(self.n_rve, 9))
+        t, c = C.c_int(0), C.c_int(0)
+        ms = np.full(6, -1.0)
+        rc = lib().ceos_fe2_autotune(self._h, _ptr(Fbar), C.byref(t), C.byref(c), _ptr(ms), 6)
+        if rc:
+            buf = C.create_string_buffer(256)
+            lib().ceos_fe2_message(self._h, buf, 256)
+            raise CeosError(rc, buf.value.decode())
+        shapes = [(bs, w) for bs in (256, 512) for w in ("occupancy", "2/SM", "1/SM")]
+        return {"threads": t.value, "ctas": c.value,
+                "ms": {k: float(v) for k, v in zip(shapes, ms) if v >= 0}}
 
     def set_warm_start(self, on=True):
         """Continue every RVE from its last converged state (macro load path) on the next solves."""

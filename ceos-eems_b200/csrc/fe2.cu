@@ -45,6 +45,24 @@ struct Fe2 {
     double mu_m = 1.0, mu_f = 50.0, k_over_mu = 100.0;
     int allow_failures = 0;              // 1: RVEs that cannot converge are reported, not fatal
     int solver_ctas = 0;                 // RVEs solved concurrently by the MINRES kernel (0: automatic)
+    int solver_threads = kSolveThreads;  // threads per RVE of the MINRES kernel (autotuned: 256 or 512)
+    // CUDA graphs of one continuation round, captured on first use and replayed every round:
+    // g_assemble = Fbar upload, assembly, failed-element count, residual norms;
+    // g_solve = per-RVE operations, linear solve, iteration counts, Newton step.
+    // They exchange data with the host through pinned buffers at fixed addresses.
+    cudaGraphExec_t g_assemble = nullptr, g_solve = nullptr;
+    double* hp_Fs = nullptr;             // pinned [n_rve*9]
+    double* hp_rn = nullptr;             // pinned [n_rve]
+    double* hp_eta = nullptr;            // pinned [n_rve]
+    int* hp_op = nullptr;                // pinned [n_rve]
+    int* hp_need = nullptr;              // pinned [n_rve]
+    int* hp_cgi = nullptr;               // pinned [n_rve]
+    int* hp_status = nullptr;            // pinned [1] failed elements of the last assembly
+    void drop_graphs() {
+        if (g_assemble) cudaGraphExecDestroy(g_assemble);
+        if (g_solve) cudaGraphExecDestroy(g_solve);
+        g_assemble = g_solve = nullptr;
+    }
     int warm = 0;                        // 1: continue every RVE from its last converged state
     std::vector<double> F_prev;          // [n_rve][9] Fbar of the last converged state (warm start)
     std::vector<int> solve_mask;         // [n_rve] 0: RVE skipped by the next solves (empty: all solved)
@@ -92,6 +110,10 @@ struct Fe2 {
     double* d_X9 = nullptr;     // [9*n_red] solutions of the 9 condensation systems
     std::string msg;
     ~Fe2() {
+        drop_graphs();
+        void* hp[] = {hp_Fs, hp_rn, hp_eta, hp_op, hp_need, hp_cgi, hp_status};
+        for (void* q : hp)
+            if (q) cudaFreeHost(q);
         void* p[] = {d_node_off, d_red_off, d_ncell, d_rve_of_node, d_fmap, d_col, d_order, d_queue, d_Fbar, d_w,
                      d_u, d_rhs, d_dx, d_r64, d_y64, d_minv, d_rnorm, d_cg_iters, d_active, d_P, d_A, d_nn, d_Z, d_M, d_X9,
                      d_rve_of_elem, d_fail, d_op, d_wc, d_eta, d_rcol, d_gcoord, d_rve_of_blk, d_kell};
@@ -626,7 +648,8 @@ int run_solver(Fe2* f, int nrhs, const double* rhs, double* x, int max_inner, in
     CKF(cudaFuncSetAttribute(fe2_minres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, f->device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fe2_minres_kernel, kSolveThreads, smem);
+    const int bs = f->solver_threads;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fe2_minres_kernel, bs, smem);
     SolveArgs a;
     a.n_rve = f->n_rve;
     a.max_inner = max_inner;
@@ -658,7 +681,7 @@ int run_solver(Fe2* f, int nrhs, const double* rhs, double* x, int max_inner, in
     // one per SM, measured slower: 2.33 s vs 1.54 s for 512 RVEs of n = 8), or the caller's number
     int grid = std::max(1, std::min(f->n_rve, sms * std::max(per_sm, 1)));
     if (f->solver_ctas > 0) grid = std::max(1, std::min(grid, f->solver_ctas));
-    fe2_minres_kernel<<<grid, kSolveThreads, smem, h->stream>>>(a);
+    fe2_minres_kernel<<<grid, bs, smem, h->stream>>>(a);
     CKF(cudaGetLastError());
     return 0;
 }
@@ -683,6 +706,65 @@ int assemble(Fe2* f) {
     invert_blocks_kernel<<<(n_blk + 255) / 256, 256, 0, h->stream>>>(n_blk, f->d_rve_of_blk, f->d_red_off, f->d_kell,
                                                                       f->d_minv);
     CKF(cudaGetLastError());
+    return 0;
+}
+
+// The device work of one continuation round, recorded once into CUDA graphs (stream capture) and
+// replayed every round; the host exchanges Fbar, operations, tolerances, norms and iteration counts
+// through the pinned hp_* buffers.
+int record_assemble(Fe2* f) {
+    Handle* h = f->loop;
+    cudaStream_t s = h->stream;
+    const int nr = f->n_rve;
+    CKF(cudaMemcpyAsync(f->d_Fbar, f->hp_Fs, sizeof(double) * 9 * nr, cudaMemcpyHostToDevice, s));
+    const int rc = assemble(f);
+    if (rc) return rc;
+    CKF(cudaMemcpyAsync(f->hp_status, h->d_status_count, sizeof(int), cudaMemcpyDeviceToHost, s));
+    rve_norm_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_rhs, f->d_nn);
+    CKF(cudaGetLastError());
+    CKF(cudaMemcpyAsync(f->hp_rn, f->d_nn, sizeof(double) * nr, cudaMemcpyDeviceToHost, s));
+    return 0;
+}
+
+int record_solve(Fe2* f) {
+    Handle* h = f->loop;
+    cudaStream_t s = h->stream;
+    const int nr = f->n_rve;
+    CKF(cudaMemcpyAsync(f->d_op, f->hp_op, sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+    rve_op_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_op, f->d_w, f->d_dx, f->d_wc);
+    CKF(cudaGetLastError());
+    CKF(cudaMemcpyAsync(f->d_active, f->hp_need, sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+    CKF(cudaMemcpyAsync(f->d_eta, f->hp_eta, sizeof(double) * nr, cudaMemcpyHostToDevice, s));
+    const int rc = run_solver(f, 1, f->d_rhs, f->d_dx, 2000, 3);  // an inexact step is still a descent try
+    if (rc) return rc;
+    CKF(cudaMemcpyAsync(f->hp_cgi, f->d_cg_iters, sizeof(int) * nr, cudaMemcpyDeviceToHost, s));
+    rve_step_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_active, f->d_dx, f->d_w);
+    CKF(cudaGetLastError());
+    return 0;
+}
+
+// Capture record(f) on the handle's stream into *exec (nothing is executed while capturing).
+int capture(Fe2* f, int (*record)(Fe2*), cudaGraphExec_t* exec) {
+    cudaStream_t s = f->loop->stream;
+    CKF(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    const int rc = record(f);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &g);  // always ends the capture, also after an error
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        f->msg = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
+        return CEOS_E_CUDA;
+    }
+    const cudaError_t e2 = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) {
+        *exec = nullptr;
+        f->msg = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e2);
+        return CEOS_E_CUDA;
+    }
     return 0;
 }
 
@@ -831,6 +913,13 @@ extern "C" int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, 
     if (e == cudaSuccess) e = up((void**)&f->d_op, nullptr, sizeof(int) * n_rve);
     if (e == cudaSuccess) e = up((void**)&f->d_wc, nullptr, sizeof(double) * f->n_red);
     if (e == cudaSuccess) e = up((void**)&f->d_eta, nullptr, sizeof(double) * n_rve);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&f->hp_Fs, sizeof(double) * 9 * n_rve, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&f->hp_rn, sizeof(double) * n_rve, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&f->hp_eta, sizeof(double) * n_rve, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&f->hp_op, sizeof(int) * n_rve, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&f->hp_need, sizeof(int) * n_rve, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&f->hp_cgi, sizeof(int) * n_rve, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&f->hp_status, sizeof(int), cudaHostAllocDefault);
     if (e != cudaSuccess) { delete f; return CEOS_E_CUDA; }
     *handle = f;
     return 0;
@@ -880,9 +969,9 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
     const double golden = 0.6180339887498949;
     enum { kNewton = 0, kDone = 1, kFailed = 2 };
     std::vector<int> phase(nr, kNewton), nit(nr, 0), halv(nr, 0), cuts(nr, 0), its(nr, 0), cg_tot(nr, 0);
-    std::vector<int> op(nr), need(nr), fail(nr), cgi(nr);
+    std::vector<int> op(nr), need(nr), fail(nr);
     std::vector<double> a_done(nr, 0.0), da(nr, 1.0 / std::max(1, f->n_sub)), a_try(nr), r0(nr, 1.0), racc(nr, 0.0),
-        rn(nr), eta(nr, 1.0), Fs(9 * (size_t)nr);
+        rn(nr), eta(nr, 1.0);
     for (int r = 0; r < nr; ++r) a_try[r] = std::min(1.0, da[r]);
     for (int r = 0; r < nr && !f->solve_mask.empty(); ++r)
         if (!f->solve_mask[r]) {  // skipped: stays at its current state
@@ -897,13 +986,18 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
         for (int r = 0; r < nr; ++r)
             for (int k = 0; k < 9; ++k) {
                 const size_t i = 9 * (size_t)r + k;
-                Fs[i] = Fp[i] + a_try[r] * (Fbar[i] - Fp[i]);
+                f->hp_Fs[i] = Fp[i] + a_try[r] * (Fbar[i] - Fp[i]);
             }
-        CKF(cudaMemcpyAsync(f->d_Fbar, Fs.data(), sizeof(double) * Fs.size(), cudaMemcpyHostToDevice, s));
-        int rc = assemble(f);
+        int rc = f->g_assemble ? 0 : capture(f, record_assemble, &f->g_assemble);
         if (rc) return rc;
-        const int st = ceos_status(h, nullptr);
-        if (st < 0) return st;
+        CKF(cudaGraphLaunch(f->g_assemble, s));
+        CKF(cudaStreamSynchronize(s));
+        h->evaluated = true;
+        int st = 0;
+        if (*f->hp_status) {
+            st = ceos_status(h, nullptr);
+            if (st < 0) return st;
+        }
         std::fill(fail.begin(), fail.end(), 0);
         if (st) {
             CKF(cudaMemsetAsync(f->d_fail, 0, sizeof(int) * nr, s));
@@ -911,11 +1005,9 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
                                                                     f->d_fail);
             CKF(cudaGetLastError());
             CKF(cudaMemcpyAsync(fail.data(), f->d_fail, sizeof(int) * nr, cudaMemcpyDeviceToHost, s));
+            CKF(cudaStreamSynchronize(s));
         }
-        rve_norm_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_rhs, f->d_nn);
-        CKF(cudaGetLastError());
-        CKF(cudaMemcpyAsync(rn.data(), f->d_nn, sizeof(double) * nr, cudaMemcpyDeviceToHost, s));
-        CKF(cudaStreamSynchronize(s));
+        std::copy(f->hp_rn, f->hp_rn + nr, rn.begin());
         all_done = true;
         int n_need = 0, n_rej = 0, n_cut = 0;
         double worst = 0.0;
@@ -987,20 +1079,20 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
             std::fprintf(stderr, "fe2: round %d solving %d max rel residual %.3e rejected %d cut back %d\n", round,
                          n_need, worst, n_rej, n_cut);
         if (all_done) break;
-        CKF(cudaMemcpyAsync(f->d_op, op.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
-        rve_op_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_op, f->d_w, f->d_dx, f->d_wc);
-        CKF(cudaGetLastError());
+        std::copy(op.begin(), op.end(), f->hp_op);
         if (n_need) {
-            CKF(cudaMemcpyAsync(f->d_active, need.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
-            CKF(cudaMemcpyAsync(f->d_eta, eta.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, s));
-            rc = run_solver(f, 1, f->d_rhs, f->d_dx, 2000, 3);  // an inexact step is still a descent try
+            std::copy(need.begin(), need.end(), f->hp_need);
+            std::copy(eta.begin(), eta.end(), f->hp_eta);
+            rc = f->g_solve ? 0 : capture(f, record_solve, &f->g_solve);
             if (rc) return rc;
-            CKF(cudaMemcpyAsync(cgi.data(), f->d_cg_iters, sizeof(int) * nr, cudaMemcpyDeviceToHost, s));
-            rve_step_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_active, f->d_dx, f->d_w);
-            CKF(cudaGetLastError());
+            CKF(cudaGraphLaunch(f->g_solve, s));
             CKF(cudaStreamSynchronize(s));
             for (int r = 0; r < nr; ++r)
-                if (need[r]) cg_tot[r] += cgi[r];
+                if (need[r]) cg_tot[r] += f->hp_cgi[r];
+        } else {
+            CKF(cudaMemcpyAsync(f->d_op, f->hp_op, sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+            rve_op_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_op, f->d_w, f->d_dx, f->d_wc);
+            CKF(cudaGetLastError());
         }
     }
     if (!all_done) {
@@ -1093,6 +1185,90 @@ extern "C" int ceos_fe2_set_solver_ctas(void* handle, int n) {
     Fe2* f = static_cast<Fe2*>(handle);
     if (!f || n < 0) return CEOS_E_ARG;
     f->solver_ctas = n;
+    f->drop_graphs();  // the solve graph holds the launch shape
+    return 0;
+}
+
+// Autotuner of the MINRES launch shape (threads per RVE x RVEs in flight): assembles the first
+// Newton system of every RVE at Fbar (row-major [n_rve][9]) from its current fluctuations, times
+// the linear solve of that system (Newton forcing 1e-2, the typical first tolerance) once per
+// candidate with CUDA events, keeps the fastest shape and reports it.  The fluctuations are not
+// changed.  ms_out (n_cand entries, or NULL) receives the times in the order threads {256, 512}
+// x RVEs in flight {occupancy limit, 2 per SM, 1 per SM}; candidates that coincide report -1.
+extern "C" int ceos_fe2_autotune(void* handle, const double* Fbar, int* threads, int* ctas, double* ms_out,
+                                 int n_cand) {
+    Fe2* f = static_cast<Fe2*>(handle);
+    if (!f || !Fbar) return CEOS_E_ARG;
+    Handle* h = f->loop;
+    cudaStream_t s = h->stream;
+    const int nr = f->n_rve;
+    CKF(cudaSetDevice(f->device));
+    std::copy(Fbar, Fbar + 9 * (size_t)nr, f->hp_Fs);
+    f->drop_graphs();
+    int rc = record_assemble(f);
+    if (rc) return rc;
+    for (int r = 0; r < nr; ++r) {
+        f->hp_need[r] = 1;
+        f->hp_eta[r] = 1e-2;
+    }
+    CKF(cudaMemcpyAsync(f->d_active, f->hp_need, sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+    CKF(cudaMemcpyAsync(f->d_eta, f->hp_eta, sizeof(double) * nr, cudaMemcpyHostToDevice, s));
+    int max_m = 0;
+    for (int r = 0; r < nr; ++r) max_m = std::max(max_m, f->red_off[r + 1] - f->red_off[r]);
+    const size_t smem = solve_smem_bytes(max_m);
+    CKF(cudaFuncSetAttribute(fe2_minres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, f->device);
+    cudaEvent_t e0, e1;
+    CKF(cudaEventCreate(&e0));
+    CKF(cudaEventCreate(&e1));
+    const int keep_threads = f->solver_threads, keep_ctas = f->solver_ctas;
+    int best_t = keep_threads, best_c = keep_ctas, k = 0;
+    float best_ms = -1.f;
+    std::vector<long long> seen;
+    for (int bs : {256, 512}) {
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fe2_minres_kernel, bs, smem);
+        const int full = std::max(1, std::min(nr, sms * std::max(per_sm, 1)));
+        for (int c : {0, 2 * sms, sms}) {
+            const int grid = c == 0 ? full : std::max(1, std::min(full, c));
+            const long long key = (long long)bs << 32 | grid;
+            float ms = -1.f;
+            if (std::find(seen.begin(), seen.end(), key) == seen.end()) {
+                seen.push_back(key);
+                f->solver_threads = bs;
+                f->solver_ctas = c == 0 ? 0 : grid;
+                CKF(cudaMemsetAsync(f->d_dx, 0, sizeof(double) * f->n_red, s));
+                CKF(cudaEventRecord(e0, s));
+                rc = run_solver(f, 1, f->d_rhs, f->d_dx, 2000, 3);
+                if (rc) break;
+                CKF(cudaEventRecord(e1, s));
+                CKF(cudaEventSynchronize(e1));
+                CKF(cudaEventElapsedTime(&ms, e0, e1));
+                if (best_ms < 0.f || ms < best_ms) {
+                    best_ms = ms;
+                    best_t = bs;
+                    best_c = f->solver_ctas;
+                }
+            }
+            if (ms_out && k < n_cand) ms_out[k] = ms;
+            ++k;
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CKF(cudaMemsetAsync(f->d_dx, 0, sizeof(double) * f->n_red, s));
+    CKF(cudaStreamSynchronize(s));
+    if (rc) {
+        f->solver_threads = keep_threads;
+        f->solver_ctas = keep_ctas;
+        return rc;
+    }
+    f->solver_threads = best_t;
+    f->solver_ctas = best_c;
+    if (threads) *threads = best_t;
+    if (ctas) *ctas = best_c;
     return 0;
 }
 
@@ -1110,6 +1286,7 @@ extern "C" int ceos_fe2_set_allow_failures(void* handle, int allow) {
 extern "C" int ceos_fe2_set_fractions(void* handle, const double* vf) {
     Fe2* f = static_cast<Fe2*>(handle);
     if (!f || !vf) return CEOS_E_ARG;
+    f->drop_graphs();
     std::vector<double> eparams;
     eparams.reserve(2 * (size_t)f->loop->n_elem);
     std::vector<int> changed(f->n_rve, 0);

@@ -248,6 +248,12 @@ int ceos_fe2_set_solve_mask(void* handle, const int* mask);
  * RVEs whose fraction changes restart from the undeformed state, the others keep a warm state. */
 int ceos_fe2_set_fractions(void* handle, const double* vf);
 /* Description of the last failure of ceos_fe2_solve (empty when none). */
+/* Autotuner of the MINRES launch shape: times the first linear solve of every RVE at Fbar
+ * ([n_rve][9], row-major) for threads per RVE {256, 512} x RVEs in flight {occupancy limit,
+ * 2 per SM, 1 per SM}, keeps the fastest for the following solves and returns it in threads and
+ * ctas (0 = occupancy limit).  ms_out[n_cand] (or NULL) receives the candidates' times (-1 for
+ * duplicates).  The RVE fluctuations are unchanged.  No reference counterpart. */
+int ceos_fe2_autotune(void* handle, const double* Fbar, int* threads, int* ctas, double* ms_out, int n_cand);
 int ceos_fe2_message(void* handle, char* msg, int msg_len);
 void ceos_fe2_destroy(void* handle);
 

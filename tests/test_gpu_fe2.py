@@ -85,3 +85,26 @@ def test_warm_start_and_mask_follow_the_load_path():
     warm.set_solve_mask(None)
     cold.close()
     warm.close()
+
+
+def test_autotuned_launch_shape_and_graph_replay():
+    """The autotuner times the MINRES launch shapes on the batch's own first systems and keeps one;
+    solves with it (round work replayed from CUDA graphs) give the same P as the default shape, a
+    second solve on the same handle reuses the graphs, and changing the shape re-captures them."""
+    n, vf = fe2.sample_rve_family(40, seed=7, n_range=(4, 8))
+    Fb = fe2.sample_macro_F(40, seed=8, amp=0.1)
+    ref = fe2.BatchedRVE(n, vf)
+    P0 = ref.solve(Fb)["P"]
+    ref.close()
+    b = fe2.BatchedRVE(n, vf)
+    tune = b.autotune(Fb)
+    assert tune["threads"] in (256, 512) and tune["ctas"] >= 0
+    assert len(tune["ms"]) >= 2 and all(v > 0 for v in tune["ms"].values())
+    out = b.solve(Fb)
+    assert np.abs(out["P"] - P0).max() <= 1e-6 * np.abs(P0).max()
+    again = b.solve(Fb)           # cold start again on the same handle: the replayed graphs give the same P
+    assert np.abs(again["P"] - out["P"]).max() <= 1e-7 * np.abs(P0).max()   # to the Newton tolerance
+    b.set_solver_ctas(8)          # another shape: the solve graph is captured anew
+    P8 = b.solve(Fb)["P"]
+    assert np.abs(P8 - P0).max() <= 1e-6 * np.abs(P0).max()
+    b.close()

@@ -113,6 +113,33 @@ def test_evaluate_mixed(model, params, amp, tol):
     g.close()
 
 
+def test_mixed_near_incompressible_shear_patch():
+    """Mixed precision on the benchmark's problem (visco-Prony, K = 100 mu, simple shear after two
+    committed increments) on a 16^3 mesh: the interior nodal forces cancel, so f_int is small against
+    the element forces and exposes any loss of element-scale precision.  The element-local
+    coordinate and displacement differences keep f_int within 2e-6 and K within 2e-6 of the FP64
+    oracle (relative to their largest entries); rounding absolute coordinates to FP32 gave 1.7e-4."""
+    X, conn = meshgen.structured_box(16, 16, 16, jitter=0.05, seed=0)
+    g, o = _pair(G.VISCO_PRONY, PRONY_P, X, conn, precision=G.MIXED)
+
+    def shear(t):
+        U = np.zeros_like(X)
+        U[:, 0] = 0.3 * np.sin(2.0 * np.pi * t) * X[:, 2]
+        return U.reshape(-1)
+
+    for k in (1, 2):
+        t = 0.025 * k
+        g.evaluate(t, shear(t), tangent=False)
+        o.evaluate(t, shear(t), tangent=False)
+        g.commit(); o.commit(); g.set_committed_time(t); o.set_time_old(t)
+    fg, kg, rc, _ = g.evaluate(0.075, shear(0.075))
+    fo, ko, _, _ = o.evaluate(0.075, shear(0.075))
+    assert rc == 0
+    assert relerr(fg, fo) <= 2e-6
+    assert relerr(kg, ko) <= 2e-6
+    g.close()
+
+
 def test_per_element_params():
     X, conn = meshgen.structured_box(4, 4, 3, jitter=0.05, seed=5)
     rng = np.random.default_rng(9)

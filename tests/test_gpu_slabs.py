@@ -45,9 +45,10 @@ def test_slab_pipelined_host_call_equals_device_call(n, scramble, precision, rto
         f_d, k_d = df.cpu().numpy(), dk.cpu().numpy()
         assert np.abs(f_h - f_d).max() <= rtol * np.abs(f_d).max()
         assert np.abs(k_h - k_d).max() <= rtol * np.abs(k_d).max()
-        # every K entry was written by the host call (the result does not depend on what kval held)
+        # every K entry was written by the host call: a second call into fresh zeros gives K again
+        # (an entry the call skipped would stay 0; exact zero counts are not compared, since a sum of
+        # FP32 contributions may cancel to 0.0 in one atomic order and not in another)
         f_h2, k_h2, _, _ = g.evaluate(0.1, U)
         assert np.abs(k_h2 - k_d).max() <= rtol * np.abs(k_d).max()
-        assert np.count_nonzero(k_h) == np.count_nonzero(k_d)
     finally:
         g.close()
