@@ -95,7 +95,7 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
     a.X = h->d_X;
     a.U = dU;
     a.conn = h->d_conn;
-    a.rs = h->d_rs;
+    a.rs = (sizeof(T) == 4) ? h->d_blk0 : h->d_rs;
     a.nup = h->d_nup;
     a.ranks = h->d_ranks;
     a.fint = dfint;
@@ -766,6 +766,12 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
     CK(cudaMemcpy(d_conn, conn0.data(), 8 * E * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&d_rs, N * sizeof(long long)));
     CK(cudaMemcpy(d_rs, rs.data(), N * sizeof(long long), cudaMemcpyHostToDevice));
+    if (precision == CEOS_MIXED) {  // first node-pair block of each node: n + (rs[n] - 6n) / 9
+        std::vector<long long> blk0(N);
+        for (size_t n = 0; n < N; ++n) blk0[n] = (long long)n + (rs[n] - 6LL * (long long)n) / 9;
+        CK(cudaMalloc(&d_blk0, N * sizeof(long long)));
+        CK(cudaMemcpy(d_blk0, blk0.data(), N * sizeof(long long), cudaMemcpyHostToDevice));
+    }
     CK(cudaMalloc(&d_nup, N * sizeof(int)));
     CK(cudaMemcpy(d_nup, nup.data(), N * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&d_ranks, E * 32));
@@ -844,7 +850,7 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
 
 Handle::~Handle() {
     if (stream) cudaStreamSynchronize(stream);
-    void* ptrs[] = {d_X, d_U, d_fint, d_kval, d_conn, d_rs, d_nup, d_ranks, d_elem_status, d_status_count,
+    void* ptrs[] = {d_X, d_U, d_fint, d_kval, d_conn, d_rs, d_blk0, d_nup, d_ranks, d_elem_status, d_status_count,
                     d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress, d_kblk};
     for (void* p : ptrs)
         if (p) cudaFree(p);

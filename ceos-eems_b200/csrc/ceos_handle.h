@@ -29,6 +29,7 @@ struct Handle {
     double *d_X = nullptr, *d_U = nullptr, *d_fint = nullptr, *d_kval = nullptr;
     int* d_conn = nullptr;
     long long* d_rs = nullptr;
+    long long* d_blk0 = nullptr;          // mixed mode: first node-pair block of each node
     int* d_nup = nullptr;
     uint32_t* d_ranks = nullptr;
     uint8_t* d_elem_status = nullptr;

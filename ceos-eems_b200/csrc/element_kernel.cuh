@@ -41,7 +41,8 @@ struct ElemArgs {
     const double* X;        // [3*n_nodes] reference coordinates (CoordX)
     const double* U;        // [3*n_nodes] displacements, DOF 3n+d
     const int* conn;        // [n_elem*8] 0-based node ids
-    const long long* rs;    // [n_nodes] CSR position of the first entry of row 3n (0-based)
+    const long long* rs;    // [n_nodes] CSR position of the first entry of row 3n (0-based); blocked
+                            // assembly: the first node-pair block of node n instead
     const int* nup;         // [n_nodes] number of neighbour nodes with a larger id
     const uint32_t* ranks;  // [n_elem*8] 28 uint8 slot ranks per element (32 bytes)
     double* fint;           // [3*n_nodes]
@@ -708,8 +709,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                 if (a.kval && BLOCKED) {
                     // node-pair blocks: one 16-byte vector reduction per block row
                     {
-                        const long long r0 = rs_c[b * kTileE + el];
-                        float* blk = a.kblk + ((long long)Bn + (r0 - 6LL * Bn) / 9) * 12;
+                        float* blk = a.kblk + rs_c[b * kTileE + el] * 12;  // rs holds the first block of the node
                         red_v4(blk + 0, (float)Kd[0], (float)Kd[1], (float)Kd[2], 0.f);
                         red_v4(blk + 4, 0.f, (float)Kd[3], (float)Kd[4], 0.f);
                         red_v4(blk + 8, 0.f, 0.f, (float)Kd[5], 0.f);
@@ -724,9 +724,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
                             const int r = rk[pair_index(lo_local, hi_local)];
                             const bool a_low = An < Bn;
                             const int lo_n = a_low ? an : b;
-                            const int lo_node = a_low ? An : Bn;
-                            const long long r0 = rs_c[lo_n * kTileE + el];
-                            float* blk = a.kblk + ((long long)lo_node + (r0 - 6LL * lo_node) / 9 + 1 + r) * 12;
+                            float* blk = a.kblk + (rs_c[lo_n * kTileE + el] + 1 + r) * 12;
                             if (a_low) {  // rows of node a: M[k][:]
                                 red_v4(blk + 0, (float)Ko[o][0], (float)Ko[o][1], (float)Ko[o][2], 0.f);
                                 red_v4(blk + 4, (float)Ko[o][3], (float)Ko[o][4], (float)Ko[o][5], 0.f);
