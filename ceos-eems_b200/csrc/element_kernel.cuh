@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
 #pragma unroll
                         for (int k = 0; k < 9; ++k) Ko[o][k] = T(0);
                 }
-#pragma unroll 1
+#pragma unroll 2
                 for (int gp = 0; gp < 8; ++gp) {
                     const T* src = sds + (size_t)gp * 7 * kTileE * 4 + el * 4;
                     T Dm[21], s0, s1, s2, s3, s4, s5, pad;
