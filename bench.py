@@ -27,6 +27,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -374,7 +375,8 @@ def main():
     rc, nf = g.status()
     assert rc == 0, ("element failures", rc, nf)
 
-    clk_path = os.path.join(ROOT, "gpurun_out", f"bench_clocks_r{rank}.csv")
+    clk_path = os.path.join(os.environ.get("CEOS_BENCH_CLOCKS_DIR", tempfile.gettempdir()),
+                            f"ceos_bench_clocks_r{rank}_{os.getpid()}.csv")
     os.makedirs(os.path.dirname(clk_path), exist_ok=True)
     sampler = clocks_sampler_start(clk_path)
     time.sleep(0.3)

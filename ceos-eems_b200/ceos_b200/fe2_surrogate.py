@@ -3,7 +3,7 @@
 Training pairs (C, vf) -> S come from the batched RVE solver itself (ceos_fe2_*): F = I + G with
 G_ij uniform in [-amp, amp] (det F > 0) and vf uniform in vf_range, one fixed RVE resolution
 n_cells (the homogenized response depends on the resolution, so the surrogate stands in for the
-RVE family of that resolution).  The RVE solver is also the judge of the surrogate's error."""
+RVE family of that resolution).  The RVE solver is also the reference the surrogate's error is measured against."""
 import time
 
 import numpy as np

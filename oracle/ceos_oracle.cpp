@@ -385,7 +385,10 @@ void visco_prony(const double* p, const M3 F, double dt, const double* st_old, d
 // Algorithm: Simo (1988) / Simo & Hughes, Computational Inelasticity (1998), Box 9.1:
 // trial b_e = F Cp^{-1} F^T, radial return on s = mu dev(bbar_e), U(J) = K/2 (1/2 (J^2-1) - ln J).
 // The return mapping (closed form for linear hardening) runs in FP64.  The consistent
-// spatial tangent is derived from the Lie derivative of tau; it is not
+// spatial tangent is the algorithmic one of Simo (1988) (Simo & Hughes 1998, Box 9.2), formed on
+// the Kirchhoff stress and divided by J: volumetric K J^2 1(x)1 - K (J^2 - 1) I, the trial
+// deviatoric modulus 2 mubar (I - 1(x)1/3) - 2/3 (s(x)1 + 1(x)s), and, when plastic, that
+// modulus scaled by (1 - beta1) with the rank-one return-mapping corrections in n.  It is not
 // symmetric and is symmetrized (D + D^T)/2 because the global matrix is stored symmetric.
 // params = [E, nu, sigma_y0, H]; state = [Cp^{-1} (Voigt 6), alpha].
 void j2_finite(const double* p, const M3 F, const double* st_old, double* st_new, double sig[6],

@@ -1,4 +1,4 @@
-"""CPU checks of the FP64 RVE oracle used to judge the batched FE^2 solver."""
+"""CPU checks of the FP64 RVE oracle that checks the batched FE^2 solver."""
 import numpy as np
 
 import fe2_oracle as F2

@@ -1,4 +1,4 @@
-"""CPU checks of the FP64 surrogate oracle that judges the GPU training and inference kernels:
+"""CPU checks of the FP64 surrogate oracle that checks the GPU training and inference kernels:
 its double-backprop parameter gradient, input gradient and Hessian against central finite
 differences."""
 import numpy as np
