@@ -114,6 +114,23 @@ def clocks_summary(path, dev):
             "samples": len(sm)}
 
 
+def max_over_ranks(x, world, device):
+    """The largest x over all ranks (the job is as slow as its slowest rank); x itself when world == 1.
+    device: where the reduction tensor lives ("cuda:k" under NCCL, "cpu" under gloo)."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, seconds):
+    """Aggregate throughput of N replicas that each processed units_per_rank in the max-over-ranks time."""
+    return world * units_per_rank / seconds
+
+
 def measured_peak_hbm():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -390,11 +407,7 @@ def main():
         step()
     ev1.record(stream)
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world, f"cuda:{dev}")
     # kernel-only durations for the roofline (events around the element-loop launch)
     g.set_options(G.OPT_TIME_KERNELS)
     kms, cms = [], []
@@ -429,16 +442,12 @@ def main():
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         e2e_step()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world, f"cuda:{dev}")
     # sanity: the device result equals the host result (up to the summation order of the atomics)
     assert torch.allclose(dfint.cpu(), f_pin, rtol=1e-10, atol=1e-12 * float(f_pin.abs().max()))
 
     ms_step = ms / args.steps
-    value = world * n_gp * args.steps / (ms * 1e-3)
+    value = whole_job_rate(n_gp * args.steps, world, ms * 1e-3)
     alg = algorithmic_bytes(g.n_nodes, n_elem, n_gp, n_dof, nnz)
     kmean = float(np.mean(kms)) * 1e-3
     peak, peak_kind = measured_peak_hbm()
@@ -446,7 +455,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic", "config": config,
-            "e2e": {"value": world * n_gp / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * n_dof,
+            "e2e": {"value": whole_job_rate(n_gp, world, e2e_s), "unit": UNIT, "h2d_bytes_per_step": 8 * n_dof,
                     "d2h_bytes_per_step": 8 * (n_dof + nnz)},
             "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
