@@ -81,6 +81,23 @@ def run_cpu_sample(X, conn, threads, nz_layers=4, reps=1):
     return n_gp / best, n_gp, best, m
 
 
+def run_cpu_single(X, conn, nz_layers=4):
+    """The oracle's element loop on one thread (the reference's serial loop) over the first nz_layers
+    element layers, after one committed increment; returns (GP updates/s, GPs, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    Xs, cs = cpu_slab(X, conn, nz_layers)
+    m = O.Model(Xs, cs, [O.VISCO_PRONY], PRONY)
+    m.evaluate_sample(DT, shear_u(Xs, DT), cs.shape[0], 1)
+    m.commit()
+    m.set_time_old(DT)
+    t0 = time.perf_counter()
+    m.evaluate_sample(2 * DT, shear_u(Xs, 2 * DT), cs.shape[0], 1)
+    secs = time.perf_counter() - t0
+    n_gp = 8 * cs.shape[0]
+    return n_gp / secs, n_gp, secs
+
+
 def clocks_sampler_start(path):
     q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -347,11 +364,15 @@ def main():
         reps = max(1, min(args.steps, 3))
         rate, n_sample, secs, _ = run_cpu_sample(X, conn, threads, nz_layers=args.nx, reps=reps)
         sample = f"whole mesh ({n_sample // 8} elements, {n_sample} GPs) per step, FP64, best of {reps}"
+        r1, g1, s1 = run_cpu_single(X, conn, nz_layers=min(4, args.nx))
         line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": warmup, "ms_per_step": secs * 1e3 * n_gp / n_sample,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": config,
-                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                                 "single_thread": {"value": r1, "unit": UNIT, "cores": 1,
+                                                   "sample": f"{g1 // 8} elements (first element layers), "
+                                                             f"serial loop, {s1:.2f} s"}},
                 "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "note": "reference Fortran not buildable (no Fortran compiler/MKL); FP64 C++ restatement of its "
                         "serial element loop with linear-search assembly, OpenMP over element colours"}
@@ -467,9 +488,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         rate, n_sample, secs, m = run_cpu_sample(X, conn, threads, nz_layers=args.nx)
+        r1, g1, s1 = run_cpu_single(X, conn, nz_layers=min(4, args.nx))
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"one evaluation of the whole mesh ({n_sample // 8} elements), FP64 "
-                                          f"oracle on {threads} threads, {secs:.2f} s"}
+                                          f"oracle on {threads} threads, {secs:.2f} s",
+                                "single_thread": {"value": r1, "unit": UNIT, "cores": 1,
+                                                  "sample": f"{g1 // 8} elements (first element layers), "
+                                                            f"serial loop, {s1:.2f} s"}}
         # error of the measured evaluation against the FP64 oracle at the same state: the oracle has
         # the same history (increments at DT and 2 DT committed) and evaluates the timed U at 3 DT
         m.commit()
