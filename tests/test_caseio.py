@@ -278,3 +278,52 @@ def test_case_driver_record_order(tmp_path):
     assert len(recs2) == 5 + 47 + 1 and recs2[5]["step"] == 4 and recs2[-1]["step"] == 50
     # a second restart finds the analysis complete
     assert c.restart(out, loop=loop)["steps_run"] == 0
+
+
+def test_restart_across_a_load_case_boundary(tmp_path):
+    """Two load cases (10 + 5 steps): an analysis stopped after the last step of load case 1 restarts at
+    (load case 2, step 1) with the U of that record, and its records carry the load-case labels."""
+    d = _edit(tmp_path, "Time_Discretization.dat", "1\t\t\t0.0E0\t\t\t1.0E0\t\t50",
+              "1 0.0 0.5 10\n2 0.5 1.0 5")
+    _edit(tmp_path, "Time_Discretization.dat", "Number of Load Cases\t\t\t\t\t\t\n1", "Number of Load Cases\n2")
+    c = io.Case(d)
+    out = str(tmp_path)
+    loop = _ScriptedLoop(c.n_dof)
+    c.run(out, loop=loop, n_steps=10)
+    _, recs = io.read_result(os.path.join(out, "FEMAnalysis.result"))
+    assert (recs[-1]["load_case"], recs[-1]["step"]) == (1, 10)
+    loop.log.clear()
+    r = c.restart(out, loop=loop)
+    assert r["first_step"] == 10
+    an = [e for e in loop.log if e[0] == "analysis"][0]
+    assert an == ("analysis", 5, recs[-1]["U"][0])
+    _, recs2 = io.read_result(os.path.join(out, "FEMAnalysis.result"))
+    new = recs2[len(recs):]
+    ends = [(x["load_case"], x["step"]) for x in new if x["flag_end_step"] == 1]
+    assert ends == [(2, s) for s in range(1, 6)]
+    assert new[0]["time"] == pytest.approx(0.6)                       # end of (2, 1)
+    # the scripted cut back in the call's second step: a substep record of (2, 2) with Flag_EndStep 0
+    assert (new[1]["load_case"], new[1]["step"], new[1]["flag_end_step"]) == (2, 2, 0)
+    assert new[1]["time"] == pytest.approx(0.6 + 0.1 * (1 - 1 / ((1 + 5 ** 0.5) / 2)))
+
+
+def test_probe_error_lines_follow_the_reference(tmp_path):
+    """ModProbe's error lines: a node beyond the mesh, a component beyond the node's dofs, a variable a
+    node does not carry; the probe then stops writing (its Active flag)."""
+    c = io.Case(os.path.join(CASES, "hexa8_svk"))
+    probes = [io.NodeProbe("far.probe", "Displacements", 10 ** 6, "1"),
+              io.NodeProbe("comp.probe", "Displacements", 11, "4"),
+              io.NodeProbe("var.probe", "Cauchy Stress", 11, "1"),
+              io.NodeProbe("all.probe", "Displacements", 11, "All")]
+    for p in probes:
+        p.initialize(str(tmp_path))
+    U = np.arange(c.n_dof, dtype=float)
+    for t in (0.1, 0.2):
+        for p in probes:
+            p.write(_View(c, t, U))
+    lines = {p.file_name: open(tmp_path / p.file_name).read().splitlines() for p in probes}
+    assert lines["far.probe"][1:] == ["ERROR - Node Number is greater than the Max Number of Nodes in the Mesh"]
+    assert lines["comp.probe"][1:] == ["ERROR: Component is greater than the available"]
+    assert lines["var.probe"][1:] == ["ERROR: Variable not available"]
+    rows = [list(map(float, ln.split())) for ln in lines["all.probe"][1:]]
+    assert rows == [[0.1, 30.0, 31.0, 32.0], [0.2, 30.0, 31.0, 32.0]]
