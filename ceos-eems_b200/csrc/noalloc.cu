@@ -15,6 +15,18 @@
 // call clears the part it uses before accumulating; two calls whose work overlaps on the GPU
 // (different streams, or different host threads without ordering) race on it and must not
 // be issued.
+//
+// The kernels keep no per-thread arrays in local memory (ptxas reports a 0-byte stack frame
+// for both), so a launch never makes the driver enlarge the context's local-memory reservation,
+// which would be a device allocation behind the caller's back.  Per-element data lives in
+// static shared memory: a CTA of 128 threads works on 16 elements, thread (element, j) with j
+// the Gauss point in the constitutive phase and the node in the assembly phase.
+//
+// Every index that comes from the caller is checked before it is used: node ids against
+// n_nodes, each CSR row triple against the layout of the upper pattern (row 3n holds 3 + 3m
+// entries, rows 3n+1 and 3n+2 two and one fewer diagonal entries) and against nnz, and every
+// node-pair block against the number of blocks the call cleared.  A failed check skips the
+// access and sets a flag; the call then returns CEOS_E_MESH.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -49,172 +61,295 @@ int scratch_on_current_device(float** out) {
     return 0;
 }
 
+constexpr int kBadGeometry = 1;  // det J <= 1e-13 (ClassStatus error 1)
+constexpr int kBadMesh = 2;      // node id, CSR row or node pair inconsistent with the pattern
+
 __device__ __forceinline__ void red_v4_na(float* p, float a, float b, float c, float d) {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
                  : "memory");
 }
 
-// First block of node n in the block layout: n + (number of upper neighbours of nodes < n).
-// With the 1-based upper CSR of the reference, row 3n starts at rowmap[3n]-1 = 6n + 9*(that sum).
-__device__ __forceinline__ long long first_block(const int* rowmap, int n) {
-    const long long rs = (long long)rowmap[3 * n] - 1;
-    return (long long)n + (rs - 6LL * n) / 9;
+// The three CSR rows of node n as the 1-based upper pattern lays them out: row 3n starts at
+// rowmap[3n]-1 with 3 + 3m entries (m upper neighbours), row 3n+1 has 2 + 3m, row 3n+2 1 + 3m.
+// The node's node-pair blocks start at block n + (r0 - 6n)/9 (one diagonal block per node and
+// one per upper neighbour of every earlier node).  ok is false when the rows do not have that
+// shape, leave [0, nnz), or their blocks leave [0, n_blocks).
+struct NodeRows {
+    long long r0, bb;
+    int m;
+    bool ok;
+};
+__device__ __forceinline__ NodeRows node_rows(const int* rowmap, int n, long long nnz, long long n_blocks) {
+    NodeRows q{0, 0, 0, false};
+    const long long r0 = (long long)rowmap[3 * n] - 1, r1 = (long long)rowmap[3 * n + 1] - 1;
+    const long long r2 = (long long)rowmap[3 * n + 2] - 1, r3 = (long long)rowmap[3 * n + 3] - 1;
+    const long long len = r1 - r0;
+    if (r0 < 0 || len < 3 || (len - 3) % 3 != 0) return q;
+    const long long m = (len - 3) / 3;
+    if (r2 - r1 != 2 + 3 * m || r3 - r2 != 1 + 3 * m || r3 > nnz) return q;
+    const long long off = r0 - 6LL * n;
+    if (off < 0 || off % 9 != 0) return q;
+    const long long bb = (long long)n + off / 9;
+    if (bb + 1 + m > n_blocks) return q;
+    q.r0 = r0;
+    q.bb = bb;
+    q.m = (int)m;
+    q.ok = true;
+    return q;
 }
 
-// Rank of node hi among the upper neighbours of node lo, read from row 3*lo of the CSR.
-__device__ __forceinline__ int neighbour_rank(const int* rowmap, const int* col, int lo, int hi) {
-    const long long rs = (long long)rowmap[3 * lo] - 1;
-    const int m = (rowmap[3 * lo + 1] - rowmap[3 * lo] - 3) / 3;
-    int l = 0, r = m - 1;
+// Rank of node hi among the upper neighbours of node lo (binary search of row 3*lo), -1 if absent.
+__device__ __forceinline__ int neighbour_rank(const int* col, const NodeRows& lo, int hi) {
+    int l = 0, r = lo.m - 1;
     const int target = 3 * hi + 1;  // 1-based column of hi's first DOF
     while (l <= r) {
         const int mid = (l + r) >> 1;
-        const int c = col[rs + 3 + 3 * mid];
+        const int c = col[lo.r0 + 3 + 3 * mid];
         if (c == target) return mid;
         if (c < target) l = mid + 1; else r = mid - 1;
     }
     return -1;
 }
 
-// One thread per element: Gauss-point update (compressible Neo-Hookean), internal force and
-// the 36 node-pair stiffness blocks, reduced into the block scratch.  FP32 element arithmetic.
-__global__ void __launch_bounds__(128) cnh_noalloc_kernel(int n_elem, const double* X, const double* U,
-                                                          const int* conn, const int* rowmap, const int* col,
-                                                          float mu, float lambda, double* fint, float* blocks,
-                                                          int* bad) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n_elem) return;
-    int nd[8];
-    float Xe[8][3], Ue[8][3];
-    for (int a = 0; a < 8; ++a) {
-        nd[a] = conn[8 * e + a] - 1;
-        for (int d = 0; d < 3; ++d) {
-            Xe[a][d] = (float)X[3 * nd[a] + d];
-            Ue[a][d] = (float)U[3 * nd[a] + d];
-        }
-    }
-    const float g3 = 0.57735026918962576f;  // 1/sqrt(3): 2x2x2 Gauss points, weight 1
-    float fe[8][3] = {};
-    float Kb[36][9] = {};  // pair (a <= b) in row-major upper order, block rows = node a
-    // Hexa8 node signs (ModElementHexa8.f90:185-192): x + for local nodes 1,2,5,6; y + for 2,3,6,7;
-    // z + for 4..7 (0-based)
-    auto sx = [](int i) { return ((i & 3) == 1 || (i & 3) == 2) ? 1.f : -1.f; };
-    auto sy = [](int i) { return (i & 3) >= 2 ? 1.f : -1.f; };
-    auto sz = [](int i) { return i >= 4 ? 1.f : -1.f; };
-    for (int gp = 0; gp < 8; ++gp) {
-        const float xi[3] = {sx(gp) * g3, sy(gp) * g3, sz(gp) * g3};
-        float dN[8][3];
-        for (int i = 0; i < 8; ++i) {
-            const float s0 = sx(i), s1 = sy(i), s2 = sz(i);
-            dN[i][0] = s0 * (1.f + s1 * xi[1]) * (1.f + s2 * xi[2]) * 0.125f;
-            dN[i][1] = s1 * (1.f + s0 * xi[0]) * (1.f + s2 * xi[2]) * 0.125f;
-            dN[i][2] = s2 * (1.f + s0 * xi[0]) * (1.f + s1 * xi[1]) * 0.125f;
-        }
-        float JX[3][3] = {}, Jc[3][3] = {};
-        for (int n = 0; n < 8; ++n)
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) {
-                    JX[i][j] += dN[n][i] * Xe[n][j];
-                    Jc[i][j] += dN[n][i] * (Xe[n][j] + Ue[n][j]);
-                }
-        const float dX = ceos::det3(JX), dC = ceos::det3(Jc);
-        if (!(dX > 1e-13f) || !(dC > 1e-13f)) {
-            atomicOr(bad, 1);
-            continue;
-        }
-        float JXi[3][3], Jci[3][3];
-        ceos::inv3(JX, dX, JXi);
-        ceos::inv3(Jc, dC, Jci);
-        float F[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
-        float g[8][3];
-        for (int n = 0; n < 8; ++n) {
-            float gX[3];
-            for (int j = 0; j < 3; ++j) {
-                gX[j] = JXi[j][0] * dN[n][0] + JXi[j][1] * dN[n][1] + JXi[j][2] * dN[n][2];
-                g[n][j] = Jci[j][0] * dN[n][0] + Jci[j][1] * dN[n][1] + Jci[j][2] * dN[n][2];
-            }
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) F[i][j] += Ue[n][i] * gX[j];
-        }
-        const float p[2] = {mu, lambda};
-        float sig[6], D[21];
-        ceos::cnh_update<float>(F, p, sig, D);
-        for (int k = 0; k < 6; ++k) sig[k] *= dC;
-        for (int k = 0; k < 21; ++k) D[k] *= dC;
-        auto Dij = [&](int i, int j) { return i <= j ? D[ceos::up21(i, j)] : D[ceos::up21(j, i)]; };
-        float q[8][3], DB[8][6][3];
-        for (int b = 0; b < 8; ++b) {
-            const float gx = g[b][0], gy = g[b][1], gz = g[b][2];
-            q[b][0] = sig[0] * gx + sig[3] * gy + sig[5] * gz;
-            q[b][1] = sig[3] * gx + sig[1] * gy + sig[4] * gz;
-            q[b][2] = sig[5] * gx + sig[4] * gy + sig[2] * gz;
-            for (int d = 0; d < 3; ++d) fe[b][d] += q[b][d];
-            for (int i = 0; i < 6; ++i) {
-                DB[b][i][0] = Dij(i, 0) * gx + Dij(i, 3) * gy + Dij(i, 5) * gz;
-                DB[b][i][1] = Dij(i, 1) * gy + Dij(i, 3) * gx + Dij(i, 4) * gz;
-                DB[b][i][2] = Dij(i, 2) * gz + Dij(i, 4) * gy + Dij(i, 5) * gx;
-            }
-        }
-        int pidx = 0;
-        for (int a = 0; a < 8; ++a)
-            for (int b = a; b < 8; ++b, ++pidx) {
-                const float ax = g[a][0], ay = g[a][1], az = g[a][2];
-                const float geo = ax * q[b][0] + ay * q[b][1] + az * q[b][2];
-                for (int l = 0; l < 3; ++l) {
-                    Kb[pidx][0 * 3 + l] += ax * DB[b][0][l] + ay * DB[b][3][l] + az * DB[b][5][l];
-                    Kb[pidx][1 * 3 + l] += ay * DB[b][1][l] + ax * DB[b][3][l] + az * DB[b][4][l];
-                    Kb[pidx][2 * 3 + l] += az * DB[b][2][l] + ay * DB[b][4][l] + ax * DB[b][5][l];
-                }
-                Kb[pidx][0] += geo; Kb[pidx][4] += geo; Kb[pidx][8] += geo;
-            }
-    }
-    for (int a = 0; a < 8; ++a)
-        for (int d = 0; d < 3; ++d) atomicAdd(fint + 3 * (size_t)nd[a] + d, (double)fe[a][d]);
-    int pidx = 0;
-    for (int a = 0; a < 8; ++a)
-        for (int b = a; b < 8; ++b, ++pidx) {
-            const float* M = Kb[pidx];  // rows of node a, columns of node b
-            if (a == b) {
-                float* blk = blocks + first_block(rowmap, nd[a]) * 12;
-                red_v4_na(blk + 0, M[0], M[1], M[2], 0.f);
-                red_v4_na(blk + 4, 0.f, M[4], M[5], 0.f);
-                red_v4_na(blk + 8, 0.f, 0.f, M[8], 0.f);
-                continue;
-            }
-            const bool a_low = nd[a] < nd[b];
-            const int lo = a_low ? nd[a] : nd[b], hi = a_low ? nd[b] : nd[a];
-            const int r = neighbour_rank(rowmap, col, lo, hi);
-            if (r < 0) { atomicOr(bad, 2); continue; }
-            float* blk = blocks + (first_block(rowmap, lo) + 1 + r) * 12;
-            if (a_low) {
-                red_v4_na(blk + 0, M[0], M[1], M[2], 0.f);
-                red_v4_na(blk + 4, M[3], M[4], M[5], 0.f);
-                red_v4_na(blk + 8, M[6], M[7], M[8], 0.f);
-            } else {
-                red_v4_na(blk + 0, M[0], M[3], M[6], 0.f);
-                red_v4_na(blk + 4, M[1], M[4], M[7], 0.f);
-                red_v4_na(blk + 8, M[2], M[5], M[8], 0.f);
-            }
-        }
+constexpr int kElemsPerCta = 16;
+constexpr int kNaThreads = 8 * kElemsPerCta;
+
+// dN/dxi of node n at Gauss point gp (ModElementHexa8.f90:211-268 at the points of :278-329).
+// Local node signs (ModElementHexa8.f90:185-192, 0-based): x + for nodes 1, 2, 5, 6; y + for
+// 2, 3, 6, 7; z + for 4..7.  The Gauss points use the same sign pattern.
+__device__ __forceinline__ float sgn_x(int i) { return ((i & 3) == 1 || (i & 3) == 2) ? 1.f : -1.f; }
+__device__ __forceinline__ float sgn_y(int i) { return (i & 3) >= 2 ? 1.f : -1.f; }
+__device__ __forceinline__ float sgn_z(int i) { return i >= 4 ? 1.f : -1.f; }
+__device__ __forceinline__ void hexa8_dN(int gp, int n, float d[3]) {
+    const float g3 = 0.57735026918962576f;  // 1/sqrt(3), weight 1
+    const float x0 = sgn_x(gp) * g3, x1 = sgn_y(gp) * g3, x2 = sgn_z(gp) * g3;
+    const float s0 = sgn_x(n), s1 = sgn_y(n), s2 = sgn_z(n);
+    d[0] = 0.125f * s0 * (1.f + s1 * x1) * (1.f + s2 * x2);
+    d[1] = 0.125f * s1 * (1.f + s0 * x0) * (1.f + s2 * x2);
+    d[2] = 0.125f * s2 * (1.f + s0 * x0) * (1.f + s1 * x1);
 }
 
-// Block scratch -> FP64 CSR values, one warp per node row block.
-__global__ void __launch_bounds__(256) blocks_to_csr_noalloc(int n_nodes, const int* rowmap, const float* blocks,
-                                                             double* K) {
+// Compressible Neo-Hookean element loop of 16 elements per CTA: Gauss-point update, internal
+// force and the 36 node-pair stiffness blocks of every element, reduced into the block scratch.
+// FP32 element arithmetic on element-local coordinate and displacement differences formed in
+// FP64; det F and ln J in FP64 (cnh_update).
+__global__ void __launch_bounds__(kNaThreads) cnh_noalloc_kernel(int n_nodes, int n_elem, const double* X,
+                                                                 const double* U, const int* conn, const int* rowmap,
+                                                                 const int* col, long long nnz, long long n_blocks,
+                                                                 float mu, float lambda, double* fint, float* blocks,
+                                                                 int* bad) {
+    __shared__ __align__(16) float s_dx[kElemsPerCta][8][4];        // X_n - X_0 (FP32)
+    __shared__ __align__(16) float s_du[kElemsPerCta][8][4];        // u_n - u_0 (FP32)
+    __shared__ __align__(16) float s_g[kElemsPerCta][8][8][4];      // [e][gp][node]: grad N (current)
+    __shared__ __align__(16) float s_ds[kElemsPerCta][8][28];       // [e][gp]: w D (21), w sigma (6)
+    __shared__ int s_node[kElemsPerCta][8];
+    __shared__ int s_elem_bad[kElemsPerCta];
+    const int t = threadIdx.x, el = t >> 3, j = t & 7;
+    const int e = blockIdx.x * kElemsPerCta + el;
+    const bool live = e < n_elem;
+    if (j == 0) s_elem_bad[el] = live ? 0 : kBadMesh;
+    __syncthreads();
+    int nid = -1;
+    if (live) {
+        nid = conn[8 * (size_t)e + j] - 1;
+        if (nid < 0 || nid >= n_nodes) {
+            atomicOr(&s_elem_bad[el], kBadMesh);
+            if (live) atomicOr(bad, kBadMesh);
+            nid = -1;
+        }
+    }
+    s_node[el][j] = nid;
+    __syncthreads();
+    const bool elem_ok = s_elem_bad[el] == 0;
+    if (elem_ok) {
+        // element-local differences in FP64, then FP32 (sum_n dN_n/dxi = 0 leaves J unchanged)
+        const int n0 = s_node[el][0];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            s_dx[el][j][d] = (float)(X[3 * (size_t)nid + d] - X[3 * (size_t)n0 + d]);
+            s_du[el][j][d] = (float)(U[3 * (size_t)nid + d] - U[3 * (size_t)n0 + d]);
+        }
+    }
+    __syncthreads();
+    // ---- Gauss point j of element el ----
+    if (elem_ok) {
+        const int gp = j;
+        float JX[3][3] = {}, Ju[3][3] = {};
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            float dn[3];
+            hexa8_dN(gp, n, dn);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    JX[i][k] += dn[i] * s_dx[el][n][k];
+                    Ju[i][k] += dn[i] * s_du[el][n][k];
+                }
+        }
+        float Jc[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) Jc[i][k] = JX[i][k] + Ju[i][k];
+        const float dX = ceos::det3(JX), dC = ceos::det3(Jc);
+        const bool geom_ok = dX > 1e-13f && dC > 1e-13f;
+        float JXi[3][3], Jci[3][3];
+        ceos::inv3(JX, geom_ok ? dX : 1.f, JXi);
+        ceos::inv3(Jc, geom_ok ? dC : 1.f, Jci);
+        float F[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                F[i][k] = (i == k ? 1.f : 0.f) + JXi[k][0] * Ju[0][i] + JXi[k][1] * Ju[1][i] + JXi[k][2] * Ju[2][i];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            float dn[3];
+            hexa8_dN(gp, n, dn);
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                s_g[el][gp][n][k] = geom_ok ? Jci[k][0] * dn[0] + Jci[k][1] * dn[1] + Jci[k][2] * dn[2] : 0.f;
+        }
+        float sig[6], D[21];
+        if (geom_ok) {
+            const float p[2] = {mu, lambda};
+            ceos::cnh_update<float>(F, p, sig, D);
+        } else {
+            atomicOr(bad, kBadGeometry);
+        }
+        const float w = geom_ok ? dC : 0.f;  // Gauss weight 1 (Hexa8 full integration)
+#pragma unroll
+        for (int k = 0; k < 21; ++k) s_ds[el][gp][k] = geom_ok ? w * D[k] : 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s_ds[el][gp][21 + k] = geom_ok ? w * sig[k] : 0.f;
+    }
+    __syncthreads();
+    if (!elem_ok) return;
+    // ---- node b = j of element el: f_int of b and the blocks (b, b+1..b+npair mod 8) ----
+    const int b = j;
+    const int npair = (b < 4) ? 4 : 3;
+    float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+    float Kd[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float Ko[4][9];
+#pragma unroll
+    for (int o = 0; o < 4; ++o)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Ko[o][k] = 0.f;
+    for (int gp = 0; gp < 8; ++gp) {
+        const float* ds = s_ds[el][gp];
+        const float gx = s_g[el][gp][b][0], gy = s_g[el][gp][b][1], gz = s_g[el][gp][b][2];
+        const float s0 = ds[21], s1 = ds[22], s2 = ds[23], s3 = ds[24], s4 = ds[25], s5 = ds[26];
+        const float q0 = s0 * gx + s3 * gy + s5 * gz;
+        const float q1 = s3 * gx + s1 * gy + s4 * gz;
+        const float q2 = s5 * gx + s4 * gy + s2 * gz;
+        f0 += q0; f1 += q1; f2 += q2;
+        float DB[6][3];  // D B_b with D read through its upper triangle
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const float d0 = ds[i <= 0 ? ceos::up21(i, 0) : ceos::up21(0, i)];
+            const float d1 = ds[i <= 1 ? ceos::up21(i, 1) : ceos::up21(1, i)];
+            const float d2 = ds[i <= 2 ? ceos::up21(i, 2) : ceos::up21(2, i)];
+            const float d3 = ds[i <= 3 ? ceos::up21(i, 3) : ceos::up21(3, i)];
+            const float d4 = ds[i <= 4 ? ceos::up21(i, 4) : ceos::up21(4, i)];
+            const float d5 = ds[i <= 5 ? ceos::up21(i, 5) : ceos::up21(5, i)];
+            DB[i][0] = d0 * gx + d3 * gy + d5 * gz;
+            DB[i][1] = d1 * gy + d3 * gx + d4 * gz;
+            DB[i][2] = d2 * gz + d4 * gy + d5 * gx;
+        }
+        {
+            const float geo = gx * q0 + gy * q1 + gz * q2;
+            Kd[0] += gx * DB[0][0] + gy * DB[3][0] + gz * DB[5][0] + geo;
+            Kd[1] += gx * DB[0][1] + gy * DB[3][1] + gz * DB[5][1];
+            Kd[2] += gx * DB[0][2] + gy * DB[3][2] + gz * DB[5][2];
+            Kd[3] += gy * DB[1][1] + gx * DB[3][1] + gz * DB[4][1] + geo;
+            Kd[4] += gy * DB[1][2] + gx * DB[3][2] + gz * DB[4][2];
+            Kd[5] += gz * DB[2][2] + gy * DB[4][2] + gx * DB[5][2] + geo;
+        }
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            if (o < npair) {
+                const int an = (b + 1 + o) & 7;
+                const float ax = s_g[el][gp][an][0], ay = s_g[el][gp][an][1], az = s_g[el][gp][an][2];
+                const float geo = ax * q0 + ay * q1 + az * q2;
+#pragma unroll
+                for (int l = 0; l < 3; ++l) {
+                    Ko[o][0 * 3 + l] += ax * DB[0][l] + ay * DB[3][l] + az * DB[5][l];
+                    Ko[o][1 * 3 + l] += ay * DB[1][l] + ax * DB[3][l] + az * DB[4][l];
+                    Ko[o][2 * 3 + l] += az * DB[2][l] + ay * DB[4][l] + ax * DB[5][l];
+                }
+                Ko[o][0] += geo; Ko[o][4] += geo; Ko[o][8] += geo;
+            }
+        }
+    }
+    // ---- scatter: f_int by FP64 atomics, blocks by 16-byte FP32 vector reductions ----
+    const int Bn = s_node[el][b];
+    atomicAdd(fint + 3 * (size_t)Bn + 0, (double)f0);
+    atomicAdd(fint + 3 * (size_t)Bn + 1, (double)f1);
+    atomicAdd(fint + 3 * (size_t)Bn + 2, (double)f2);
+    const NodeRows rb = node_rows(rowmap, Bn, nnz, n_blocks);
+    if (!rb.ok) {
+        atomicOr(bad, kBadMesh);
+        return;
+    }
+    {
+        float* blk = blocks + rb.bb * 12;
+        red_v4_na(blk + 0, Kd[0], Kd[1], Kd[2], 0.f);
+        red_v4_na(blk + 4, 0.f, Kd[3], Kd[4], 0.f);
+        red_v4_na(blk + 8, 0.f, 0.f, Kd[5], 0.f);
+    }
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+        if (o < npair) {
+            const int An = s_node[el][(b + 1 + o) & 7];
+            if (An == Bn) {  // an element that repeats a node has no such node pair in the pattern
+                atomicOr(bad, kBadMesh);
+                continue;
+            }
+            const bool a_low = An < Bn;  // the rows of a node pair belong to the smaller node
+            const NodeRows lo = a_low ? node_rows(rowmap, An, nnz, n_blocks) : rb;
+            const int r = lo.ok ? neighbour_rank(col, lo, a_low ? Bn : An) : -1;
+            if (r < 0) {
+                atomicOr(bad, kBadMesh);
+                continue;
+            }
+            float* blk = blocks + (lo.bb + 1 + r) * 12;  // r < lo.m, so the block is below n_blocks
+            if (a_low) {  // rows of node a: M[k][:]
+                red_v4_na(blk + 0, Ko[o][0], Ko[o][1], Ko[o][2], 0.f);
+                red_v4_na(blk + 4, Ko[o][3], Ko[o][4], Ko[o][5], 0.f);
+                red_v4_na(blk + 8, Ko[o][6], Ko[o][7], Ko[o][8], 0.f);
+            } else {      // rows of node b: M[:][l]
+                red_v4_na(blk + 0, Ko[o][0], Ko[o][3], Ko[o][6], 0.f);
+                red_v4_na(blk + 4, Ko[o][1], Ko[o][4], Ko[o][7], 0.f);
+                red_v4_na(blk + 8, Ko[o][2], Ko[o][5], Ko[o][8], 0.f);
+            }
+        }
+    }
+}
+
+// Block scratch -> FP64 CSR values, one warp per node row block.  Rows that fail the layout
+// check are left unwritten and flagged.
+__global__ void __launch_bounds__(256) blocks_to_csr_noalloc(int n_nodes, const int* rowmap, long long nnz,
+                                                             long long n_blocks, const float* blocks, double* K,
+                                                             int* bad) {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; n < n_nodes; n += warps) {
-        const long long rs = (long long)rowmap[3 * n] - 1;
-        const int m = (rowmap[3 * n + 1] - rowmap[3 * n] - 3) / 3;
-        const float* blk = blocks + first_block(rowmap, n) * 12;
+        const NodeRows q = node_rows(rowmap, n, nnz, n_blocks);
+        if (!q.ok) {
+            if (lane == 0) atomicOr(bad, kBadMesh);
+            continue;
+        }
+        const int m = q.m;
+        const float* blk = blocks + q.bb * 12;
         for (int k = 0; k < 3; ++k) {
-            const long long rstart = rs + (k == 0 ? 0LL : (k == 1 ? 3LL + 3LL * m : 5LL + 6LL * m));
+            const long long rstart = q.r0 + (k == 0 ? 0LL : (k == 1 ? 3LL + 3LL * m : 5LL + 6LL * m));
             const int ndg = 3 - k, len = ndg + 3 * m;
             for (int p = lane; p < len; p += 32) {
-                int j, l;
-                if (p < ndg) { j = 0; l = k + p; }
-                else { const int pp = p - ndg; j = 1 + pp / 3; l = pp - 3 * (pp / 3); }
-                K[rstart + p] = (double)blk[j * 12 + 4 * k + l];
+                int jb, l;
+                if (p < ndg) { jb = 0; l = k + p; }
+                else { const int pp = p - ndg; jb = 1 + pp / 3; l = pp - 3 * (pp / 3); }
+                K[rstart + p] = (double)blk[jb * 12 + 4 * k + l];
             }
         }
     }
@@ -242,16 +377,18 @@ extern "C" int ceos_cnh_assemble_noalloc(int n_nodes, int n_elem, const double* 
     int* bad = reinterpret_cast<int*>(scratch + n_blocks * 12);
     if (cudaMemsetAsync(scratch, 0, (size_t)n_blocks * 48 + 16, s) != cudaSuccess) return CEOS_E_CUDA;
     if (cudaMemsetAsync(fint_device, 0, sizeof(double) * 3 * (size_t)n_nodes, s) != cudaSuccess) return CEOS_E_CUDA;
-    cnh_noalloc_kernel<<<(n_elem + 127) / 128, 128, 0, s>>>(n_elem, X_device, U_device, conn_device, rowmap_device,
-                                                            col_device, (float)mu, (float)lambda, fint_device,
-                                                            scratch, bad);
+    const unsigned grid = (unsigned)((n_elem + kElemsPerCta - 1) / kElemsPerCta);
+    cnh_noalloc_kernel<<<grid, kNaThreads, 0, s>>>(n_nodes, n_elem, X_device, U_device, conn_device, rowmap_device,
+                                                  col_device, nnz, n_blocks, (float)mu, (float)lambda, fint_device,
+                                                  scratch, bad);
     if (cudaGetLastError() != cudaSuccess) return CEOS_E_CUDA;
-    blocks_to_csr_noalloc<<<(n_nodes + 7) / 8, 256, 0, s>>>(n_nodes, rowmap_device, scratch, kval_device);
+    blocks_to_csr_noalloc<<<(n_nodes + 7) / 8, 256, 0, s>>>(n_nodes, rowmap_device, nnz, n_blocks, scratch,
+                                                            kval_device, bad);
     if (cudaGetLastError() != cudaSuccess) return CEOS_E_CUDA;
     int hbad = 0;
     if (cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return CEOS_E_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return CEOS_E_CUDA;
-    if (hbad & 1) return 1;  // det J <= 1e-13 in some element (ClassStatus error 1)
-    if (hbad & 2) return CEOS_E_MESH;
+    if (hbad & kBadMesh) return CEOS_E_MESH;   // the mesh or pattern does not match (K incomplete)
+    if (hbad & kBadGeometry) return 1;         // det J <= 1e-13 in some element (ClassStatus error 1)
     return 0;
 }
