@@ -177,3 +177,50 @@ def macro_surrogate_run(sur, nx=32, stretch=1.2, n_steps=10, seed=12, tol=1e-6, 
            "stats": dict(m.stats)}
     m.close()
     return out
+
+
+def experiment(n_train=200000, epochs=2000, log=None):
+    """The learned-surrogate experiment: training data from the batched RVE solver, training,
+    held-out stress error, a 4^3 macro head-to-head of surrogate and direct FE^2, and the 32^3
+    surrogate macro run.  Returns one JSON-ready record."""
+    import json
+
+    rec = {"metric": "FE2 macro step time: surrogate vs direct", "unit": "s", "higher_is_better": False,
+           "dtype": "bf16 training / f32 inference / f64 RVE", "data": "synthetic"}
+    F, vf = sample_points(n_train, seed=1, small_fraction=0.5)
+    P, _, st = rve_stresses(F, vf, batch=8192)
+    Fv, vfv = sample_points(4096, seed=99)
+    Pv, _, _ = rve_stresses(Fv, vfv, batch=4096)
+    Ft, vft = sample_points(8192, seed=7)
+    _, _, st_tan = rve_stresses(Ft, vft, batch=8192, tangent=True)
+    sur, hist, t_train = fit(F, vf, P, epochs=epochs, batch=2048, lr0=3e-3, lr1=3e-6)
+    Pp, fl = predict_P(sur, Fv, vfv)
+    rec["training"] = {"samples": int(n_train), "rve_n_cells": 6, "data_s": st["seconds"],
+                       "rve_per_s": st["rve_per_s"], "rve_per_s_with_tangent": st_tan["rve_per_s"],
+                       "failed_rves": st["failed"], "epochs": epochs, "batch": 2048,
+                       "adam_steps": epochs * (n_train // 2048), "train_s": t_train,
+                       "loss_first_epoch": float(hist[0]), "loss_last_epoch": float(hist[-1])}
+    rec["validation_stress_error"] = stress_errors(Pp[~fl], Pv[~fl])
+    rec["validation_out_of_range"] = int(fl.sum())
+    if log:
+        print(json.dumps({"partial": "training", "training": rec["training"],
+                          "validation": rec["validation_stress_error"]}), file=log, flush=True)
+    small = macro_compare(sur, nx=4)
+    rec["macro_4cube"] = {k: small[k] for k in ("direct", "surrogate", "stress_error_per_step",
+                                                "constitutive_error_per_step")}
+    rec["speedup_4cube_in_range_steps"] = [d / s for d, s, fb in zip(small["direct"]["step_s"],
+                                                                    small["surrogate"]["step_s"],
+                                                                    small["surrogate"]["fallback_points"]) if fb == 0]
+    if log:
+        print(json.dumps({"partial": "4cube", "macro_4cube": rec["macro_4cube"],
+                          "speedup": rec["speedup_4cube_in_range_steps"]}), file=log, flush=True)
+    big = macro_surrogate_run(sur, nx=32)
+    s32 = np.array(big["step_s"])
+    rec["macro_32cube"] = {"surrogate": {k: big[k] for k in ("step_s", "newton", "fallback_points", "stopped")},
+                           "surrogate_stats": big["stats"]}
+    rec["value"] = float(s32.mean()) if s32.size else None
+    rec["config"] = {"workload": "FE2 uniaxial stretch to 1.2 in 10 increments; macro 32^3 Hexa8 (262,144 GPs) and "
+                                 "4^3 head-to-head; periodic fibre RVEs n=6, vf U[0.1,0.4], mu_f/mu_m=50, K/mu=100",
+                     "surrogate": "MLP 7-128x4-1 softplus energy of (C, vf)"}
+    sur.close()
+    return rec
