@@ -223,8 +223,18 @@ class ElementLoop:
     def store_stress(self, on=True):
         self.set_options(OPT_STORE_STRESS if on else 0)
 
+    def launches_per_evaluation(self, tangent=True):
+        """Kernels that one device-resident evaluation launches: one (the fused element loop and CSR
+        assembly in mixed precision with a tangent, the element loop otherwise)."""
+        return 1
+
+    def kernel_names(self):
+        """Names of the kernels of one device-resident evaluation with a tangent."""
+        return ["element_assemble_kernel" if self.precision == MIXED else "element_loop_kernel"]
+
     def kernel_time_ms(self):
-        """(element-loop kernel ms, K conversion kernel ms) of the last evaluation."""
+        """(evaluation kernel ms, 0) of the last evaluation: the element loop with its K assembly is one
+        launch (the second entry was a separate K conversion kernel in earlier builds)."""
         ms = (C.c_float * 2)()
         _check(lib().ceos_kernel_time(self._h, ms))
         return ms[0], ms[1]

@@ -11,6 +11,7 @@
 #include "../../include/ceos_gpu.h"
 #include "ceos_handle.h"
 #include "element_kernel.cuh"
+#include "schedule.h"
 
 namespace ceos {
 
@@ -76,15 +77,15 @@ void model_init_state(int model, double* st) {
 template <typename T>
 size_t elem_smem(const Handle* h) { return SmemLayout<T>(h->ns_used).total; }
 
-// One launch of the element loop over elements [e0, e1) and, in mixed mode with a tangent, the
-// conversion of the node row blocks [n0, n1) (final once every element touching them has run).
+// One evaluation launch.  CEOS_MIXED with a tangent: the fused element loop + assembly over the
+// queue items of element slab `slab` (the whole queue when the host evaluates in one slab).
+// Otherwise: the element loop over elements [e0, e1) with the static tile schedule (K by FP64
+// atomics in CEOS_FP64 mode, no K without a tangent).
 template <typename T, int MODEL>
 int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s, int e0, int e1,
-                 int n0, int n1) {
-    ElemArgs<T> a;
+                 int slab) {
+    ElemArgs<T> a{};
     a.n_elem = h->n_elem;
-    a.e_begin = e0;
-    a.e_end = e1;
     for (int k = 0; k < 12; ++k) a.pu[k] = T(0);
     if (h->param_mode == 0)
         for (int k = 0; k < h->n_params && k < 12; ++k) a.pu[k] = (T)h->host_params[k];
@@ -95,7 +96,6 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
     a.X = h->d_X;
     a.U = dU;
     a.conn = h->d_conn;
-    a.rs = (sizeof(T) == 4) ? h->d_blk0 : h->d_rs;
     a.nup = h->d_nup;
     a.ranks = h->d_ranks;
     a.fint = dfint;
@@ -112,84 +112,106 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
     a.elem_status = h->d_elem_status;
     a.status_count = h->d_status_count;
     a.gp_stress = (h->options & CEOS_OPT_STORE_STRESS) ? reinterpret_cast<T*>(h->d_gp_stress) : nullptr;
-    a.kblk = h->d_kblk;
     const size_t smem = elem_smem<T>(h);
-    CK(cudaFuncSetAttribute(element_loop_kernel<T, MODEL, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int n_tiles = (a.e_end - a.e_begin + kTileE - 1) / kTileE;
-    int grid = std::min(n_tiles, h->grid_cap);
     const bool timed = (h->options & CEOS_OPT_TIME_KERNELS) && h->ev_k0;
+    if constexpr (sizeof(T) == 4) {
+        if (dkval) {
+            a.e_begin = 0;
+            a.e_end = h->n_elem;
+            a.rs = h->d_blk0;
+            a.kblk = h->d_kblk;
+            a.ring_mask = h->ring_blocks - 1;
+            a.csr_rs = h->d_rs;
+            a.queue = h->d_queue;
+            a.q_begin = slab < 0 ? 0 : h->slab_q[slab];                 // slab -1: the whole queue
+            a.q_end = slab < 0 ? (int)h->queue.size() : h->slab_q[slab + 1];
+            a.ticket = h->d_ticket;
+            a.tile_done = h->d_flags;
+            a.conv_done = h->d_flags + h->n_tiles;
+            a.epoch = h->epoch;
+            a.conv = static_cast<const int4*>(h->d_conv);
+            a.tile_wait = static_cast<const int2*>(h->d_tile_wait);
+            a.sched_err = h->d_sched_err;
+            CK(cudaMemsetAsync(h->d_ticket, 0, sizeof(unsigned), s));
+            CK(cudaFuncSetAttribute(element_assemble_kernel<MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            const int nq = a.q_end - a.q_begin;
+            if (timed) CK(cudaEventRecord(h->ev_k0, s));
+            if (nq > 0) {
+                element_assemble_kernel<MODEL><<<std::min(nq, h->grid_cap), kThreads, smem, s>>>(a);
+                CK(cudaGetLastError());
+            }
+            if (timed) {
+                CK(cudaEventRecord(h->ev_k1, s));
+                CK(cudaEventRecord(h->ev_k2, s));
+            }
+            return 0;
+        }
+    }
+    a.e_begin = e0;
+    a.e_end = e1;
+    a.rs = h->d_rs;
+    CK(cudaFuncSetAttribute(element_loop_kernel<T, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int n_tiles = (a.e_end - a.e_begin + kTileE - 1) / kTileE;
+    const int grid = std::min(n_tiles, h->grid_cap);
     if (timed) CK(cudaEventRecord(h->ev_k0, s));
     if (n_tiles > 0) {
-        element_loop_kernel<T, MODEL, (sizeof(T) == 4)><<<grid, kThreads, smem, s>>>(a);
+        element_loop_kernel<T, MODEL><<<grid, kThreads, smem, s>>>(a);
         CK(cudaGetLastError());
     }
-    if (timed) CK(cudaEventRecord(h->ev_k1, s));
-    if (sizeof(T) == 4 && dkval && n1 > n0) {
-        // FP32 node-pair blocks -> FP64 CSR (every K entry written once), scratch re-zeroed
-        const int cgrid = std::min(h->grid_cap > 0 ? 148 * 8 : 1184, (n1 - n0 + 7) / 8);
-        kblock_to_csr_kernel<<<cgrid, 256, 0, s>>>(n0, n1, h->d_rs, h->d_nup, h->d_kblk, dkval);
-        CK(cudaGetLastError());
+    if (timed) {
+        CK(cudaEventRecord(h->ev_k1, s));
+        CK(cudaEventRecord(h->ev_k2, s));
     }
-    if (timed) CK(cudaEventRecord(h->ev_k2, s));
     return 0;
 }
 
 template <typename T>
 int launch_elem(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s, int e0, int e1,
-                int n0, int n1) {
+                int slab) {
     switch (h->model) {
-        case M_CNH: return launch_model<T, M_CNH>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
-        case M_NH_Q1P0: return launch_model<T, M_NH_Q1P0>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
-        case M_SVK: return launch_model<T, M_SVK>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
-        case M_J2_SMALL: return launch_model<T, M_J2_SMALL>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
-        case M_VISCO_PRONY: return launch_model<T, M_VISCO_PRONY>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
-        case M_J2_FINITE: return launch_model<T, M_J2_FINITE>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
-        case M_VISCO_VAR: return launch_model<T, M_VISCO_VAR>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
-        case M_EXTERNAL: return launch_model<T, M_EXTERNAL>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
+        case M_CNH: return launch_model<T, M_CNH>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
+        case M_NH_Q1P0: return launch_model<T, M_NH_Q1P0>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
+        case M_SVK: return launch_model<T, M_SVK>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
+        case M_J2_SMALL: return launch_model<T, M_J2_SMALL>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
+        case M_VISCO_PRONY: return launch_model<T, M_VISCO_PRONY>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
+        case M_J2_FINITE: return launch_model<T, M_J2_FINITE>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
+        case M_VISCO_VAR: return launch_model<T, M_VISCO_VAR>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
+        case M_EXTERNAL: return launch_model<T, M_EXTERNAL>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
     }
     return CEOS_E_MODEL;
 }
 
+template <typename K>
+int blocks_per_sm(K kernel, size_t smem) {
+    int per_sm = 1;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
+    return (e != cudaSuccess || per_sm < 1) ? 1 : per_sm;
+}
+
+// Resident CTAs per SM of the evaluation kernel of this handle (the fused kernel in mixed mode).
+template <typename T, int MODEL>
+int model_blocks_per_sm(Handle* h) {
+    const size_t smem = elem_smem<T>(h);
+    if constexpr (sizeof(T) == 4) return blocks_per_sm(element_assemble_kernel<MODEL>, smem);
+    return blocks_per_sm(element_loop_kernel<T, MODEL>, smem);
+}
+
 template <typename T>
 int occupancy_grid(Handle* h) {
-    int per_sm = 1, dev = h->device, sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t e = cudaSuccess;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    int per_sm = 1;
     switch (h->model) {
-        case M_CNH:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_CNH, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_CNH, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
-            break;
-        case M_NH_Q1P0:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_NH_Q1P0, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_NH_Q1P0, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
-            break;
-        case M_SVK:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_SVK, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_SVK, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
-            break;
-        case M_J2_SMALL:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_J2_SMALL, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_J2_SMALL, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
-            break;
-        case M_VISCO_PRONY:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_VISCO_PRONY, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_VISCO_PRONY, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
-            break;
-        case M_J2_FINITE:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_J2_FINITE, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_J2_FINITE, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
-            break;
-        case M_VISCO_VAR:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_VISCO_VAR, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_VISCO_VAR, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
-            break;
-        case M_EXTERNAL:
-            e = cudaFuncSetAttribute(element_loop_kernel<T, M_EXTERNAL, (sizeof(T) == 4)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)elem_smem<T>(h));
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, element_loop_kernel<T, M_EXTERNAL, (sizeof(T) == 4)>, kThreads, elem_smem<T>(h));
-            break;
+        case M_CNH: per_sm = model_blocks_per_sm<T, M_CNH>(h); break;
+        case M_NH_Q1P0: per_sm = model_blocks_per_sm<T, M_NH_Q1P0>(h); break;
+        case M_SVK: per_sm = model_blocks_per_sm<T, M_SVK>(h); break;
+        case M_J2_SMALL: per_sm = model_blocks_per_sm<T, M_J2_SMALL>(h); break;
+        case M_VISCO_PRONY: per_sm = model_blocks_per_sm<T, M_VISCO_PRONY>(h); break;
+        case M_J2_FINITE: per_sm = model_blocks_per_sm<T, M_J2_FINITE>(h); break;
+        case M_VISCO_VAR: per_sm = model_blocks_per_sm<T, M_VISCO_VAR>(h); break;
+        case M_EXTERNAL: per_sm = model_blocks_per_sm<T, M_EXTERNAL>(h); break;
     }
-    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     h->blocks_per_sm = per_sm;
     return sms * per_sm;
 }
@@ -281,6 +303,11 @@ int build_pattern(Handle* h, const int* conn1) {
 
 }  // namespace ceos
 
+namespace ceos {
+static void plan_slab_bounds(Handle* h);
+static int build_schedule(Handle* h);
+}  // namespace ceos
+
 using namespace ceos;
 
 extern "C" int ceos_create(const ceos_mesh* mesh, const ceos_material* mats, int n_mat, int precision_mode,
@@ -311,6 +338,11 @@ extern "C" int ceos_create(const ceos_mesh* mesh, const ceos_material* mats, int
     rc = h->allocate_device(mesh, mats, n_mat);
     if (rc) { std::fprintf(stderr, "ceos_create: %s\n", h->msg.c_str()); delete h; return rc; }
     h->grid_cap = (precision_mode == CEOS_FP64) ? occupancy_grid<double>(h) : occupancy_grid<float>(h);
+    plan_slab_bounds(h);
+    if (precision_mode == CEOS_MIXED) {
+        rc = build_schedule(h);
+        if (rc) { std::fprintf(stderr, "ceos_create: %s\n", h->msg.c_str()); delete h; return rc; }
+    }
     {
         double tab[8][8][3];
         hexa8_dN_table(tab);
@@ -389,22 +421,30 @@ static int evaluate_prologue(Handle* h, double time, double* dfint, double* dkva
     CK(cudaMemsetAsync(h->d_status_count, 0, sizeof(int), s));
     CK(cudaMemsetAsync(dfint, 0, sizeof(double) * 3 * (size_t)h->n_nodes, s));
     // FP64 mode accumulates straight into K (zeroed here); the mixed mode writes every K entry
-    // from its FP32 block scratch, so K needs no clearing.
+    // from its FP32 node-pair blocks, so K needs no clearing.
     if (dkval && h->precision == CEOS_FP64) CK(cudaMemsetAsync(dkval, 0, sizeof(double) * (size_t)h->nnz, s));
+    if (dkval && h->precision == CEOS_MIXED) {
+        ++h->epoch;  // the flags of this evaluation's tiles and conversion items
+        if (h->ring_dirty) {  // an aborted evaluation may have left partial sums in the ring
+            CK(cudaMemsetAsync(h->d_kblk, 0, (size_t)h->ring_blocks * 12 * sizeof(float), s));
+            h->ring_dirty = false;
+        }
+    }
     return 0;
 }
 
+// Elements [e0, e1) = slab `slab` of the host-buffer plan (slab -1: the whole mesh).
 static int evaluate_range(Handle* h, double time, const double* dU, double* dfint, double* dkval, cudaStream_t s,
-                          int e0, int e1, int n0, int n1) {
+                          int e0, int e1, int slab) {
     const double dt = time - h->time_old;
-    return (h->precision == CEOS_FP64) ? launch_elem<double>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1)
-                                       : launch_elem<float>(h, dt, dU, dfint, dkval, s, e0, e1, n0, n1);
+    return (h->precision == CEOS_FP64) ? launch_elem<double>(h, dt, dU, dfint, dkval, s, e0, e1, slab)
+                                       : launch_elem<float>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
 }
 
 int evaluate_device(Handle* h, double time, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
     int rc = evaluate_prologue(h, time, dfint, dkval, s);
     if (rc) return rc;
-    rc = evaluate_range(h, time, dU, dfint, dkval, s, 0, h->n_elem, 0, h->n_nodes);
+    rc = evaluate_range(h, time, dU, dfint, dkval, s, 0, h->n_elem, -1);  // one launch over every slab
     if (rc) return rc;
     h->evaluated = true;
     return 0;
@@ -415,12 +455,12 @@ int evaluate_device(Handle* h, double time, const double* dU, double* dfint, dou
 // of the row order (a running maximum over the nodes of the last slab touching them).  Meshes whose
 // numbering follows a sweep (structured or banded) finish a growing prefix after every slab; any
 // other numbering simply leaves the copies to the end.
-static int plan_slabs(Handle* h) {
+static void plan_slab_bounds(Handle* h) {
     const int kMinElemPerSlab = 16384;
     int ns = std::min(4, h->n_elem / kMinElemPerSlab);
     if (ns < 1) ns = 1;
     // boundaries on whole tiles of kTileE elements: the kernel stages state rows with 16-byte copies
-    // from st_old + e_begin + 32 t, which must stay 16-byte aligned
+    // from st_old + 32 t, which must stay 16-byte aligned
     h->slab_e.assign(ns + 1, 0);
     for (int c = 1; c < ns; ++c) h->slab_e[c] = (int)((long long)h->n_elem * c / ns / kTileE * kTileE);
     h->slab_e[ns] = h->n_elem;
@@ -435,12 +475,48 @@ static int plan_slabs(Handle* h) {
         h->slab_node_end[c] = n;
     }
     h->slab_node_end[ns - 1] = h->n_nodes;
-    if (ns > 1) {
+    h->n_slabs = ns;
+}
+
+static int ensure_copy_stream(Handle* h) {
+    if (h->n_slabs > 1 && !h->copy_stream) {
         CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
-        h->slab_ev.assign(ns, nullptr);
+        h->slab_ev.assign(h->n_slabs, nullptr);
         for (auto& ev : h->slab_ev) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     }
-    h->n_slabs = ns;
+    return 0;
+}
+
+// Work queue of the fused element loop + assembly (mixed mode): planned on the host
+// (plan_schedule, schedule.cpp), uploaded with the ring of node-pair blocks it sizes.
+static int build_schedule(Handle* h) {
+    SchedulePlan p;
+    const int rc = plan_schedule(h->n_nodes, h->n_elem, h->conn0.data(), h->rs.data(), h->nup.data(), h->n_blocks,
+                                 h->slab_e, h->slab_node_end, kTileE, h->grid_cap, kStageDoubles, p);
+    if (rc) {
+        h->msg = p.err;
+        return rc;
+    }
+    h->queue = p.queue;
+    h->slab_q = p.slab_q;
+    h->n_tiles = p.n_tiles;
+    h->n_conv = (int)p.conv.size();
+    h->ring_blocks = (uint32_t)p.ring_blocks;
+    const size_t T = h->n_tiles, J = h->n_conv;
+    CK(cudaMalloc(&h->d_queue, h->queue.size() * sizeof(int)));
+    CK(cudaMemcpy(h->d_queue, h->queue.data(), h->queue.size() * sizeof(int), cudaMemcpyHostToDevice));
+    static_assert(sizeof(ConvItem) == sizeof(int4) && sizeof(TileWait) == sizeof(int2), "item layouts");
+    CK(cudaMalloc(&h->d_conv, J * sizeof(int4)));
+    CK(cudaMemcpy(h->d_conv, p.conv.data(), J * sizeof(int4), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&h->d_tile_wait, T * sizeof(int2)));
+    CK(cudaMemcpy(h->d_tile_wait, p.tile_wait.data(), T * sizeof(int2), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&h->d_flags, (T + J) * sizeof(unsigned)));
+    CK(cudaMemset(h->d_flags, 0, (T + J) * sizeof(unsigned)));
+    CK(cudaMalloc(&h->d_ticket, sizeof(unsigned)));
+    CK(cudaMalloc(&h->d_sched_err, sizeof(int)));
+    CK(cudaMemset(h->d_sched_err, 0, sizeof(int)));
+    CK(cudaMalloc(&h->d_kblk, (size_t)h->ring_blocks * 12 * sizeof(float)));
+    CK(cudaMemset(h->d_kblk, 0, (size_t)h->ring_blocks * 12 * sizeof(float)));
     return 0;
 }
 }  // namespace ceos
@@ -456,6 +532,16 @@ extern "C" int ceos_evaluate_device(void* handle, double time, const double* U_d
 extern "C" int ceos_status(void* handle, int* n_failed) {
     Handle* h = static_cast<Handle*>(handle);
     if (!h) return CEOS_E_ARG;
+    if (h->d_sched_err) {  // a bounded wait of the fused assembly gave up: K is incomplete
+        int err = 0;
+        CK(cudaMemcpy(&err, h->d_sched_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) {
+            CK(cudaMemset(h->d_sched_err, 0, sizeof(int)));
+            h->ring_dirty = true;
+            h->msg = "fused assembly: a dependency wait exceeded its bound";
+            return CEOS_E_CUDA;
+        }
+    }
     int cnt = 0;
     CK(cudaMemcpy(&cnt, h->d_status_count, sizeof(int), cudaMemcpyDeviceToHost));
     if (n_failed) *n_failed = cnt;
@@ -475,8 +561,8 @@ extern "C" int ceos_evaluate(void* handle, double time, const double* U, double*
     CK(cudaSetDevice(h->device));
     cudaStream_t s = h->stream;
     const size_t nd = 3 * (size_t)h->n_nodes;
-    if (h->n_slabs == 0) {
-        const int rc = plan_slabs(h);
+    {
+        const int rc = ensure_copy_stream(h);
         if (rc) return rc;
     }
     CK(cudaMemcpyAsync(h->d_U, U, nd * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -484,7 +570,7 @@ extern "C" int ceos_evaluate(void* handle, double time, const double* U, double*
     int rc = evaluate_prologue(h, time, h->d_fint, dk, s);
     if (rc) return rc;
     if (h->n_slabs == 1) {
-        rc = evaluate_range(h, time, h->d_U, h->d_fint, dk, s, 0, h->n_elem, 0, h->n_nodes);
+        rc = evaluate_range(h, time, h->d_U, h->d_fint, dk, s, 0, h->n_elem, -1);
         if (rc) return rc;
         CK(cudaMemcpyAsync(fint, h->d_fint, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
         if (kval) CK(cudaMemcpyAsync(kval, h->d_kval, (size_t)h->nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -493,7 +579,7 @@ extern "C" int ceos_evaluate(void* handle, double time, const double* U, double*
         int n_done = 0;
         for (int c = 0; c < h->n_slabs; ++c) {
             const int n_end = h->slab_node_end[c];
-            rc = evaluate_range(h, time, h->d_U, h->d_fint, dk, s, h->slab_e[c], h->slab_e[c + 1], n_done, n_end);
+            rc = evaluate_range(h, time, h->d_U, h->d_fint, dk, s, h->slab_e[c], h->slab_e[c + 1], c);
             if (rc) return rc;
             if (n_end > n_done) {
                 CK(cudaEventRecord(h->slab_ev[c], s));
@@ -812,12 +898,9 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
         CK(cudaMemcpy(d_mat_id, mid.data(), E * sizeof(int), cudaMemcpyHostToDevice));
     }
     host_params = P;
-    if (precision == CEOS_MIXED) {
-        // blocked FP32 assembly scratch and per-node arrival counters
-        n_blocks = (long long)N + (nnz - 6LL * (long long)N) / 9;
-        CK(cudaMalloc(&d_kblk, (size_t)n_blocks * 12 * sizeof(float)));
-        CK(cudaMemset(d_kblk, 0, (size_t)n_blocks * 12 * sizeof(float)));
-    }
+    // node-pair blocks of the FP32 assembly: one diagonal block per node, one per upper neighbour
+    // (the ring that holds them is sized with the schedule, build_schedule)
+    n_blocks = (long long)N + (nnz - 6LL * (long long)N) / 9;
     // state variables actually used (the Prony model reads/writes only nb of its 4 branch slots)
     ns_used = nstate;
     if (model == M_VISCO_PRONY && param_mode == 0) ns_used = 6 + 6 * std::max(0, std::min(4, (int)P[2]));
@@ -851,7 +934,8 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
 Handle::~Handle() {
     if (stream) cudaStreamSynchronize(stream);
     void* ptrs[] = {d_X, d_U, d_fint, d_kval, d_conn, d_rs, d_blk0, d_nup, d_ranks, d_elem_status, d_status_count,
-                    d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress, d_kblk};
+                    d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress, d_kblk, d_queue, d_conv,
+                    d_tile_wait, d_flags, d_ticket, d_sched_err};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (ev_k0) cudaEventDestroy(ev_k0);

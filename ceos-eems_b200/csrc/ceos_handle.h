@@ -38,8 +38,22 @@ struct Handle {
     int* d_mat_id = nullptr;
     void* d_state[2] = {nullptr, nullptr};
     void* d_gp_stress = nullptr;
-    float* d_kblk = nullptr;              // mixed mode: FP32 node-pair block scratch
+    float* d_kblk = nullptr;              // mixed mode: ring of FP32 node-pair blocks (ring_blocks of them)
     long long n_blocks = 0;
+    // fused assembly schedule (mixed mode with a tangent): a queue of element tiles and CSR
+    // conversion items, split at the element slabs of the host-buffer evaluation
+    std::vector<int> queue;               // >= 0 tile, < 0 conversion item -(j+1)
+    std::vector<int> slab_q;              // [n_slabs + 1] queue position where slab c starts
+    int n_tiles = 0, n_conv = 0;
+    uint32_t ring_blocks = 0;             // power of two; block b lives in slot b & (ring_blocks - 1)
+    int* d_queue = nullptr;
+    void* d_conv = nullptr;               // int4 [n_conv] {first node, end node, first tile, last tile}
+    void* d_tile_wait = nullptr;          // int2 [n_tiles] conversion items that last used the tile's slots
+    unsigned* d_flags = nullptr;          // [n_tiles] tile done, [n_conv] conversion done (epoch values)
+    unsigned* d_ticket = nullptr;         // work counter of the running launch
+    int* d_sched_err = nullptr;           // a bounded wait gave up
+    unsigned epoch = 0;
+    bool ring_dirty = false;              // an aborted evaluation may have left non-zero slots
     int cur_old = 0;                      // index of the committed state buffer
     bool evaluated = false;
     double time_old = 0.0, time_eval = 0.0;

@@ -16,10 +16,24 @@
 //   phase B : thread (node b, element e) accumulates over the 8 Gauss points the internal force
 //             of node b (B^T sigma, ElementInternalForce :547-563) and its 3x3 stiffness blocks
 //             K_ab = B_a^T D B_b + (g_a . sigma g_b) I (ElementStiffnessMatrix :320-348) for the
-//             node pairs it owns, then scatters them with FP64 atomics into f_int and the upper
-//             CSR through the precomputed slot map.
+//             node pairs it owns, then scatters them into f_int and K.
 // Warp-uniform roles (gp or b is the warp index) keep control flow convergent; the shared
 // layouts put the element index innermost so every shared access is conflict-free.
+//
+// Two kernels use these phases:
+//   element_loop_kernel<T, MODEL>: static tile schedule; K by FP64 atomics straight into the
+//     CSR values (CEOS_FP64), or no K (an evaluation without tangent);
+//   element_assemble_kernel<MODEL>: CEOS_MIXED with a tangent.  K accumulates in FP32 node-pair
+//     blocks (3 rows x 4 floats per node pair) by 16-byte vector reductions, and the same launch
+//     turns finished blocks into the FP64 CSR rows.  The blocks live in a ring of 2^k blocks
+//     (block b in slot b & mask) sized to stay in L2, so the FP32 accumulation never travels to
+//     HBM: HBM sees the inputs once and the FP64 K once.  The CTAs take work from a queue built on
+//     the host: element tiles, and conversion items (a run of node rows) placed after the last
+//     tile that touches those rows.  A conversion item waits until those tiles have reduced;
+//     a tile waits until the items that last used its ring slots have written their rows and
+//     zeroed the slots.  Every wait is for work earlier in the queue (the host checks this), so
+//     the earliest unfinished item can always proceed; each wait is also bounded and reports a
+//     scheduling error instead of hanging.
 #pragma once
 #include "ceos_common.cuh"
 #include "materials.cuh"
@@ -29,6 +43,8 @@ namespace ceos {
 
 constexpr int kTileE = 32;
 constexpr int kThreads = 256;
+constexpr int kEndItem = -0x7fffffff - 1;   // queue sentinel: no more work
+constexpr unsigned long long kWaitNs = 200ull * 1000 * 1000;  // bound of every flag wait: 200 ms
 
 // dN/dxi of the 8 nodes at the 8 Gauss points (ModElementHexa8.f90:211-268, points :278-329).
 // (defined once: this header is included by a single translation unit)
@@ -37,7 +53,7 @@ __constant__ double c_dN[8][8][3];
 template <typename T>
 struct ElemArgs {
     int n_elem;
-    int e_begin, e_end;     // element range of this launch
+    int e_begin, e_end;     // element range of this launch (static schedule)
     const double* X;        // [3*n_nodes] reference coordinates (CoordX)
     const double* U;        // [3*n_nodes] displacements, DOF 3n+d
     const int* conn;        // [n_elem*8] 0-based node ids
@@ -61,9 +77,19 @@ struct ElemArgs {
     uint8_t* elem_status;   // [n_elem]
     int* status_count;      // failed elements
     T* gp_stress;           // [6][8][n_elem] or nullptr
-    // Blocked FP32 assembly (CEOS_MIXED): node-pair blocks of 3 rows x 4 floats, node n's row
-    // block starts at block n + (rs[n] - 6n)/9 (diagonal block, then one per upper neighbour).
-    float* kblk;            // [n_blocks*12] accumulation scratch, zero between evaluations
+    // ---- fused assembly (element_assemble_kernel) ----
+    float* kblk;            // ring of FP32 node-pair blocks, 12 floats each, zero between evaluations
+    uint32_t ring_mask;     // block b lives in slot b & ring_mask
+    const long long* csr_rs;   // [n_nodes] CSR position of row 3n (0-based)
+    const int* queue;       // work items: >= 0 element tile, < 0 conversion item -(j+1)
+    int q_begin, q_end;     // this launch's part of the queue
+    unsigned* ticket;       // work counter, zero at launch
+    unsigned* tile_done;    // [n_tiles] = epoch once the tile's reductions are complete
+    unsigned* conv_done;    // [n_conv] = epoch once the item's rows are written and slots zeroed
+    unsigned epoch;
+    const int4* conv;       // [n_conv] {first node, end node, first tile, last tile} of an item
+    const int2* tile_wait;  // [n_tiles] items [x, y) that last used the ring slots of the tile
+    int* sched_err;         // set when a wait exceeds its bound
 };
 
 // Dynamic shared-memory layout of one CTA.  Arrays indexed [..][e] with the element index
@@ -94,6 +120,26 @@ struct SmemLayout {
         total = o;
     }
 };
+// The conversion of a run of CSR rows stages its FP64 values in the g and ds regions (unused
+// between tiles), so an item holds at most this many K values.
+constexpr int kStageDoubles = (int)((sizeof(float) * 8 * 8 * kTileE * 4 + sizeof(float) * 8 * 7 * kTileE * 4) / 8) - 2;
+
+template <typename T>
+struct SmemPtrs {
+    T *g, *ds, *st, *kd;
+    double *x, *u;
+    float* xf;
+    long long* rs;
+    int *nup, *node, *status;
+    uint32_t* ranks;
+    CEOS_D SmemPtrs(unsigned char* raw, const SmemLayout<T>& L)
+        : g(reinterpret_cast<T*>(raw + L.g)), ds(reinterpret_cast<T*>(raw + L.ds)),
+          st(reinterpret_cast<T*>(raw + L.st)), kd(reinterpret_cast<T*>(raw + L.kd)),
+          x(reinterpret_cast<double*>(raw + L.x)), u(reinterpret_cast<double*>(raw + L.u)),
+          xf(reinterpret_cast<float*>(raw + L.xf)), rs(reinterpret_cast<long long*>(raw + L.rs)),
+          nup(reinterpret_cast<int*>(raw + L.nup)), node(reinterpret_cast<int*>(raw + L.node)),
+          status(reinterpret_cast<int*>(raw + L.status)), ranks(reinterpret_cast<uint32_t*>(raw + L.ranks)) {}
+};
 
 CEOS_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 CEOS_D void cp_async4(void* dst, const void* src) {
@@ -107,6 +153,41 @@ CEOS_D void cp_async16(void* dst, const void* src) {
 }
 CEOS_D void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 CEOS_D void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+CEOS_D unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+CEOS_D void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+CEOS_D unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;\n" : "=l"(t));
+    return t;
+}
+
+// One warp waits until flags[lo..hi) all equal epoch.  Gives up when kWaitNs pass or when another
+// CTA has given up (*err set): then it sets *err and returns false.  The result is the same in
+// every lane.
+CEOS_D bool warp_wait_flags(const unsigned* flags, int lo, int hi, unsigned epoch, int lane, int* err) {
+    bool ok = true;
+    const unsigned long long t0 = global_ns();
+    for (int i = lo + lane; i < hi && ok; i += 32) {
+        while (ld_acquire_u32(flags + i) != epoch) {
+            if (*reinterpret_cast<volatile int*>(err) != 0 || global_ns() - t0 > kWaitNs) {
+                ok = false;
+                break;
+            }
+            __nanosleep(100);
+        }
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    if (!ok && lane == 0) atomicOr(err, 1);
+    return ok;
+}
 
 // Gauss-point state access: committed values from the prefetched shared copy, new values
 // streamed to global memory with the evict-first hint (L2 is kept for the K scatter).
@@ -170,7 +251,7 @@ CEOS_D void ld4(const T* p, T& a, T& b, T& c, T& d) {
     }
 }
 
-// Stage the connectivity and slot ranks of tile `tile` into buffer `buf` (async).
+// Stage the connectivity and slot ranks of the tile starting at element e0 into one buffer (async).
 template <typename T>
 CEOS_D void prefetch_conn(const ElemArgs<T>& a, int e0, int* node_s, uint32_t* ranks_s, int t) {
     const int e = t >> 3, n = t & 7;
@@ -184,7 +265,7 @@ CEOS_D void prefetch_conn(const ElemArgs<T>& a, int e0, int* node_s, uint32_t* r
 // tile whose node ids are already in node_s (async).
 template <typename T>
 CEOS_D void prefetch_nodes_state(const ElemArgs<T>& a, int e0, const int* node_s, double* xs, double* us,
-                                 float* xf, long long* rs_s, int* nup_s, T* st_s, int t) {
+                                 long long* rs_s, int* nup_s, T* st_s, int t) {
     const int lane = t & 31, n = t >> 5;
     if (e0 + lane < a.e_end) {
         const int node = node_s[n * kTileE + lane];
@@ -216,55 +297,462 @@ CEOS_D void red_v4(float* p, float a, float b, float c, float d) {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
 }
 
-// Convert the row block of `node` from the FP32 block scratch into its three FP64 CSR rows and
-// zero the scratch again.  Executed by a whole warp: lanes walk each CSR row segment in order,
-// so every store instruction writes 32 consecutive doubles (full sectors).
-CEOS_D void finalize_row_block(int node, long long rs, int m, float* kblk, double* K, int lane) {
-    const long long bb = (long long)node + (rs - 6LL * node) / 9;  // first block of this node
-    const float* blk = kblk + bb * 12;
+// FP32 mode: one FP64 -> FP32 conversion per (node, element), of the differences to the element's
+// node 0: X_n - X_0 and u_n - u_0 are formed in FP64, so the FP32 values keep their relative
+// precision at the element scale (absolute coordinates rounded to FP32 would perturb an element of
+// size h by ~6e-8 / h, which the bulk modulus of a nearly incompressible material amplifies in
+// f_int).  J_X and J_u are unchanged by the shift because sum_n dN_n/dxi = 0.  Contains barriers.
+CEOS_D void stage_local_differences(const SmemPtrs<float>& s, int warp, int lane) {
+    const int n = warp, el = lane;
+    const double* xp = s.x + (n * kTileE + el) * 3;
+    const double* up = s.u + (n * kTileE + el) * 3;
+    const double* x0 = s.x + el * 3;
+    const double* u0 = s.u + el * 3;
+    const float4 dx = make_float4((float)(xp[0] - x0[0]), (float)(xp[1] - x0[1]), (float)(xp[2] - x0[2]), 0.f);
+    const float4 du = make_float4((float)(up[0] - u0[0]), (float)(up[1] - u0[1]), (float)(up[2] - u0[2]), 0.f);
+    __syncthreads();  // every thread has read the FP64 staging that the FP32 tile overlays
+    float4* dst = reinterpret_cast<float4*>(s.xf + (n * kTileE + el) * 8);
+    dst[0] = dx;
+    dst[1] = du;
+    __syncthreads();
+}
+
+// Phase A for thread (gp = warp, element = lane) of the tile at e0.
+template <typename T, int MODEL>
+CEOS_D void phase_a(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp, int lane) {
+    constexpr int NP = ModelInfo<MODEL>::nparams;
+    const int gp = warp, el = lane, e = e0 + el;
+    if (e >= a.e_end) return;
+    int status = 0;
+    // J_X = sum dN/dxi (x) X and J_u = sum dN/dxi (x) u; the current Jacobian is J_X + J_u, and
+    // F = I + (J_X^-1 J_u)^T equals DeformationGradient's I + sum u (x) grad_X N with the
+    // displacement gradient formed from small numbers (no I + O(1) cancellation in FP32)
+    T JX[3][3] = {}, Ju[3][3] = {};
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        // row 3n+k: the diagonal-block entries l >= k, then 3 entries per upper neighbour block
-        const long long rstart = rs + (k == 0 ? 0LL : (k == 1 ? 3LL + 3LL * m : 5LL + 6LL * m));
-        const int nd = 3 - k, len = nd + 3 * m;
-        for (int p = lane; p < len; p += 32) {
-            int j, l;
-            if (p < nd) { j = 0; l = k + p; }
-            else { const int pp = p - nd; j = 1 + pp / 3; l = pp - 3 * (pp / 3); }
-            K[rstart + p] = (double)__ldcg(blk + j * 12 + 4 * k + l);
+    for (int n = 0; n < 8; ++n) {
+        T X[3], u[3];
+        if constexpr (sizeof(T) == 4) {
+            const float4* q = reinterpret_cast<const float4*>(s.xf + (n * kTileE + el) * 8);
+            const float4 xv = q[0], uv = q[1];
+            X[0] = xv.x; X[1] = xv.y; X[2] = xv.z;
+            u[0] = uv.x; u[1] = uv.y; u[2] = uv.z;
+        } else {
+            const double* xp = s.x + (n * kTileE + el) * 3;
+            const double* up = s.u + (n * kTileE + el) * 3;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                X[d] = (T)xp[d];
+                u[d] = (T)up[d];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const T dn = (T)c_dN[gp][n][i];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                JX[i][j] += dn * X[j];
+                Ju[i][j] += dn * u[j];
+            }
         }
     }
-    __syncwarp();
-    float4* z = reinterpret_cast<float4*>(kblk + bb * 12);
-    for (int q = lane; q < 3 * (1 + m); q += 32) __stcg(z + q, make_float4(0.f, 0.f, 0.f, 0.f));
+    T Jc[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Jc[i][j] = JX[i][j] + Ju[i][j];
+    const T detJX = det3(JX);
+    const T detJ = det3(Jc);
+    if (!(detJX > T(1.0e-13)) || !(detJ > T(1.0e-13))) status |= 1;
+    T JXi[3][3], Jci[3][3];
+    inv3(JX, detJX, JXi);
+    inv3(Jc, detJ, Jci);
+    // F[i][j] = delta_ij + sum_k JXi[j][k] Ju[k][i]
+    T F[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            F[i][j] = (i == j ? T(1) : T(0)) + (JXi[j][0] * Ju[0][i] + JXi[j][1] * Ju[1][i] + JXi[j][2] * Ju[2][i]);
+    // current gradients grad_x N of the 8 nodes for phase B
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        const T d0 = (T)c_dN[gp][n][0], d1 = (T)c_dN[gp][n][1], d2 = (T)c_dN[gp][n][2];
+        T gx[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) gx[j] = (status & 1) ? T(0) : Jci[j][0] * d0 + Jci[j][1] * d1 + Jci[j][2] * d2;
+        st4<T>(s.g + ((gp * 8 + n) * kTileE + el) * 4, gx[0], gx[1], gx[2], T(0));
+    }
+    // constitutive update
+    T p[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        if (a.param_mode == 0) p[k] = a.pu[k];
+        else if (a.param_mode == 1) p[k] = a.params[(size_t)k * a.n_elem + e];
+        else p[k] = a.params[(size_t)__ldg(a.mat_id + e) * a.n_params + k];
+    }
+    StateIO<T> io{s.st + gp * kTileE + el, a.st_new, (size_t)8 * a.ld, (size_t)gp * a.ld + e};
+    T sig[6], D[21];
+    if (status & 1) {
+        if constexpr (MODEL == M_NH_Q1P0)
+            if (gp == 0) s.kd[el] = T(0);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sig[k] = T(0);
+#pragma unroll
+        for (int k = 0; k < 21; ++k) D[k] = T(0);
+        for (int k = 0; k < a.ns_used; ++k) io.st(k, io.ld(k));
+    } else {
+        T ebr[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (MODEL == M_VISCO_PRONY && a.param_mode != 0)
+                ebr[k] = texp<T>((T)(-a.dt) / (T(2) * p[4 + 2 * k]));
+            else
+                ebr[k] = a.ebr[k];
+        }
+        if constexpr (MODEL == M_NH_Q1P0) {
+            // Jbar = V / V0 (ElementVolume, ModElement.f90:1313-1427): every Gauss-point
+            // thread of the element sums the same 8 determinants (no barrier needed)
+            double V = 0.0, V0 = 0.0;
+#pragma unroll 1
+            for (int g2 = 0; g2 < 8; ++g2) {
+                T JX2[3][3] = {}, Jc2[3][3] = {};
+#pragma unroll
+                for (int n = 0; n < 8; ++n) {
+                    T X[3], x[3];
+                    if constexpr (sizeof(T) == 4) {
+                        const float4* q = reinterpret_cast<const float4*>(s.xf + (n * kTileE + el) * 8);
+                        const float4 xv = q[0], uv = q[1];
+                        X[0] = xv.x; X[1] = xv.y; X[2] = xv.z;
+                        x[0] = xv.x + uv.x; x[1] = xv.y + uv.y; x[2] = xv.z + uv.z;
+                    } else {
+                        const double* xp = s.x + (n * kTileE + el) * 3;
+                        const double* up = s.u + (n * kTileE + el) * 3;
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            X[d] = (T)xp[d];
+                            x[d] = (T)(xp[d] + up[d]);
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const T dn = (T)c_dN[g2][n][i];
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) {
+                            JX2[i][j] += dn * X[j];
+                            Jc2[i][j] += dn * x[j];
+                        }
+                    }
+                }
+                V0 += (double)det3(JX2);
+                V += (double)det3(Jc2);
+            }
+            const double Jbar = V / V0;
+            nh_q1p0_update<T>(F, p, Jbar, sig, D);
+            if (gp == 0) s.kd[el] = (T)(nh_q1p0_d2psi((double)p[1], Jbar) / V0);
+        } else {
+            status |= run_material<T, MODEL>(F, p, ebr, a.dt, io, sig, D);
+        }
+    }
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) finite = finite && isfinite(sig[k]);
+    if (!finite) status |= 4;
+    if (a.gp_stress) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) a.gp_stress[((size_t)k * 8 + gp) * a.n_elem + e] = sig[k];
+    }
+    const T w = (status & 5) ? T(0) : detJ;  // Gauss weight is 1 (Hexa8 full integration)
+    T* dst = s.ds + (size_t)gp * 7 * kTileE * 4 + el * 4;
+#pragma unroll
+    for (int q = 0; q < 5; ++q)
+        st4<T>(dst + q * kTileE * 4, w * D[4 * q], w * D[4 * q + 1], w * D[4 * q + 2], w * D[4 * q + 3]);
+    st4<T>(dst + 5 * kTileE * 4, w * D[20], w * sig[0], w * sig[1], w * sig[2]);
+    st4<T>(dst + 6 * kTileE * 4, w * sig[3], w * sig[4], w * sig[5], w);  // w: Mean Dilatation
+    if (status) atomicOr(&s.status[el], status);
 }
 
-// Block scratch -> FP64 CSR values of K, one warp per node row block; leaves the scratch zero.
-__global__ void __launch_bounds__(256) kblock_to_csr_kernel(int n_begin, int n_end, const long long* __restrict__ rs,
-                                                            const int* __restrict__ nup, float* kblk, double* K) {
-    const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int n = n_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); n < n_end; n += warps)
-        finalize_row_block(n, __ldg(rs + n), __ldg(nup + n), kblk, K, lane);
+// Element status of the tile (threads t < kTileE), then clear the shared status words.
+template <typename T>
+CEOS_D void tile_status(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int t) {
+    if (t < kTileE) {
+        if (e0 + t < a.e_end) {
+            const int st = s.status[t];
+            a.elem_status[e0 + t] = (uint8_t)st;
+            if (st) atomicAdd(a.status_count, 1);
+        }
+        s.status[t] = 0;
+    }
 }
 
-template <typename T, int MODEL, bool BLOCKED>
+enum : int { SCATTER_CSR64 = 0, SCATTER_RING = 1 };
+
+// Phase B for thread (node b = warp, element = lane) of the tile at e0; node_c, rs_c, nup_c and
+// ranks_c are the tile's buffers.  SCATTER_CSR64: K by FP64 atomics into the CSR values (skipped
+// when a.kval is null); SCATTER_RING: K by FP32 vector reductions into the node-pair block ring.
+template <typename T, int MODEL, int SCATTER>
+CEOS_D void phase_b(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp, int lane, const int* node_c,
+                    const long long* rs_c, const int* nup_c, const uint32_t* ranks_c) {
+    const int b = warp, el = lane, e = e0 + el;
+    if (e >= a.e_end) return;
+    const int npair = (b < 4) ? 4 : 3;  // off-diagonal partners a = b+1..b+npair (mod 8)
+    T f0 = 0, f1 = 0, f2 = 0;
+    T Kd[6] = {0, 0, 0, 0, 0, 0};
+    T Ko[4][9];
+    // Mean Dilatation: Bdiv of node b and of its partners, sum_gp w detJ grad N (current)
+    T bdb[3] = {T(0), T(0), T(0)}, bda[4][3] = {};
+    // FP32: the 3x3 blocks accumulate two columns per packed FMA (sm_100 FFMA2).  Row 0
+    // pairs column 2 with the geometric term g_a . sigma g_b, which enters the diagonal
+    // of the block once after the Gauss-point loop.
+    float2 Pa[4][3], Pc[4], Da = {0.f, 0.f}, Dc = {0.f, 0.f};
+    float Pr[4][2], d11 = 0.f, d12 = 0.f, d22 = 0.f;
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            Pa[o][0] = Pa[o][1] = Pa[o][2] = Pc[o] = make_float2(0.f, 0.f);
+            Pr[o][0] = Pr[o][1] = 0.f;
+        }
+    } else {
+#pragma unroll
+        for (int o = 0; o < 4; ++o)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Ko[o][k] = T(0);
+    }
+#pragma unroll 2
+    for (int gp = 0; gp < 8; ++gp) {
+        const T* src = s.ds + (size_t)gp * 7 * kTileE * 4 + el * 4;
+        T Dm[21], s0, s1, s2, s3, s4, s5, pad;
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+            ld4<T>(src + q * kTileE * 4, Dm[4 * q], Dm[4 * q + 1], Dm[4 * q + 2], Dm[4 * q + 3]);
+        ld4<T>(src + 5 * kTileE * 4, Dm[20], s0, s1, s2);
+        T wgp;
+        ld4<T>(src + 6 * kTileE * 4, s3, s4, s5, wgp);
+        const T* gsrc = s.g + (size_t)gp * 8 * kTileE * 4 + el * 4;
+        T gx, gy, gz;
+        ld4<T>(gsrc + b * kTileE * 4, gx, gy, gz, pad);
+        if constexpr (MODEL == M_NH_Q1P0) {
+            bdb[0] += wgp * gx;
+            bdb[1] += wgp * gy;
+            bdb[2] += wgp * gz;
+        }
+        // sigma g_b: the internal force of node b and the geometric term
+        const T q0 = s0 * gx + s3 * gy + s5 * gz;
+        const T q1 = s3 * gx + s1 * gy + s4 * gz;
+        const T q2 = s5 * gx + s4 * gy + s2 * gz;
+        f0 += q0; f1 += q1; f2 += q2;
+        // DB = D B_b (6x3), D symmetric from its upper triangle
+        T DB[6][3];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const T d0 = Dm[i <= 0 ? up21(i, 0) : up21(0, i)];
+            const T d1 = Dm[i <= 1 ? up21(i, 1) : up21(1, i)];
+            const T d2 = Dm[i <= 2 ? up21(i, 2) : up21(2, i)];
+            const T d3 = Dm[i <= 3 ? up21(i, 3) : up21(3, i)];
+            const T d4 = Dm[i <= 4 ? up21(i, 4) : up21(4, i)];
+            const T d5 = Dm[i <= 5 ? up21(i, 5) : up21(5, i)];
+            DB[i][0] = d0 * gx + d3 * gy + d5 * gz;
+            DB[i][1] = d1 * gy + d3 * gx + d4 * gz;
+            DB[i][2] = d2 * gz + d4 * gy + d5 * gx;
+        }
+        if constexpr (sizeof(T) == 4) {
+            float2 P[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) P[i] = make_float2(DB[i][0], DB[i][1]);
+            const float2 z0 = make_float2(DB[0][2], q0), z3 = make_float2(DB[3][2], q1),
+                         z5 = make_float2(DB[5][2], q2);
+            {   // diagonal block (b,b), upper 6
+                const float2 bx = make_float2(gx, gx), by = make_float2(gy, gy), bz = make_float2(gz, gz);
+                Da = __ffma2_rn(bx, P[0], Da); Da = __ffma2_rn(by, P[3], Da); Da = __ffma2_rn(bz, P[5], Da);
+                Dc = __ffma2_rn(bx, z0, Dc);   Dc = __ffma2_rn(by, z3, Dc);   Dc = __ffma2_rn(bz, z5, Dc);
+                d11 += gy * P[1].y + gx * P[3].y + gz * P[4].y;
+                d12 += gy * DB[1][2] + gx * DB[3][2] + gz * DB[4][2];
+                d22 += gz * DB[2][2] + gy * DB[4][2] + gx * DB[5][2];
+            }
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+                if (o < npair) {
+                    const int an = (b + 1 + o) & 7;
+                    T ax, ay, az;
+                    ld4<T>(gsrc + an * kTileE * 4, ax, ay, az, pad);
+                    if constexpr (MODEL == M_NH_Q1P0) {
+                        bda[o][0] += wgp * ax;
+                        bda[o][1] += wgp * ay;
+                        bda[o][2] += wgp * az;
+                    }
+                    const float2 bx = make_float2(ax, ax), by = make_float2(ay, ay), bz = make_float2(az, az);
+                    Pa[o][0] = __ffma2_rn(bx, P[0], Pa[o][0]);
+                    Pa[o][0] = __ffma2_rn(by, P[3], Pa[o][0]);
+                    Pa[o][0] = __ffma2_rn(bz, P[5], Pa[o][0]);
+                    Pc[o] = __ffma2_rn(bx, z0, Pc[o]);
+                    Pc[o] = __ffma2_rn(by, z3, Pc[o]);
+                    Pc[o] = __ffma2_rn(bz, z5, Pc[o]);
+                    Pa[o][1] = __ffma2_rn(by, P[1], Pa[o][1]);
+                    Pa[o][1] = __ffma2_rn(bx, P[3], Pa[o][1]);
+                    Pa[o][1] = __ffma2_rn(bz, P[4], Pa[o][1]);
+                    Pr[o][0] += ay * DB[1][2] + ax * DB[3][2] + az * DB[4][2];
+                    Pa[o][2] = __ffma2_rn(bz, P[2], Pa[o][2]);
+                    Pa[o][2] = __ffma2_rn(by, P[4], Pa[o][2]);
+                    Pa[o][2] = __ffma2_rn(bx, P[5], Pa[o][2]);
+                    Pr[o][1] += az * DB[2][2] + ay * DB[4][2] + ax * DB[5][2];
+                }
+            }
+        } else {
+            // diagonal block (b,b), upper 6
+            {
+                const T geo = gx * q0 + gy * q1 + gz * q2;
+                Kd[0] += gx * DB[0][0] + gy * DB[3][0] + gz * DB[5][0] + geo;
+                Kd[1] += gx * DB[0][1] + gy * DB[3][1] + gz * DB[5][1];
+                Kd[2] += gx * DB[0][2] + gy * DB[3][2] + gz * DB[5][2];
+                Kd[3] += gy * DB[1][1] + gx * DB[3][1] + gz * DB[4][1] + geo;
+                Kd[4] += gy * DB[1][2] + gx * DB[3][2] + gz * DB[4][2];
+                Kd[5] += gz * DB[2][2] + gy * DB[4][2] + gx * DB[5][2] + geo;
+            }
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+                if (o < npair) {
+                    const int an = (b + 1 + o) & 7;
+                    T ax, ay, az;
+                    ld4<T>(gsrc + an * kTileE * 4, ax, ay, az, pad);
+                    const T geo = ax * q0 + ay * q1 + az * q2;
+                    if constexpr (MODEL == M_NH_Q1P0) {
+                        bda[o][0] += wgp * ax;
+                        bda[o][1] += wgp * ay;
+                        bda[o][2] += wgp * az;
+                    }
+#pragma unroll
+                    for (int l = 0; l < 3; ++l) {
+                        Ko[o][0 * 3 + l] += ax * DB[0][l] + ay * DB[3][l] + az * DB[5][l];
+                        Ko[o][1 * 3 + l] += ay * DB[1][l] + ax * DB[3][l] + az * DB[4][l];
+                        Ko[o][2 * 3 + l] += az * DB[2][l] + ay * DB[4][l] + ax * DB[5][l];
+                    }
+                    Ko[o][0] += geo; Ko[o][4] += geo; Ko[o][8] += geo;
+                }
+            }
+        }
+    }
+    if constexpr (sizeof(T) == 4) {  // unpack the column pairs, add the geometric terms
+        const float gb = Dc.y;
+        Kd[0] = Da.x + gb; Kd[1] = Da.y; Kd[2] = Dc.x;
+        Kd[3] = d11 + gb;  Kd[4] = d12;  Kd[5] = d22 + gb;
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            const float ga = Pc[o].y;
+            Ko[o][0] = Pa[o][0].x + ga; Ko[o][1] = Pa[o][0].y; Ko[o][2] = Pc[o].x;
+            Ko[o][3] = Pa[o][1].x;      Ko[o][4] = Pa[o][1].y + ga; Ko[o][5] = Pr[o][0];
+            Ko[o][6] = Pa[o][2].x;      Ko[o][7] = Pa[o][2].y; Ko[o][8] = Pr[o][1] + ga;
+        }
+    }
+    if constexpr (MODEL == M_NH_Q1P0) {  // Bdiv^T Bdiv d2psi/dJbar2 / V0 (ModElement.f90:463-466)
+        const T kd = isfinite(s.kd[el]) ? s.kd[el] : T(0);  // failed elements have Bdiv = 0
+        Kd[0] += kd * bdb[0] * bdb[0];
+        Kd[1] += kd * bdb[0] * bdb[1];
+        Kd[2] += kd * bdb[0] * bdb[2];
+        Kd[3] += kd * bdb[1] * bdb[1];
+        Kd[4] += kd * bdb[1] * bdb[2];
+        Kd[5] += kd * bdb[2] * bdb[2];
+#pragma unroll
+        for (int o = 0; o < 4; ++o)
+            if (o < npair)
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+#pragma unroll
+                    for (int l = 0; l < 3; ++l) Ko[o][k * 3 + l] += kd * bda[o][k] * bdb[l];
+    }
+    // ---- scatter ----
+    const int Bn = node_c[b * kTileE + el];
+    atomicAdd(a.fint + 3 * (size_t)Bn + 0, (double)f0);
+    atomicAdd(a.fint + 3 * (size_t)Bn + 1, (double)f1);
+    atomicAdd(a.fint + 3 * (size_t)Bn + 2, (double)f2);
+    if constexpr (SCATTER == SCATTER_CSR64) {
+        if (!a.kval) return;
+        {
+            const long long r0 = rs_c[b * kTileE + el];
+            const int m = nup_c[b * kTileE + el];
+            const long long r1 = r0 + 3 + 3 * m, r2 = r1 + 2 + 3 * m;
+            double* K = a.kval;
+            atomicAdd(K + r0 + 0, (double)Kd[0]);
+            atomicAdd(K + r0 + 1, (double)Kd[1]);
+            atomicAdd(K + r0 + 2, (double)Kd[2]);
+            atomicAdd(K + r1 + 0, (double)Kd[3]);
+            atomicAdd(K + r1 + 1, (double)Kd[4]);
+            atomicAdd(K + r2 + 0, (double)Kd[5]);
+        }
+        const uint8_t* rk = reinterpret_cast<const uint8_t*>(ranks_c + el * 8);
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            if (o < npair) {
+                const int an = (b + 1 + o) & 7;
+                const int An = node_c[an * kTileE + el];
+                const int lo_local = an < b ? an : b, hi_local = an < b ? b : an;
+                const int r = rk[pair_index(lo_local, hi_local)];
+                const bool a_low = An < Bn;  // rows belong to the smaller global node
+                const int lo_n = a_low ? an : b;
+                const long long r0 = rs_c[lo_n * kTileE + el];
+                const int m = nup_c[lo_n * kTileE + el];
+                const long long row0 = r0 + 3 + 3 * r;
+                const long long row1 = r0 + (3 + 3 * m) + 2 + 3 * r;
+                const long long row2 = r0 + (3 + 3 * m) + (2 + 3 * m) + 1 + 3 * r;
+                double* K = a.kval;
+                if (a_low) {  // (3A+k, 3B+l) += M[k][l]
+#pragma unroll
+                    for (int l = 0; l < 3; ++l) {
+                        atomicAdd(K + row0 + l, (double)Ko[o][0 * 3 + l]);
+                        atomicAdd(K + row1 + l, (double)Ko[o][1 * 3 + l]);
+                        atomicAdd(K + row2 + l, (double)Ko[o][2 * 3 + l]);
+                    }
+                } else {  // (3B+l, 3A+k) += M[k][l]
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        atomicAdd(K + row0 + k, (double)Ko[o][k * 3 + 0]);
+                        atomicAdd(K + row1 + k, (double)Ko[o][k * 3 + 1]);
+                        atomicAdd(K + row2 + k, (double)Ko[o][k * 3 + 2]);
+                    }
+                }
+            }
+        }
+    } else {
+        // node-pair blocks in the ring: one 16-byte vector reduction per block row; rs_c holds the
+        // first block of each node, the slot of block q is q & ring_mask
+        const uint32_t mask = a.ring_mask;
+        {
+            float* blk = a.kblk + (size_t)((uint32_t)rs_c[b * kTileE + el] & mask) * 12;
+            red_v4(blk + 0, (float)Kd[0], (float)Kd[1], (float)Kd[2], 0.f);
+            red_v4(blk + 4, 0.f, (float)Kd[3], (float)Kd[4], 0.f);
+            red_v4(blk + 8, 0.f, 0.f, (float)Kd[5], 0.f);
+        }
+        const uint8_t* rk = reinterpret_cast<const uint8_t*>(ranks_c + el * 8);
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            if (o < npair) {
+                const int an = (b + 1 + o) & 7;
+                const int An = node_c[an * kTileE + el];
+                const int lo_local = an < b ? an : b, hi_local = an < b ? b : an;
+                const int r = rk[pair_index(lo_local, hi_local)];
+                const bool a_low = An < Bn;
+                const int lo_n = a_low ? an : b;
+                float* blk = a.kblk + (size_t)(((uint32_t)rs_c[lo_n * kTileE + el] + 1u + (uint32_t)r) & mask) * 12;
+                if (a_low) {  // rows of node a: M[k][:]
+                    red_v4(blk + 0, (float)Ko[o][0], (float)Ko[o][1], (float)Ko[o][2], 0.f);
+                    red_v4(blk + 4, (float)Ko[o][3], (float)Ko[o][4], (float)Ko[o][5], 0.f);
+                    red_v4(blk + 8, (float)Ko[o][6], (float)Ko[o][7], (float)Ko[o][8], 0.f);
+                } else {      // rows of node b: M[:][l]
+                    red_v4(blk + 0, (float)Ko[o][0], (float)Ko[o][3], (float)Ko[o][6], 0.f);
+                    red_v4(blk + 4, (float)Ko[o][1], (float)Ko[o][4], (float)Ko[o][7], 0.f);
+                    red_v4(blk + 8, (float)Ko[o][2], (float)Ko[o][5], (float)Ko[o][8], 0.f);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Static schedule: FP64 mode (K by FP64 atomics) and evaluations without a tangent
+// ---------------------------------------------------------------------------------------------
+template <typename T, int MODEL>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop_kernel(ElemArgs<T> a) {
-    constexpr int NP = ModelInfo<MODEL>::nparams;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SmemLayout<T> L(a.ns_used);
-    T* sg = reinterpret_cast<T*>(smem_raw + L.g);
-    T* sds = reinterpret_cast<T*>(smem_raw + L.ds);
-    T* sst = reinterpret_cast<T*>(smem_raw + L.st);
-    double* sx = reinterpret_cast<double*>(smem_raw + L.x);
-    double* su = reinterpret_cast<double*>(smem_raw + L.u);
-    float* sxf = reinterpret_cast<float*>(smem_raw + L.xf);
-    long long* srs = reinterpret_cast<long long*>(smem_raw + L.rs);
-    int* snup = reinterpret_cast<int*>(smem_raw + L.nup);
-    int* snode = reinterpret_cast<int*>(smem_raw + L.node);
-    uint32_t* sranks = reinterpret_cast<uint32_t*>(smem_raw + L.ranks);
-    int* sstatus = reinterpret_cast<int*>(smem_raw + L.status);
-    T* skd = reinterpret_cast<T*>(smem_raw + L.kd);
+    const SmemPtrs<T> s(smem_raw, L);
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int n_tiles = (a.e_end - a.e_begin + kTileE - 1) / kTileE;
@@ -273,12 +761,12 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
     int tile = blockIdx.x;
     if (tile >= n_tiles) return;
     // prologue: connectivity of the first tile, then its node data and state
-    prefetch_conn(a, a.e_begin + tile * kTileE, snode, sranks, t);
+    prefetch_conn(a, a.e_begin + tile * kTileE, s.node, s.ranks, t);
     cp_commit();
-    if (t < kTileE) sstatus[t] = 0;
+    if (t < kTileE) s.status[t] = 0;
     cp_wait_all();
     __syncthreads();
-    prefetch_nodes_state(a, a.e_begin + tile * kTileE, snode, sx, su, sxf, srs, snup, sst, t);
+    prefetch_nodes_state(a, a.e_begin + tile * kTileE, s.node, s.x, s.u, s.rs, s.nup, s.st, t);
     cp_commit();
 
     for (int it = 0; tile < n_tiles; ++it, tile += gridDim.x) {
@@ -286,459 +774,186 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
         const int e0 = a.e_begin + tile * kTileE;
         const int next = tile + gridDim.x;
         const int e0n = a.e_begin + next * kTileE;
-        int* node_c = snode + buf * NB;
-        long long* rs_c = srs + buf * NB;
-        int* nup_c = snup + buf * NB;
-        const uint32_t* ranks_c = sranks + buf * NB;
         cp_wait_all();
         __syncthreads();  // node data and state of this tile are in shared memory
         if (next < n_tiles) {
-            prefetch_conn(a, e0n, snode + (buf ^ 1) * NB, sranks + (buf ^ 1) * NB, t);
+            prefetch_conn(a, e0n, s.node + (buf ^ 1) * NB, s.ranks + (buf ^ 1) * NB, t);
             cp_commit();
         }
-        if constexpr (sizeof(T) == 4) {
-            // One FP64 -> FP32 conversion per (node, element), of the differences to the element's
-            // node 0: X_n - X_0 and u_n - u_0 are formed in FP64, so the FP32 values keep their
-            // relative precision at the element scale (absolute coordinates rounded to FP32 would
-            // perturb an element of size h by ~6e-8 / h, which the bulk modulus of a nearly
-            // incompressible material amplifies in f_int).  J_X and J_u are unchanged by the shift
-            // because sum_n dN_n/dxi = 0.
-            const int n = warp, el = lane;
-            const double* xp = sx + (n * kTileE + el) * 3;
-            const double* up = su + (n * kTileE + el) * 3;
-            const double* x0 = sx + el * 3;
-            const double* u0 = su + el * 3;
-            const float4 dx = make_float4((float)(xp[0] - x0[0]), (float)(xp[1] - x0[1]), (float)(xp[2] - x0[2]), 0.f);
-            const float4 du = make_float4((float)(up[0] - u0[0]), (float)(up[1] - u0[1]), (float)(up[2] - u0[2]), 0.f);
-            __syncthreads();  // every thread has read the FP64 staging that the FP32 tile overlays
-            float4* dst = reinterpret_cast<float4*>(sxf + (n * kTileE + el) * 8);
-            dst[0] = dx;
-            dst[1] = du;
-            __syncthreads();
-        }
-
-        // ---------------- phase A: thread (gp = warp, element = lane) -----------------------
-        {
-            const int gp = warp, el = lane, e = e0 + el;
-            if (e < a.e_end) {
-                int status = 0;
-                // J_X = sum dN/dxi (x) X and J_u = sum dN/dxi (x) u; the current Jacobian is J_X + J_u, and
-                // F = I + (J_X^-1 J_u)^T equals DeformationGradient's I + sum u (x) grad_X N with the
-                // displacement gradient formed from small numbers (no I + O(1) cancellation in FP32)
-                T JX[3][3] = {}, Ju[3][3] = {};
-#pragma unroll
-                for (int n = 0; n < 8; ++n) {
-                    T X[3], u[3];
-                    if constexpr (sizeof(T) == 4) {
-                        const float4* q = reinterpret_cast<const float4*>(sxf + (n * kTileE + el) * 8);
-                        const float4 xv = q[0], uv = q[1];
-                        X[0] = xv.x; X[1] = xv.y; X[2] = xv.z;
-                        u[0] = uv.x; u[1] = uv.y; u[2] = uv.z;
-                    } else {
-                        const double* xp = sx + (n * kTileE + el) * 3;
-                        const double* up = su + (n * kTileE + el) * 3;
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            X[d] = (T)xp[d];
-                            u[d] = (T)up[d];
-                        }
-                    }
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        const T dn = (T)c_dN[gp][n][i];
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) {
-                            JX[i][j] += dn * X[j];
-                            Ju[i][j] += dn * u[j];
-                        }
-                    }
-                }
-                T Jc[3][3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) Jc[i][j] = JX[i][j] + Ju[i][j];
-                const T detJX = det3(JX);
-                const T detJ = det3(Jc);
-                if (!(detJX > T(1.0e-13)) || !(detJ > T(1.0e-13))) status |= 1;
-                T JXi[3][3], Jci[3][3];
-                inv3(JX, detJX, JXi);
-                inv3(Jc, detJ, Jci);
-                // F[i][j] = delta_ij + sum_k JXi[j][k] Ju[k][i]
-                T F[3][3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j)
-                        F[i][j] = (i == j ? T(1) : T(0)) + (JXi[j][0] * Ju[0][i] + JXi[j][1] * Ju[1][i] + JXi[j][2] * Ju[2][i]);
-                // current gradients grad_x N of the 8 nodes for phase B
-#pragma unroll
-                for (int n = 0; n < 8; ++n) {
-                    const T d0 = (T)c_dN[gp][n][0], d1 = (T)c_dN[gp][n][1], d2 = (T)c_dN[gp][n][2];
-                    T gx[3];
-#pragma unroll
-                    for (int j = 0; j < 3; ++j)
-                        gx[j] = (status & 1) ? T(0) : Jci[j][0] * d0 + Jci[j][1] * d1 + Jci[j][2] * d2;
-                    st4<T>(sg + ((gp * 8 + n) * kTileE + el) * 4, gx[0], gx[1], gx[2], T(0));
-                }
-                // constitutive update
-                T p[NP];
-#pragma unroll
-                for (int k = 0; k < NP; ++k) {
-                    if (a.param_mode == 0) p[k] = a.pu[k];
-                    else if (a.param_mode == 1) p[k] = a.params[(size_t)k * a.n_elem + e];
-                    else p[k] = a.params[(size_t)__ldg(a.mat_id + e) * a.n_params + k];
-                }
-                StateIO<T> io{sst + gp * kTileE + el, a.st_new, (size_t)8 * a.ld, (size_t)gp * a.ld + e};
-                T sig[6], D[21];
-                if (status & 1) {
-                    if constexpr (MODEL == M_NH_Q1P0)
-                        if (gp == 0) skd[el] = T(0);
-#pragma unroll
-                    for (int k = 0; k < 6; ++k) sig[k] = T(0);
-#pragma unroll
-                    for (int k = 0; k < 21; ++k) D[k] = T(0);
-                    for (int k = 0; k < a.ns_used; ++k) io.st(k, io.ld(k));
-                } else {
-                    T ebr[4];
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        if (MODEL == M_VISCO_PRONY && a.param_mode != 0)
-                            ebr[k] = texp<T>((T)(-a.dt) / (T(2) * p[4 + 2 * k]));
-                        else
-                            ebr[k] = a.ebr[k];
-                    }
-                    if constexpr (MODEL == M_NH_Q1P0) {
-                        // Jbar = V / V0 (ElementVolume, ModElement.f90:1313-1427): every Gauss-point
-                        // thread of the element sums the same 8 determinants (no barrier needed)
-                        double V = 0.0, V0 = 0.0;
-#pragma unroll 1
-                        for (int g2 = 0; g2 < 8; ++g2) {
-                            T JX2[3][3] = {}, Jc2[3][3] = {};
-#pragma unroll
-                            for (int n = 0; n < 8; ++n) {
-                                T X[3], x[3];
-                                if constexpr (sizeof(T) == 4) {
-                                    const float4* q = reinterpret_cast<const float4*>(sxf + (n * kTileE + el) * 8);
-                                    const float4 xv = q[0], uv = q[1];
-                                    X[0] = xv.x; X[1] = xv.y; X[2] = xv.z;
-                                    x[0] = xv.x + uv.x; x[1] = xv.y + uv.y; x[2] = xv.z + uv.z;
-                                } else {
-                                    const double* xp = sx + (n * kTileE + el) * 3;
-                                    const double* up = su + (n * kTileE + el) * 3;
-#pragma unroll
-                                    for (int d = 0; d < 3; ++d) {
-                                        X[d] = (T)xp[d];
-                                        x[d] = (T)(xp[d] + up[d]);
-                                    }
-                                }
-#pragma unroll
-                                for (int i = 0; i < 3; ++i) {
-                                    const T dn = (T)c_dN[g2][n][i];
-#pragma unroll
-                                    for (int j = 0; j < 3; ++j) {
-                                        JX2[i][j] += dn * X[j];
-                                        Jc2[i][j] += dn * x[j];
-                                    }
-                                }
-                            }
-                            V0 += (double)det3(JX2);
-                            V += (double)det3(Jc2);
-                        }
-                        const double Jbar = V / V0;
-                        nh_q1p0_update<T>(F, p, Jbar, sig, D);
-                        if (gp == 0) skd[el] = (T)(nh_q1p0_d2psi((double)p[1], Jbar) / V0);
-                    } else {
-                        status |= run_material<T, MODEL>(F, p, ebr, a.dt, io, sig, D);
-                    }
-                }
-                bool finite = true;
-#pragma unroll
-                for (int k = 0; k < 6; ++k) finite = finite && isfinite(sig[k]);
-                if (!finite) status |= 4;
-                if (a.gp_stress) {
-#pragma unroll
-                    for (int k = 0; k < 6; ++k) a.gp_stress[((size_t)k * 8 + gp) * a.n_elem + e] = sig[k];
-                }
-                const T w = (status & 5) ? T(0) : detJ;  // Gauss weight is 1 (Hexa8 full integration)
-                T* dst = sds + (size_t)gp * 7 * kTileE * 4 + el * 4;
-#pragma unroll
-                for (int q = 0; q < 5; ++q)
-                    st4<T>(dst + q * kTileE * 4, w * D[4 * q], w * D[4 * q + 1], w * D[4 * q + 2], w * D[4 * q + 3]);
-                st4<T>(dst + 5 * kTileE * 4, w * D[20], w * sig[0], w * sig[1], w * sig[2]);
-                st4<T>(dst + 6 * kTileE * 4, w * sig[3], w * sig[4], w * sig[5], w);  // w: Mean Dilatation
-                if (status) atomicOr(&sstatus[el], status);
-            }
-        }
+        if constexpr (sizeof(T) == 4) stage_local_differences(s, warp, lane);
+        phase_a<T, MODEL>(a, s, e0, warp, lane);
         cp_wait_all();    // connectivity of the next tile has landed
         __syncthreads();  // phase A results visible; x, u and state buffers are free
         if (next < n_tiles) {
-            prefetch_nodes_state(a, e0n, snode + (buf ^ 1) * NB, sx, su, sxf, srs + (buf ^ 1) * NB,
-                                 snup + (buf ^ 1) * NB, sst, t);
+            prefetch_nodes_state(a, e0n, s.node + (buf ^ 1) * NB, s.x, s.u, s.rs + (buf ^ 1) * NB,
+                                 s.nup + (buf ^ 1) * NB, s.st, t);
             cp_commit();
         }
-        if (t < kTileE) {
-            if (e0 + t < a.e_end) {
-                const int st = sstatus[t];
-                a.elem_status[e0 + t] = (uint8_t)st;
-                if (st) atomicAdd(a.status_count, 1);
-            }
-            sstatus[t] = 0;
-        }
+        tile_status(a, s, e0, t);
+        phase_b<T, MODEL, SCATTER_CSR64>(a, s, e0, warp, lane, s.node + buf * NB, s.rs + buf * NB, s.nup + buf * NB,
+                                         s.ranks + buf * NB);
+    }
+    cp_wait_all();
+}
 
-        // ---------------- phase B: thread (node b = warp, element = lane) -------------------
-        {
-            const int b = warp, el = lane, e = e0 + el;
-            if (e < a.e_end) {
-                const int npair = (b < 4) ? 4 : 3;  // off-diagonal partners a = b+1..b+npair (mod 8)
-                T f0 = 0, f1 = 0, f2 = 0;
-                T Kd[6] = {0, 0, 0, 0, 0, 0};
-                T Ko[4][9];
-                // Mean Dilatation: Bdiv of node b and of its partners, sum_gp w detJ grad N (current)
-                T bdb[3] = {T(0), T(0), T(0)}, bda[4][3] = {};
-                // FP32: the 3x3 blocks accumulate two columns per packed FMA (sm_100 FFMA2).  Row 0
-                // pairs column 2 with the geometric term g_a . sigma g_b, which enters the diagonal
-                // of the block once after the Gauss-point loop.
-                float2 Pa[4][3], Pc[4], Da = {0.f, 0.f}, Dc = {0.f, 0.f};
-                float Pr[4][2], d11 = 0.f, d12 = 0.f, d22 = 0.f;
-                if constexpr (sizeof(T) == 4) {
+// ---------------------------------------------------------------------------------------------
+// Fused schedule (CEOS_MIXED with a tangent): element tiles and CSR conversion items
+// ---------------------------------------------------------------------------------------------
+
+// Conversion item: the CSR rows of nodes [n0, n1) from their ring blocks.  The FP64 values are
+// staged in shared memory so that the K rows (contiguous from csr_rs[n0]) are written with
+// 16-byte streaming stores; the ring blocks are re-zeroed for their next occupant.
+CEOS_D void convert_rows(const ElemArgs<float>& a, int n0, int n1, double* stage, int t) {
+    const int lane = t & 31, warp = t >> 5;
+    const long long base = a.csr_rs[n0];
+    const int head = (int)(base & 1);  // stage index of K[base + p] is p + head (16-byte pairs)
+    const uint32_t mask = a.ring_mask;
+    for (int n = n0 + warp; n < n1; n += kThreads / 32) {
+        const int m = __ldg(a.nup + n);
+        const int rel = (int)(__ldg(a.csr_rs + n) - base) + head;
+        const uint32_t bb = (uint32_t)__ldg(a.rs + n);
 #pragma unroll
-                    for (int o = 0; o < 4; ++o) {
-                        Pa[o][0] = Pa[o][1] = Pa[o][2] = Pc[o] = make_float2(0.f, 0.f);
-                        Pr[o][0] = Pr[o][1] = 0.f;
-                    }
+        for (int k = 0; k < 3; ++k) {
+            const int rowoff = rel + (k == 0 ? 0 : (k == 1 ? 3 + 3 * m : 5 + 6 * m));
+            for (int j = lane; j <= m; j += 32) {
+                const float4 v = __ldcg(reinterpret_cast<const float4*>(a.kblk + (size_t)((bb + j) & mask) * 12 + 4 * k));
+                if (j == 0) {  // diagonal block: entries l = k..2 of row k
+                    double* d = stage + rowoff;
+                    if (k == 0) { d[0] = v.x; d[1] = v.y; d[2] = v.z; }
+                    else if (k == 1) { d[0] = v.y; d[1] = v.z; }
+                    else { d[0] = v.z; }
                 } else {
-#pragma unroll
-                    for (int o = 0; o < 4; ++o)
-#pragma unroll
-                        for (int k = 0; k < 9; ++k) Ko[o][k] = T(0);
-                }
-#pragma unroll 2
-                for (int gp = 0; gp < 8; ++gp) {
-                    const T* src = sds + (size_t)gp * 7 * kTileE * 4 + el * 4;
-                    T Dm[21], s0, s1, s2, s3, s4, s5, pad;
-#pragma unroll
-                    for (int q = 0; q < 5; ++q)
-                        ld4<T>(src + q * kTileE * 4, Dm[4 * q], Dm[4 * q + 1], Dm[4 * q + 2], Dm[4 * q + 3]);
-                    ld4<T>(src + 5 * kTileE * 4, Dm[20], s0, s1, s2);
-                    T wgp;
-                    ld4<T>(src + 6 * kTileE * 4, s3, s4, s5, wgp);
-                    const T* gsrc = sg + (size_t)gp * 8 * kTileE * 4 + el * 4;
-                    T gx, gy, gz;
-                    ld4<T>(gsrc + b * kTileE * 4, gx, gy, gz, pad);
-                    if constexpr (MODEL == M_NH_Q1P0) {
-                        bdb[0] += wgp * gx;
-                        bdb[1] += wgp * gy;
-                        bdb[2] += wgp * gz;
-                    }
-                    // sigma g_b: the internal force of node b and the geometric term
-                    const T q0 = s0 * gx + s3 * gy + s5 * gz;
-                    const T q1 = s3 * gx + s1 * gy + s4 * gz;
-                    const T q2 = s5 * gx + s4 * gy + s2 * gz;
-                    f0 += q0; f1 += q1; f2 += q2;
-                    // DB = D B_b (6x3), D symmetric from its upper triangle
-                    T DB[6][3];
-#pragma unroll
-                    for (int i = 0; i < 6; ++i) {
-                        const T d0 = Dm[i <= 0 ? up21(i, 0) : up21(0, i)];
-                        const T d1 = Dm[i <= 1 ? up21(i, 1) : up21(1, i)];
-                        const T d2 = Dm[i <= 2 ? up21(i, 2) : up21(2, i)];
-                        const T d3 = Dm[i <= 3 ? up21(i, 3) : up21(3, i)];
-                        const T d4 = Dm[i <= 4 ? up21(i, 4) : up21(4, i)];
-                        const T d5 = Dm[i <= 5 ? up21(i, 5) : up21(5, i)];
-                        DB[i][0] = d0 * gx + d3 * gy + d5 * gz;
-                        DB[i][1] = d1 * gy + d3 * gx + d4 * gz;
-                        DB[i][2] = d2 * gz + d4 * gy + d5 * gx;
-                    }
-                    if constexpr (sizeof(T) == 4) {
-                        float2 P[6];
-#pragma unroll
-                        for (int i = 0; i < 6; ++i) P[i] = make_float2(DB[i][0], DB[i][1]);
-                        const float2 z0 = make_float2(DB[0][2], q0), z3 = make_float2(DB[3][2], q1),
-                                     z5 = make_float2(DB[5][2], q2);
-                        {   // diagonal block (b,b), upper 6
-                            const float2 bx = make_float2(gx, gx), by = make_float2(gy, gy), bz = make_float2(gz, gz);
-                            Da = __ffma2_rn(bx, P[0], Da); Da = __ffma2_rn(by, P[3], Da); Da = __ffma2_rn(bz, P[5], Da);
-                            Dc = __ffma2_rn(bx, z0, Dc);   Dc = __ffma2_rn(by, z3, Dc);   Dc = __ffma2_rn(bz, z5, Dc);
-                            d11 += gy * P[1].y + gx * P[3].y + gz * P[4].y;
-                            d12 += gy * DB[1][2] + gx * DB[3][2] + gz * DB[4][2];
-                            d22 += gz * DB[2][2] + gy * DB[4][2] + gx * DB[5][2];
-                        }
-#pragma unroll
-                        for (int o = 0; o < 4; ++o) {
-                            if (o < npair) {
-                                const int an = (b + 1 + o) & 7;
-                                T ax, ay, az;
-                                ld4<T>(gsrc + an * kTileE * 4, ax, ay, az, pad);
-                                if constexpr (MODEL == M_NH_Q1P0) {
-                                    bda[o][0] += wgp * ax;
-                                    bda[o][1] += wgp * ay;
-                                    bda[o][2] += wgp * az;
-                                }
-                                const float2 bx = make_float2(ax, ax), by = make_float2(ay, ay), bz = make_float2(az, az);
-                                Pa[o][0] = __ffma2_rn(bx, P[0], Pa[o][0]);
-                                Pa[o][0] = __ffma2_rn(by, P[3], Pa[o][0]);
-                                Pa[o][0] = __ffma2_rn(bz, P[5], Pa[o][0]);
-                                Pc[o] = __ffma2_rn(bx, z0, Pc[o]);
-                                Pc[o] = __ffma2_rn(by, z3, Pc[o]);
-                                Pc[o] = __ffma2_rn(bz, z5, Pc[o]);
-                                Pa[o][1] = __ffma2_rn(by, P[1], Pa[o][1]);
-                                Pa[o][1] = __ffma2_rn(bx, P[3], Pa[o][1]);
-                                Pa[o][1] = __ffma2_rn(bz, P[4], Pa[o][1]);
-                                Pr[o][0] += ay * DB[1][2] + ax * DB[3][2] + az * DB[4][2];
-                                Pa[o][2] = __ffma2_rn(bz, P[2], Pa[o][2]);
-                                Pa[o][2] = __ffma2_rn(by, P[4], Pa[o][2]);
-                                Pa[o][2] = __ffma2_rn(bx, P[5], Pa[o][2]);
-                                Pr[o][1] += az * DB[2][2] + ay * DB[4][2] + ax * DB[5][2];
-                            }
-                        }
-                    } else {
-                        // diagonal block (b,b), upper 6
-                        {
-                            const T geo = gx * q0 + gy * q1 + gz * q2;
-                            Kd[0] += gx * DB[0][0] + gy * DB[3][0] + gz * DB[5][0] + geo;
-                            Kd[1] += gx * DB[0][1] + gy * DB[3][1] + gz * DB[5][1];
-                            Kd[2] += gx * DB[0][2] + gy * DB[3][2] + gz * DB[5][2];
-                            Kd[3] += gy * DB[1][1] + gx * DB[3][1] + gz * DB[4][1] + geo;
-                            Kd[4] += gy * DB[1][2] + gx * DB[3][2] + gz * DB[4][2];
-                            Kd[5] += gz * DB[2][2] + gy * DB[4][2] + gx * DB[5][2] + geo;
-                        }
-#pragma unroll
-                        for (int o = 0; o < 4; ++o) {
-                            if (o < npair) {
-                                const int an = (b + 1 + o) & 7;
-                                T ax, ay, az;
-                                ld4<T>(gsrc + an * kTileE * 4, ax, ay, az, pad);
-                                const T geo = ax * q0 + ay * q1 + az * q2;
-                                if constexpr (MODEL == M_NH_Q1P0) {
-                                    bda[o][0] += wgp * ax;
-                                    bda[o][1] += wgp * ay;
-                                    bda[o][2] += wgp * az;
-                                }
-#pragma unroll
-                                for (int l = 0; l < 3; ++l) {
-                                    Ko[o][0 * 3 + l] += ax * DB[0][l] + ay * DB[3][l] + az * DB[5][l];
-                                    Ko[o][1 * 3 + l] += ay * DB[1][l] + ax * DB[3][l] + az * DB[4][l];
-                                    Ko[o][2 * 3 + l] += az * DB[2][l] + ay * DB[4][l] + ax * DB[5][l];
-                                }
-                                Ko[o][0] += geo; Ko[o][4] += geo; Ko[o][8] += geo;
-                            }
-                        }
-                    }
-                }
-                if constexpr (sizeof(T) == 4) {  // unpack the column pairs, add the geometric terms
-                    const float gb = Dc.y;
-                    Kd[0] = Da.x + gb; Kd[1] = Da.y; Kd[2] = Dc.x;
-                    Kd[3] = d11 + gb;  Kd[4] = d12;  Kd[5] = d22 + gb;
-#pragma unroll
-                    for (int o = 0; o < 4; ++o) {
-                        const float ga = Pc[o].y;
-                        Ko[o][0] = Pa[o][0].x + ga; Ko[o][1] = Pa[o][0].y; Ko[o][2] = Pc[o].x;
-                        Ko[o][3] = Pa[o][1].x;      Ko[o][4] = Pa[o][1].y + ga; Ko[o][5] = Pr[o][0];
-                        Ko[o][6] = Pa[o][2].x;      Ko[o][7] = Pa[o][2].y; Ko[o][8] = Pr[o][1] + ga;
-                    }
-                }
-                if constexpr (MODEL == M_NH_Q1P0) {  // Bdiv^T Bdiv d2psi/dJbar2 / V0 (ModElement.f90:463-466)
-                    const T kd = isfinite(skd[el]) ? skd[el] : T(0);  // failed elements have Bdiv = 0
-                    Kd[0] += kd * bdb[0] * bdb[0];
-                    Kd[1] += kd * bdb[0] * bdb[1];
-                    Kd[2] += kd * bdb[0] * bdb[2];
-                    Kd[3] += kd * bdb[1] * bdb[1];
-                    Kd[4] += kd * bdb[1] * bdb[2];
-                    Kd[5] += kd * bdb[2] * bdb[2];
-#pragma unroll
-                    for (int o = 0; o < 4; ++o)
-                        if (o < npair)
-#pragma unroll
-                            for (int k = 0; k < 3; ++k)
-#pragma unroll
-                                for (int l = 0; l < 3; ++l) Ko[o][k * 3 + l] += kd * bda[o][k] * bdb[l];
-                }
-                // ---- scatter ----
-                const int Bn = node_c[b * kTileE + el];
-                atomicAdd(a.fint + 3 * (size_t)Bn + 0, (double)f0);
-                atomicAdd(a.fint + 3 * (size_t)Bn + 1, (double)f1);
-                atomicAdd(a.fint + 3 * (size_t)Bn + 2, (double)f2);
-                if (a.kval && !BLOCKED) {
-                    {
-                        const long long r0 = rs_c[b * kTileE + el];
-                        const int m = nup_c[b * kTileE + el];
-                        const long long r1 = r0 + 3 + 3 * m, r2 = r1 + 2 + 3 * m;
-                        double* K = a.kval;
-                        atomicAdd(K + r0 + 0, (double)Kd[0]);
-                        atomicAdd(K + r0 + 1, (double)Kd[1]);
-                        atomicAdd(K + r0 + 2, (double)Kd[2]);
-                        atomicAdd(K + r1 + 0, (double)Kd[3]);
-                        atomicAdd(K + r1 + 1, (double)Kd[4]);
-                        atomicAdd(K + r2 + 0, (double)Kd[5]);
-                    }
-                    const uint8_t* rk = reinterpret_cast<const uint8_t*>(ranks_c + el * 8);
-#pragma unroll
-                    for (int o = 0; o < 4; ++o) {
-                        if (o < npair) {
-                            const int an = (b + 1 + o) & 7;
-                            const int An = node_c[an * kTileE + el];
-                            const int lo_local = an < b ? an : b, hi_local = an < b ? b : an;
-                            const int r = rk[pair_index(lo_local, hi_local)];
-                            const bool a_low = An < Bn;  // rows belong to the smaller global node
-                            const int lo_n = a_low ? an : b;
-                            const long long r0 = rs_c[lo_n * kTileE + el];
-                            const int m = nup_c[lo_n * kTileE + el];
-                            const long long row0 = r0 + 3 + 3 * r;
-                            const long long row1 = r0 + (3 + 3 * m) + 2 + 3 * r;
-                            const long long row2 = r0 + (3 + 3 * m) + (2 + 3 * m) + 1 + 3 * r;
-                            double* K = a.kval;
-                            if (a_low) {  // (3A+k, 3B+l) += M[k][l]
-#pragma unroll
-                                for (int l = 0; l < 3; ++l) {
-                                    atomicAdd(K + row0 + l, (double)Ko[o][0 * 3 + l]);
-                                    atomicAdd(K + row1 + l, (double)Ko[o][1 * 3 + l]);
-                                    atomicAdd(K + row2 + l, (double)Ko[o][2 * 3 + l]);
-                                }
-                            } else {  // (3B+l, 3A+k) += M[k][l]
-#pragma unroll
-                                for (int k = 0; k < 3; ++k) {
-                                    atomicAdd(K + row0 + k, (double)Ko[o][k * 3 + 0]);
-                                    atomicAdd(K + row1 + k, (double)Ko[o][k * 3 + 1]);
-                                    atomicAdd(K + row2 + k, (double)Ko[o][k * 3 + 2]);
-                                }
-                            }
-                        }
-                    }
-                }
-                if (a.kval && BLOCKED) {
-                    // node-pair blocks: one 16-byte vector reduction per block row
-                    {
-                        float* blk = a.kblk + rs_c[b * kTileE + el] * 12;  // rs holds the first block of the node
-                        red_v4(blk + 0, (float)Kd[0], (float)Kd[1], (float)Kd[2], 0.f);
-                        red_v4(blk + 4, 0.f, (float)Kd[3], (float)Kd[4], 0.f);
-                        red_v4(blk + 8, 0.f, 0.f, (float)Kd[5], 0.f);
-                    }
-                    const uint8_t* rk = reinterpret_cast<const uint8_t*>(ranks_c + el * 8);
-#pragma unroll
-                    for (int o = 0; o < 4; ++o) {
-                        if (o < npair) {
-                            const int an = (b + 1 + o) & 7;
-                            const int An = node_c[an * kTileE + el];
-                            const int lo_local = an < b ? an : b, hi_local = an < b ? b : an;
-                            const int r = rk[pair_index(lo_local, hi_local)];
-                            const bool a_low = An < Bn;
-                            const int lo_n = a_low ? an : b;
-                            float* blk = a.kblk + (rs_c[lo_n * kTileE + el] + 1 + r) * 12;
-                            if (a_low) {  // rows of node a: M[k][:]
-                                red_v4(blk + 0, (float)Ko[o][0], (float)Ko[o][1], (float)Ko[o][2], 0.f);
-                                red_v4(blk + 4, (float)Ko[o][3], (float)Ko[o][4], (float)Ko[o][5], 0.f);
-                                red_v4(blk + 8, (float)Ko[o][6], (float)Ko[o][7], (float)Ko[o][8], 0.f);
-                            } else {      // rows of node b: M[:][l]
-                                red_v4(blk + 0, (float)Ko[o][0], (float)Ko[o][3], (float)Ko[o][6], 0.f);
-                                red_v4(blk + 4, (float)Ko[o][1], (float)Ko[o][4], (float)Ko[o][7], 0.f);
-                                red_v4(blk + 8, (float)Ko[o][2], (float)Ko[o][5], (float)Ko[o][8], 0.f);
-                            }
-                        }
-                    }
+                    double* d = stage + rowoff + (3 - k) + 3 * (j - 1);
+                    d[0] = v.x; d[1] = v.y; d[2] = v.z;
                 }
             }
         }
+        __syncwarp();
+        for (int q = lane; q < 3 * (m + 1); q += 32) {
+            const int j = q / 3, k = q - 3 * j;
+            __stcg(reinterpret_cast<float4*>(a.kblk + (size_t)((bb + j) & mask) * 12 + 4 * k),
+                   make_float4(0.f, 0.f, 0.f, 0.f));
+        }
+    }
+    __syncthreads();
+    const long long end = a.csr_rs[n1 - 1] + 6 + 9LL * __ldg(a.nup + n1 - 1);
+    const int L = (int)(end - base);
+    double* K = a.kval + base - head;  // 16-byte aligned: base - head is even
+    const int npairs = (L + head + 1) >> 1;
+    for (int i = t; i < npairs; i += kThreads) {
+        const int p0 = 2 * i, p1 = p0 + 1;
+        if (p0 >= head && p1 < head + L) {
+            __stcs(reinterpret_cast<double2*>(K + p0), *reinterpret_cast<const double2*>(stage + p0));
+        } else {
+            if (p0 >= head && p0 < head + L) __stcs(K + p0, stage[p0]);
+            if (p1 >= head && p1 < head + L) __stcs(K + p1, stage[p1]);
+        }
+    }
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<float> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_item[2];
+    __shared__ int s_abort;
+    const SmemLayout<float> L(a.ns_used);
+    const SmemPtrs<float> s(smem_raw, L);
+    double* stage = reinterpret_cast<double*>(smem_raw + L.g);  // g and ds are contiguous
+    const int t = threadIdx.x;
+    const int lane = t & 31, warp = t >> 5;
+    constexpr int NB = 8 * kTileE;
+
+    auto fetch = [&]() -> int {
+        const unsigned k = atomicAdd(a.ticket, 1u);
+        const long long pos = (long long)a.q_begin + k;
+        return pos < a.q_end ? __ldg(a.queue + pos) : kEndItem;
+    };
+    int slot = 0;
+    if (t == 0) {
+        s_item[0] = fetch();
+        s_abort = 0;
+    }
+    if (t < kTileE) s.status[t] = 0;
+    __syncthreads();
+    int cur = s_item[0];
+    int buf = 0;  // the connectivity and node data of `cur` (a tile) are staged in buffer buf
+    if (cur >= 0) {
+        prefetch_conn(a, cur * kTileE, s.node, s.ranks, t);
+        cp_commit();
+        cp_wait_all();
+        __syncthreads();
+        prefetch_nodes_state(a, cur * kTileE, s.node, s.x, s.u, s.rs, s.nup, s.st, t);
+        cp_commit();
+    }
+    while (cur != kEndItem) {
+        slot ^= 1;
+        if (t == 0) s_item[slot] = fetch();
+        __syncthreads();
+        const int next = s_item[slot];
+        if (cur >= 0) {
+            // ---------------- element tile ----------------
+            const int e0 = cur * kTileE;
+            const int nb = buf ^ 1;
+            cp_wait_all();
+            __syncthreads();  // node data and state of this tile are in shared memory
+            if (next >= 0) {
+                prefetch_conn(a, next * kTileE, s.node + nb * NB, s.ranks + nb * NB, t);
+                cp_commit();
+            }
+            stage_local_differences(s, warp, lane);
+            phase_a<float, MODEL>(a, s, e0, warp, lane);
+            if (warp == 0) {  // the ring slots of this tile must have been released by their last user
+                const int2 wr = __ldg(a.tile_wait + cur);
+                if (wr.y > wr.x && !warp_wait_flags(a.conv_done, wr.x, wr.y, a.epoch, lane, a.sched_err) && lane == 0)
+                    s_abort = 1;
+            }
+            cp_wait_all();    // connectivity of the next tile has landed
+            __syncthreads();  // phase A results visible; x, u and state buffers are free
+            if (s_abort) break;
+            if (next >= 0) {
+                prefetch_nodes_state(a, next * kTileE, s.node + nb * NB, s.x, s.u, s.rs + nb * NB, s.nup + nb * NB,
+                                     s.st, t);
+                cp_commit();
+            }
+            tile_status(a, s, e0, t);
+            phase_b<float, MODEL, SCATTER_RING>(a, s, e0, warp, lane, s.node + buf * NB, s.rs + buf * NB,
+                                                s.nup + buf * NB, s.ranks + buf * NB);
+            __syncthreads();
+            if (t == 0) {
+                __threadfence();
+                st_release_u32(a.tile_done + cur, a.epoch);
+            }
+            if (next >= 0) buf = nb;
+        } else {
+            // ---------------- conversion item ----------------
+            const int4 c = __ldg(a.conv + (-cur - 1));
+            if (next >= 0) {  // stage the next tile meanwhile (buffers the conversion does not use)
+                prefetch_conn(a, next * kTileE, s.node + buf * NB, s.ranks + buf * NB, t);
+                cp_commit();
+            }
+            // every tile that reduces into these rows has finished: tiles [c.z, c.w]
+            {
+                const int per = (c.w - c.z + 1 + kThreads / 32 - 1) / (kThreads / 32);
+                const int lo = c.z + warp * per, hi = min(c.w + 1, lo + per);
+                if (hi > lo && !warp_wait_flags(a.tile_done, lo, hi, a.epoch, lane, a.sched_err) && lane == 0)
+                    s_abort = 1;
+            }
+            if (next >= 0) cp_wait_all();
+            __syncthreads();
+            if (s_abort) break;
+            if (next >= 0) {
+                prefetch_nodes_state(a, next * kTileE, s.node + buf * NB, s.x, s.u, s.rs + buf * NB, s.nup + buf * NB,
+                                     s.st, t);
+                cp_commit();
+            }
+            convert_rows(a, c.x, c.y, stage, t);
+            __syncthreads();
+            if (t == 0) {
+                __threadfence();
+                st_release_u32(a.conv_done + (-cur - 1), a.epoch);
+            }
+        }
+        cur = next;
     }
     cp_wait_all();
 }

@@ -122,9 +122,10 @@ int ceos_set_state(void* handle, int which, const double* in);
 int ceos_gp_stress(void* handle, double* out);
 enum { CEOS_OPT_STORE_STRESS = 1, CEOS_OPT_TIME_KERNELS = 2 };
 int ceos_set_options(void* handle, int options);
-/* With CEOS_OPT_TIME_KERNELS set, CUDA events bracket the kernels of every evaluation; this
- * returns their device times (ms) for the last evaluation (synchronizes): ms[0] the fused element
- * loop, ms[1] the FP32-block to FP64-CSR conversion of K (0 in CEOS_FP64 mode). */
+/* With CEOS_OPT_TIME_KERNELS set, CUDA events bracket the kernel of every evaluation; this
+ * returns its device time (ms) for the last evaluation (synchronizes): ms[0] the element loop
+ * with its K assembly (one launch: in CEOS_MIXED the FP32 node-pair blocks become FP64 CSR rows
+ * inside the same launch), ms[1] = 0. */
 int ceos_kernel_time(void* handle, float* ms);
 int ceos_set_committed_time(void* handle, double t);
 
