@@ -81,6 +81,7 @@ def lib():
                                     ip, P]
         L.ceos_analysis_set_callback.argtypes = [P, STEP_CALLBACK, P]
         L.ceos_analysis_set_initial.argtypes = [P, P]
+        L.ceos_analysis_set_device_solver.argtypes = [P, I, D, I]
         _lib = L
     return _lib
 
@@ -245,11 +246,13 @@ class ElementLoop:
         return out.reshape(self.n_elem, 8, 6)
 
     def analysis(self, bc, tol, itmax, norm_mode, norm_type=2, max_cutbacks=10, probe_dofs=(), max_log=100000,
-                 on_step=None, U0=None):
+                 on_step=None, U0=None, device_solver=False, lin_tol=1e-12, lin_max_iter=20000):
         """Quasi-static analysis of one load case through ceos_analysis.  on_step(time, load_case, step,
         cutback, substep, flag_end_step, n_iterations, U) is called for every converged substep (the
         WriteFEMResults call sites); a True return stops the analysis.  U0 starts from given
-        displacements (a restart) instead of zero."""
+        displacements (a restart) instead of zero.  device_solver: the Newton iteration stays on the
+        device (boundary conditions as kernels, PCG to lin_tol) instead of the host factorization."""
+        _check(lib().ceos_analysis_set_device_solver(self._h, 1 if device_solver else 0, lin_tol, lin_max_iter))
         n_steps = len(bc["t0"])
         iters = np.zeros(n_steps, np.int32)
         cuts = np.zeros(n_steps, np.int32)

@@ -124,3 +124,43 @@ def config1_bc(X, n_steps=10, stretch=1.5, extra_rotation_constraint=True):
     presc = [3 * n + 1 for n in np.nonzero(f["x1"])[0]]
     tab = [[0.0, 0.0], [1.0, (stretch - 1.0) * L]]
     return bc_from_tables(t_init, dt, sorted(fixed), presc, [tab] * len(presc), [], [])
+
+
+def config2_bc(X, n_steps=40, dt=0.025, amplitude=0.3, freq=1.0):
+    """Config 2 BCs (project-chosen): cyclic simple shear gamma(t) = amplitude sin(2 pi freq t) of the
+    unit cube; bottom face z = 0 fixed, top face z = 1 moved by u_x = gamma(t) (times its height) with
+    u_y = u_z = 0; n_steps increments of dt, the table holding gamma at every step end."""
+    f = node_grid_index(X)
+    t_init = np.array([k * dt for k in range(n_steps)])
+    H = X[:, 2].max() - X[:, 2].min()
+    fixed = set()
+    for n in np.nonzero(f["z0"])[0]:
+        for d in range(3):
+            fixed.add(3 * n + d + 1)
+    top = np.nonzero(f["z1"])[0]
+    for n in top:
+        fixed.add(3 * n + 2)
+        fixed.add(3 * n + 3)
+    tk = np.arange(n_steps + 1) * dt
+    tab = np.stack([tk, amplitude * np.sin(2.0 * np.pi * freq * tk) * H], axis=1).tolist()
+    presc = [3 * n + 1 for n in top]
+    return bc_from_tables(t_init, np.full(n_steps, dt), sorted(fixed), presc, [tab] * len(presc), [], [])
+
+
+def config3_bc(X, n_steps=50, strain=0.05):
+    """Config 3 BCs: uniaxial tension of the plate along x to `strain` (engineering) in n_steps equal
+    increments of pseudo-time [0, 1]: face x = 0 has u_x = 0, the symmetry planes y = 0 and z = 0
+    have u_y = 0 and u_z = 0, face x = L is displaced by strain * L."""
+    f = node_grid_index(X)
+    t_init, dt = uniform_steps(0.0, 1.0, n_steps)
+    L = X[:, 0].max() - X[:, 0].min()
+    fixed = set()
+    for n in np.nonzero(f["x0"])[0]:
+        fixed.add(3 * n + 1)
+    for n in np.nonzero(f["y0"])[0]:
+        fixed.add(3 * n + 2)
+    for n in np.nonzero(f["z0"])[0]:
+        fixed.add(3 * n + 3)
+    presc = [3 * n + 1 for n in np.nonzero(f["x1"])[0]]
+    tab = [[0.0, 0.0], [1.0, strain * L]]
+    return bc_from_tables(t_init, dt, sorted(fixed), presc, [tab] * len(presc), [], [])

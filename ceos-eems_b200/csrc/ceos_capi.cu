@@ -346,7 +346,15 @@ extern "C" int ceos_create(const ceos_mesh* mesh, const ceos_material* mats, int
     {
         double tab[8][8][3];
         hexa8_dN_table(tab);
-        if (cudaMemcpyToSymbol(c_dN, tab, sizeof(tab)) != cudaSuccess) { delete h; return CEOS_E_CUDA; }
+        float tabf[8][8][3];
+        for (int g = 0; g < 8; ++g)
+            for (int n = 0; n < 8; ++n)
+                for (int i = 0; i < 3; ++i) tabf[g][n][i] = (float)tab[g][n][i];
+        if (cudaMemcpyToSymbol(c_dN, tab, sizeof(tab)) != cudaSuccess ||
+            cudaMemcpyToSymbol(c_dNf, tabf, sizeof(tabf)) != cudaSuccess) {
+            delete h;
+            return CEOS_E_CUDA;
+        }
     }
     *handle = h;
     return 0;

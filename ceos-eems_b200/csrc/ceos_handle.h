@@ -72,6 +72,9 @@ struct Handle {
     ceos_step_callback step_cb = nullptr;
     void* step_user = nullptr;
     std::vector<double> U_start;          // empty: start from U = 0
+    bool device_newton = false;           // ceos_analysis keeps K on the device and solves by PCG
+    double lin_tol = 1e-12;
+    int lin_max_iter = 20000;
 
     size_t elem_bytes() const { return precision == CEOS_FP64 ? sizeof(double) : sizeof(float); }
     size_t state_bytes() const { return (size_t)nstate * 8 * ld * elem_bytes(); }

@@ -49,6 +49,13 @@ constexpr unsigned long long kWaitNs = 200ull * 1000 * 1000;  // bound of every 
 // dN/dxi of the 8 nodes at the 8 Gauss points (ModElementHexa8.f90:211-268, points :278-329).
 // (defined once: this header is included by a single translation unit)
 __constant__ double c_dN[8][8][3];
+__constant__ float c_dNf[8][8][3];  // the same table rounded to FP32 for the mixed-precision path
+
+template <typename T>
+CEOS_D T dN_at(int gp, int n, int i) {
+    if constexpr (sizeof(T) == 4) return c_dNf[gp][n][i];
+    else return c_dN[gp][n][i];
+}
 
 template <typename T>
 struct ElemArgs {
@@ -347,7 +354,7 @@ CEOS_D void phase_a(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            const T dn = (T)c_dN[gp][n][i];
+            const T dn = dN_at<T>(gp, n, i);
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
                 JX[i][j] += dn * X[j];
@@ -376,7 +383,7 @@ CEOS_D void phase_a(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp
     // current gradients grad_x N of the 8 nodes for phase B
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
-        const T d0 = (T)c_dN[gp][n][0], d1 = (T)c_dN[gp][n][1], d2 = (T)c_dN[gp][n][2];
+        const T d0 = dN_at<T>(gp, n, 0), d1 = dN_at<T>(gp, n, 1), d2 = dN_at<T>(gp, n, 2);
         T gx[3];
 #pragma unroll
         for (int j = 0; j < 3; ++j) gx[j] = (status & 1) ? T(0) : Jci[j][0] * d0 + Jci[j][1] * d1 + Jci[j][2] * d2;
@@ -435,7 +442,7 @@ CEOS_D void phase_a(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp
                     }
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
-                        const T dn = (T)c_dN[g2][n][i];
+                        const T dn = dN_at<T>(g2, n, i);
 #pragma unroll
                         for (int j = 0; j < 3; ++j) {
                             JX2[i][j] += dn * X[j];

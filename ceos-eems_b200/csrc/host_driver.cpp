@@ -6,10 +6,12 @@
 #include <algorithm>
 #include <cmath>
 #include <deque>
+#include <memory>
 #include <vector>
 
 #include "../../include/ceos_gpu.h"
 #include "ceos_handle.h"
+#include "device_newton.h"
 
 namespace {
 
@@ -160,6 +162,15 @@ extern "C" int ceos_analysis_set_initial(void* handle, const double* U0) {
     return 0;
 }
 
+extern "C" int ceos_analysis_set_device_solver(void* handle, int on, double lin_tol, int lin_max_iter) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || (on && (!(lin_tol > 0.0) || lin_max_iter < 1))) return CEOS_E_ARG;
+    h->device_newton = on != 0;
+    h->lin_tol = lin_tol;
+    h->lin_max_iter = lin_max_iter;
+    return 0;
+}
+
 extern "C" int ceos_analysis(void* handle, int n_steps, const double* step_t0, const double* step_dt, int n_fixed,
                              const int* fixed_dofs, int n_presc, const int* presc_dofs, const double* presc_init,
                              const double* presc_final, int n_force, const int* force_dofs, const double* force_init,
@@ -187,8 +198,26 @@ extern "C" int ceos_analysis(void* handle, int n_steps, const double* step_t0, c
             if (is_fixed[r] || is_fixed[c]) zf.push_back(k);
             if (is_fixed[r] && c == r) of.push_back(k);
         }
+    // device-resident Newton (ceos_analysis_set_device_solver): the same boundary conditions as
+    // kernels, K stays on the device and a PCG replaces the host factorization
+    std::unique_ptr<ceos::DeviceNewton> dn;
     SkylineLDLT lin;
-    lin.analyse(h);
+    if (h->device_newton) {
+        std::vector<uint8_t> kind(n, 0);
+        for (int r = 0; r < n; ++r) kind[r] = (uint8_t)((is_presc[r] ? 1 : 0) | (is_fixed[r] ? 2 : 0));
+        std::vector<long long> zero_pos, one_pos;
+        for (int r = 0; r < n; ++r)
+            for (int k = rowmap[r] - 1; k < rowmap[r + 1] - 1; ++k) {
+                const int c = col[k] - 1;
+                if (!kind[r] && !kind[c]) continue;
+                (c == r ? one_pos : zero_pos).push_back(k);
+            }
+        dn.reset(new ceos::DeviceNewton());
+        rc = dn->setup(h, kind, col, zero_pos, one_pos);
+        if (rc) return rc;
+    } else {
+        lin.analyse(h);
+    }
     std::vector<double> U(n, 0.0), Uconv(n), Ubar(n), Ubar0(n), Fext(n), Fext0(n), dFext(n), dUp(n);
     if (!h->U_start.empty()) {  // restart: U of the last converged step
         if ((int)h->U_start.size() != n) return CEOS_E_ARG;
@@ -226,7 +255,34 @@ extern "C" int ceos_analysis(void* handle, int n_steps, const double* step_t0, c
             int it = 0;
             double normR0 = 0.0;
             bool converged = false;
-            while (true) {
+            if (dn) {
+                rc = dn->set_targets(Fext.data(), Ubar.data(), X.data());
+                if (rc) return rc;
+            }
+            while (dn) {
+                double normR = 0.0;
+                int st = 0;
+                rc = dn->residual(Time, it, norm_type, &normR, &st);
+                if (rc) return rc;
+                if (st) break;  // element failure: cut back
+                if (nl < max_log && norm_log) norm_log[nl] = normR;
+                ++nl;
+                if (it == 0) normR0 = normR;
+                const double thr = norm_mode == 0 ? normR0 * tol : tol;
+                if (it > 0 && normR < thr) {
+                    converged = true;
+                    rc = dn->get_X(X.data());
+                    if (rc) return rc;
+                    break;
+                }
+                if (it >= itmax) break;
+                ++it;
+                int lin_iters = 0;
+                rc = dn->solve_and_update(h->lin_tol, h->lin_max_iter, &lin_iters);
+                if (rc == CEOS_E_SOLVER) break;  // no converged correction: cut back as on a singular system
+                if (rc) return rc;
+            }
+            while (!dn) {
                 int nfail = 0;
                 const int st = ceos_evaluate(handle, Time, X.data(), fint.data(), kval.data(), &nfail);
                 if (st < 0) return st;

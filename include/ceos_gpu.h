@@ -214,9 +214,10 @@ void ceos_sur_destroy(void* handle);
 /* ---- Batched FE^2 micro problems (no reference counterpart: CEOS solves one RVE at a time,
  * MultiScale/ModMultiscaleAnalysis.f90:445-470) ------------------------------------------------
  * n_rve periodic RVEs, RVE r a unit cube of n_cells[r]^3 Hexa8 cells with one cylindrical fibre
- * along z of nominal volume fraction vf[r] (cells whose centroid lies strictly inside the fibre); both
- * phases compressible Neo-Hookean (model 7), matrix shear modulus mu_matrix, fibre modulus
- * stiff_ratio * mu_matrix, bulk modulus k_over_mu * mu in each phase. */
+ * along z of volume fraction vf[r]: each cell carries the fibre's area fraction of its cross-section
+ * (16 x 16 sub-points) and moduli mixed by it; both phases compressible Neo-Hookean (model 7),
+ * matrix shear modulus mu_matrix, fibre modulus stiff_ratio * mu_matrix, bulk modulus
+ * k_over_mu * mu in each phase. */
 int ceos_fe2_create(int n_rve, const int* n_cells, const double* vf, double mu_matrix, double stiff_ratio,
                     double k_over_mu, int device, void** handle);
 /* Mesh sizes and the discretised fibre fraction of every RVE (any pointer may be NULL). */
@@ -280,6 +281,17 @@ int ceos_analysis_set_callback(void* handle, ceos_step_callback cb, void* user);
  * ModFEMAnalysis.f90:2827-2956: U of the last converged step read back from FEMAnalysis.result);
  * U0 [n_dof] is copied, NULL clears it.  The next ceos_analysis consumes it. */
 int ceos_analysis_set_initial(void* handle, const double* U0);
+/* Device-resident Newton for the following ceos_analysis calls on this handle (on != 0): each
+ * iteration evaluates into device buffers (ceos_evaluate_device), applies the boundary conditions
+ * of ApplyBoundaryConditionsNEW (ModBoundaryConditions.f90:246-340: R -= K Ubar at the first
+ * iteration through the upper-symmetric product of :289-333, constrained rows and columns of K
+ * zeroed with a unit diagonal, :344-536) as kernels, reduces the residual norm on the device and
+ * solves K DX = -R with the device block-Jacobi PCG to the relative residual lin_tol (at most
+ * lin_max_iter iterations) in place of the PARDISO solve (ModPardisoSolver.f90:343-380).  Only
+ * the norm (8 bytes per iteration) and U at converged substeps return to the host; K never
+ * leaves the device.  A PCG that misses lin_tol counts as a failed iteration (cut back).
+ * on = 0 restores the host factorization. */
+int ceos_analysis_set_device_solver(void* handle, int on, double lin_tol, int lin_max_iter);
 
 int ceos_analysis(void* handle, int n_steps, const double* step_t0, const double* step_dt,
                   int n_fixed, const int* fixed_dofs,

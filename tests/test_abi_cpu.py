@@ -38,3 +38,17 @@ def test_bad_arguments_rejected_without_gpu():
     h = ctypes.c_void_p()
     assert lib.ceos_create(None, None, 0, 0, 0, ctypes.byref(h)) == -1
     assert lib.ceos_pattern(None, None, None, None, None, None) == -1
+
+
+def test_fortran_module_binds_exported_symbols():
+    """include/ceos_gpu_mod.f90 (the ISO_C_BINDING module a Fortran host uses) binds only symbols the
+    library exports, and its derived types match the C structs field by field."""
+    src = open(os.path.join(ROOT, "include", "ceos_gpu_mod.f90")).read()
+    names = set(re.findall(r'bind\(C,\s*name="(ceos_[a-z0-9_]+)"\)', src))
+    assert {"ceos_create", "ceos_pattern", "ceos_evaluate", "ceos_commit_state", "ceos_last_error",
+            "ceos_destroy"} <= names
+    lib = ctypes.CDLL(ceos_b200.LIBPATH)
+    assert all(hasattr(lib, n) for n in names), names
+    assert "integer(c_int) :: n_nodes, n_elem" in src and "type(c_ptr) :: X, conn, mat_id" in src
+    assert "integer(c_int) :: model, per_element, n_params" in src and "type(c_ptr) :: params" in src
+    assert max(len(ln) for ln in src.splitlines()) <= 132  # free-form source line limit
