@@ -52,15 +52,17 @@ def spatial_from_PA(F, P, A):
     return s6, np.stack(D, axis=1)
 
 
-def uniaxial_bc(X):
-    """Uniaxial stretch with symmetry planes: u_x = 0 on x = 0, u_y = 0 on y = 0, u_z = 0 on z = 0, face
-    x = 1 prescribed in x.  The planes remove the rigid modes without a point constraint (a pinned
-    corner concentrates strain in its elements).  Returns (fixed 0-based dofs, prescribed dofs)."""
+def uniaxial_bc(X, axis=0):
+    """Uniaxial stretch along `axis` with symmetry planes: u_x = 0 on x = 0, u_y = 0 on y = 0, u_z = 0
+    on z = 0, the far face normal to `axis` prescribed along it.  The planes remove the rigid modes
+    without a point constraint (a pinned corner concentrates strain in its elements).  Returns
+    (fixed 0-based dofs, prescribed dofs)."""
     f = meshgen.node_grid_index(X)
     fixed = set(3 * n for n in np.nonzero(f["x0"])[0])
     fixed.update(3 * n + 1 for n in np.nonzero(f["y0"])[0])
     fixed.update(3 * n + 2 for n in np.nonzero(f["z0"])[0])
-    presc = np.array([3 * n for n in np.nonzero(f["x1"])[0]], np.int64)
+    far = np.nonzero(f["xyz"[axis] + "1"])[0]
+    presc = np.array([3 * n + axis for n in far], np.int64)
     return np.array(sorted(fixed), np.int64), presc
 
 
@@ -73,7 +75,7 @@ class MacroFE2:
     one of its Gauss points owns an n_cells^3 periodic RVE of that fraction."""
 
     def __init__(self, nx, vf_elem, n_cells=6, surrogate=None, mu_matrix=1.0, stiff_ratio=50.0, k_over_mu=100.0,
-                 device=0):
+                 device=0, axis=0):
         self._L = _setup()
         X, conn = meshgen.structured_box(nx, nx, nx, jitter=0.0)
         self.X = X
@@ -95,7 +97,8 @@ class MacroFE2:
         self.F = torch.zeros(9 * self.n_gp, dtype=torch.float64, device=dev)
         self.vf_dev = torch.as_tensor(self.vf_elem, device=dev)
         self.flags = torch.zeros(self.n_gp, dtype=torch.int32, device=dev)
-        fixed, self.presc = uniaxial_bc(X)
+        self.axis = axis  # direction of the uniaxial stretch (the RVE fibres run along z = axis 2)
+        fixed, self.presc = uniaxial_bc(X, axis)
         mask = np.zeros(self.n_dof, np.uint8)
         mask[fixed] = 1
         mask[self.presc] = 1
@@ -223,14 +226,15 @@ class MacroFE2:
 
     # ---- Newton -------------------------------------------------------------------------------
     def predict(self, ux_target):
-        """Initial guess of a load step: the homogeneous uniaxial field u = (e x, -e y/2, -e z/2) for
-        the first step, then secant extrapolation of the last two converged fields (prescribing the
-        loaded face alone would put the whole increment into one element layer)."""
+        """Initial guess of a load step: the homogeneous uniaxial field (e along the load axis, -e/2 across
+        it) for the first step, then secant extrapolation of the last two converged fields (prescribing
+        the loaded face alone would put the whole increment into one element layer)."""
         Xd = torch.as_tensor(self.X, device=self.dev)
-        L = float(self.X[:, 0].max() - self.X[:, 0].min())
+        ax = self.axis
+        L = float(self.X[:, ax].max() - self.X[:, ax].min())
         if self._hist is None:
             e = ux_target / L
-            U = torch.stack([e * Xd[:, 0], -0.5 * e * Xd[:, 1], -0.5 * e * Xd[:, 2]], dim=1).reshape(-1)
+            U = torch.stack([(e if d == ax else -0.5 * e) * Xd[:, d] for d in range(3)], dim=1).reshape(-1)
         else:
             (u1, U1), (u0, U0) = self._hist
             U = U1 + (U1 - U0) * ((ux_target - u1) / (u1 - u0)) if u1 != u0 else U1.clone()
@@ -241,7 +245,8 @@ class MacroFE2:
     _sticky = None  # points on RVE solves in the current load step
 
     def newton_step(self, ux_target, mode, tol=1e-6, max_newton=15, pcg_tol=1e-8):
-        """One load step: x1-face displacement ux_target; returns Newton iterations."""
+        """One load step: displacement ux_target of the loaded face along the load axis; returns Newton
+        iterations."""
         self.predict(ux_target)
         self._sticky = None
         self.U[torch.as_tensor(self.presc, device=self.dev)] = ux_target
@@ -291,9 +296,9 @@ class MacroFE2:
         raise CeosError(1, f"macro Newton did not converge (residual {rn:.3e}, first {r0:.3e})")
 
     def run(self, stretch=1.2, n_steps=10, mode="surrogate", tol=1e-6, max_newton=15):
-        """Uniaxial stretch of the x1 face to `stretch` in n_steps increments.  Returns per-step wall
+        """Uniaxial stretch of the loaded face to `stretch` in n_steps increments.  Returns per-step wall
         times (s), Newton iterations and fallback points."""
-        L = self.X[:, 0].max() - self.X[:, 0].min()
+        L = self.X[:, self.axis].max() - self.X[:, self.axis].min()
         times, its, fbs = [], [], []
         for k in range(1, n_steps + 1):
             fb0 = self.stats["fallback_points"]

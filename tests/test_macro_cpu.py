@@ -56,3 +56,27 @@ def test_stress_error_measures_and_sampling():
     assert np.all((vf >= 0.1) & (vf <= 0.4))
     # the scaled half has smaller strains on average
     assert np.abs(G[:200]).mean() < np.abs(G[200:]).mean()
+
+
+def test_path_samples_follow_the_uniaxial_macro_load():
+    """The surrogate's training data covers the macro load path: stretch along the fibre axis up to
+    1.26, nearly isochoric lateral contraction, local perturbations of a few percent."""
+    from ceos_b200 import fe2_surrogate as FS
+    F, vf = FS.sample_points(1000, seed=5, path_fraction=0.5, axis=2)
+    path = F[500:]
+    lam = path[:, 2, 2]
+    assert lam.max() > 1.2 and lam.min() > 0.9
+    J = np.linalg.det(path)
+    assert np.all(np.abs(J - 1.0) < 0.25) and np.all(J > 0)
+    C33 = np.einsum("nk,nk->n", path[:, :, 2], path[:, :, 2])
+    assert C33.max() > 1.44            # the training box reaches C33 of stretch 1.2
+    cube = F[:500] - np.eye(3)
+    assert np.all(np.abs(cube) <= 0.15 + 1e-12)
+
+
+def test_uniaxial_bc_along_the_fibre_axis():
+    X, _ = meshgen.structured_box(3, 3, 3, jitter=0.0)
+    fixed, presc = uniaxial_bc(X, axis=2)
+    assert len(presc) == 16 and np.all(presc % 3 == 2)
+    assert np.all(X[presc // 3, 2] == 1.0)
+    assert len(set(fixed) & set(presc)) == 0 and len(fixed) == 3 * 16
