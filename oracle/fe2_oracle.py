@@ -108,3 +108,96 @@ class RVE:
             Pm = self.solve(np.asarray(Fbar).reshape(-1) - dF).reshape(-1)
             A[:, kL] = (Pp - Pm) / (2 * h)
         return A
+
+
+def reference_periodic_T(X, tol=1e-6):
+    """The periodic map T of the reference's BuildT (FEM/Modules/ModMultiscalePeriodicFEMSoE.f90:226-895),
+    restated: boundary nodes are classified by coordinates (tolerance 1e-6) into the minus/plus faces,
+    edges and the 8 vertices; every plus node is tied to the minus node with the same remaining
+    coordinates (T row of the plus dof = the minus node's column, its own column nulled), the 7 other
+    vertices to XmYmZm, and the nulled columns are removed (the NulCols compaction, :854-871).  Returns
+    (T [3 n_nodes x n_red] sparse, the 24 full vertex dofs that the analysis fixes, :874-897 with
+    ModFEMAnalysis.f90:1526-1535).
+
+    One branch of the reference is restated by its evident intent: for the YpZm edge (:773-783) the
+    reference zeroes only two of the node's diagonal entries and records Xp(n) instead of YpZm(n) in
+    NulCols; here the YpZm node is tied like the YmZp and YpZp edges."""
+    n = X.shape[0]
+    lo, hi = X.min(axis=0), X.max(axis=0)
+    at_lo = np.abs(X - lo) < tol
+    at_hi = np.abs(X - hi) < tol
+    on_b = at_lo | at_hi
+    minus_of = np.arange(n)                       # independent partner of every node
+    key = {}
+    for a in range(n):                            # minus-side representatives by reduced coordinates
+        if not on_b[a].any():
+            continue
+        if at_hi[a].any():
+            continue
+        key[tuple(np.round(np.where(at_lo[a], -1.0, X[a]) / tol).astype(np.int64))] = a
+    for a in range(n):
+        if not at_hi[a].any():
+            continue
+        # the partner lies on the minus side of every axis on which a lies on the plus side
+        q = np.where(at_hi[a] | at_lo[a], -1.0, X[a])
+        minus_of[a] = key[tuple(np.round(q / tol).astype(np.int64))]
+    rows, cols = [], []
+    keep = np.ones(3 * n, bool)
+    for a in range(n):
+        if minus_of[a] != a:
+            keep[3 * a:3 * a + 3] = False
+    newcol = np.cumsum(keep) - 1
+    for a in range(n):
+        m = minus_of[a]
+        for d in range(3):
+            rows.append(3 * a + d)
+            cols.append(newcol[3 * m + d])
+    T = sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(3 * n, int(keep.sum())))
+    vert = np.nonzero(on_b.all(axis=1))[0]
+    vdofs = np.array([3 * a + d for a in vert for d in range(3)])
+    return T, vdofs
+
+
+class RVEReference(RVE):
+    """One periodic RVE solved in the reference's periodic formulation: u = (Fbar - I) Y + T w with the
+    reference's T (reference_periodic_T), the vertex dofs fixed by the rows and columns of
+    ApplyBoundaryConditionsNEW (zero, unit diagonal, zero residual), the reduced system T^T K T and
+    residual T^T R of EvaluateKt (ModMultiscalePeriodicFEMSoE.f90:77-182), Taylor displacement as the
+    first iterate (ExpandFluctuation, :190-222), and HomogenizeStress.
+
+    The reference also sets FMacroFinal(3,3) = 1/(F11 F22) (MultiScale/ModMultiscaleBoundaryConditions.f90:260),
+    but no later statement reads FMacroFinal: the prescribed displacements use FMacroInitial and
+    DeltaFMacro only.  The override therefore has no effect and is not restated."""
+
+    def __init__(self, n, vf, **kw):
+        super().__init__(n, vf, **kw)
+        self.T, self.vdofs = reference_periodic_T(self.X)
+        self.n_red = self.T.shape[1]
+
+    def solve(self, Fbar, tol=1e-10, itmax=25):
+        Fbar = np.asarray(Fbar, dtype=np.float64).reshape(3, 3)
+        w = np.zeros(self.n_red)
+        aff = (self.X @ (Fbar - np.eye(3)).T).reshape(-1)
+        nfull = aff.size
+        fixed = np.zeros(nfull, bool)
+        fixed[self.vdofs] = True
+        keepm = sp.diags((~fixed).astype(float))
+        r0 = None
+        for it in range(itmax):
+            U = aff + self.T @ w
+            fint, kval, rc, _ = self.model.evaluate(0.0, U)
+            assert rc == 0
+            Rf = -fint
+            Rf[fixed] = 0.0
+            R = self.T.T @ Rf
+            nr = np.linalg.norm(R)
+            r0 = nr if r0 is None else r0
+            if nr <= tol * max(r0, 1e-300) or nr <= 1e-11 * np.linalg.norm(fint):
+                break
+            K = self._K(kval)
+            Km = (keepm @ K @ keepm + sp.diags(fixed.astype(float))).tocsr()
+            Kred = (self.T.T @ Km @ self.T).tocsc()
+            w += spla.spsolve(Kred, R)
+        self.U = U
+        self.iters = it
+        return self.model.homogenize(U)

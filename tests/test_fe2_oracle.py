@@ -39,3 +39,31 @@ def test_partial_volume_fibre_fraction():
     # an interior cell of the fibre is pure fibre, a corner cell pure matrix
     phi = F2.fibre_fraction(8, 0.4 / np.pi)
     assert phi[4, 4] == 1.0 and phi[0, 0] == 0.0
+
+
+def test_reference_periodic_map_structure():
+    """The reference's BuildT on an n^3 RVE: n^3 independent nodes (minus faces, edges, vertex and
+    interior), every plus node tied to its periodic image, the 8 vertices to one node."""
+    for n in (2, 3, 4):
+        X, conn, phi, ind = F2.rve_mesh(n, 0.2)
+        T, vdofs = F2.reference_periodic_T(X)
+        assert T.shape == (3 * X.shape[0], 3 * n ** 3)
+        assert np.all(np.asarray(T.sum(axis=1)).ravel() == 1.0)
+        assert len(vdofs) == 24
+        cols = T.tocsr().indices.reshape(-1, 3)[:, 0]
+        assert len(set(cols[vdofs[::3] // 3])) == 1          # all vertices share one column
+        # the same grouping as the project's periodic map: equal T columns <=> equal index mod n
+        same = (cols[:, None] == cols[None, :])
+        same_ind = (ind[:, None] == ind[None, :])
+        assert np.array_equal(same, same_ind)
+
+
+def test_reference_periodic_formulation_equals_project_formulation():
+    """An isochoric macro deformation (F33 = 1/(F11 F22), so the reference's F33 line is the identity)
+    with in-plane shear: the reference's T^T K T formulation with fixed vertices and the project's
+    periodic map with one fixed independent node give the same homogenized stress."""
+    Fb = np.array([[1.08, 0.05, 0.0], [0.0, 0.96, 0.0], [0.0, 0.0, 1.0 / (1.08 * 0.96)]])
+    for n, vf in ((3, 0.3), (4, 0.2)):
+        Pp = F2.RVE(n, vf).solve(Fb)
+        Pr = F2.RVEReference(n, vf).solve(Fb)
+        assert np.abs(Pr - Pp).max() <= 1e-9 * np.abs(Pp).max(), (n, np.abs(Pr - Pp).max())

@@ -108,3 +108,16 @@ def test_autotuned_launch_shape_and_graph_replay():
     P8 = b.solve(Fb)["P"]
     assert np.abs(P8 - P0).max() <= 1e-6 * np.abs(P0).max()
     b.close()
+
+
+def test_batched_rve_matches_reference_periodic_formulation():
+    """One RVE under an isochoric macro deformation (F33 = 1/(F11 F22), in-plane shear) against the
+    oracle's restatement of the reference's own periodic formulation: BuildT, fixed vertices,
+    T^T K T (ModMultiscalePeriodicFEMSoE.f90:77-182, 226-895) and HomogenizeStress.  Bar 1e-7."""
+    Fb = np.array([[1.08, 0.05, 0.0], [0.0, 0.96, 0.0], [0.0, 0.0, 1.0 / (1.08 * 0.96)]])
+    for n, vf in ((4, 0.3), (6, 0.2)):
+        b = fe2.BatchedRVE(np.array([n], np.int32), np.array([vf]))
+        P = b.solve(Fb[None])["P"][0]
+        b.close()
+        Pr = F2.RVEReference(n, vf).solve(Fb)
+        assert np.abs(P - Pr).max() <= 1e-7 * np.abs(Pr).max(), (n, np.abs(P - Pr).max())
