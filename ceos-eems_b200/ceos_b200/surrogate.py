@@ -26,6 +26,7 @@ def _setup():
     L.ceos_sur_material_device.argtypes = [P, I, P, C.c_longlong, P, P, I, C.c_longlong, P, P]
     L.ceos_sur_set_reference.argtypes = [P, D, D]
     L.ceos_sur_message.argtypes = [P, C.c_char_p, I]
+    L.ceos_sur_set_gemm.argtypes = [P, I]
     L.ceos_sur_destroy.argtypes = [P]
     L.ceos_sur_destroy.restype = None
     return L
@@ -64,6 +65,11 @@ class Surrogate:
             buf = C.create_string_buffer(256)
             self._L.ceos_sur_message(self._h, buf, 256)
             raise CeosError(rc, buf.value.decode())
+
+    def set_gemm(self, path):
+        """128-wide layer GEMMs of training: "tcgen05" (tensor cores, TMEM accumulators) or "mma"
+        (mma.sync on warps)."""
+        self._check(self._L.ceos_sur_set_gemm(self._h, {"mma": 0, "tcgen05": 1}[path]))
 
     def set_params(self, theta):
         th = np.ascontiguousarray(theta, dtype=np.float32)

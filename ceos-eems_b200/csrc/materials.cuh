@@ -340,7 +340,8 @@ CEOS_D void j2_finite_update(const T F[3][3], const T* p, const T* st, T* stn, T
     const double Jd = det3_fp64(F);
     const double lnJd = log(Jd);
     const T J = (T)Jd;
-    const T J23 = (T)exp(-2.0 / 3.0 * lnJd);
+    // J^(-2/3) from the FP64 ln J; the power itself in the element arithmetic type
+    const T J23 = texp<T>((T)(-2.0 / 3.0 * lnJd));
     const T Ie = J23 * (be[0] + be[1] + be[2]) / T(3);
     const T mub = mu * Ie;
     T s[6];
@@ -351,6 +352,7 @@ CEOS_D void j2_finite_update(const T F[3][3], const T* p, const T* st, T* stn, T
     const double alpha = st[6];
     const double fd = nsd - sqrt(2.0 / 3.0) * (sy + H * alpha);
     const bool plastic = fd > 0.0;
+    const double inv_h = 1.0 / (3.0 * (double)mub + H);
     T n[6];
     const T ns = (T)nsd;
 #pragma unroll
@@ -358,8 +360,9 @@ CEOS_D void j2_finite_update(const T F[3][3], const T* p, const T* st, T* stn, T
     double gd = 0.0;
     T snew[6];
     if (plastic) {
-        gd = 3.0 * (double)mub * fd / (3.0 * (double)mub + H);
-        stn[6] = (T)(alpha + sqrt(2.0 / 3.0) * gd / (2.0 * (double)mub));
+        // gd = 3 mub fd / (3 mub + H); the alpha increment sqrt(2/3) gd / (2 mub) = sqrt(2/3) 1.5 fd / (3 mub + H)
+        gd = 3.0 * (double)mub * fd * inv_h;
+        stn[6] = (T)(alpha + sqrt(2.0 / 3.0) * 1.5 * fd * inv_h);
     } else {
         stn[6] = (T)alpha;
     }
@@ -390,8 +393,8 @@ CEOS_D void j2_finite_update(const T F[3][3], const T* p, const T* st, T* stn, T
         for (int k = 0; k < 6; ++k) n2[k] = nm[I[k]][0] * nm[0][Jx[k]] + nm[I[k]][1] * nm[1][Jx[k]] + nm[I[k]][2] * nm[2][Jx[k]];
     }
     const T beta1 = plastic ? (T)(gd / nsd) : T(0);
-    const T b0inv = plastic ? (T)(3.0 * (double)mub / (3.0 * (double)mub + H)) : T(0);
-    const T cH = plastic ? (T)(2.0 * fd * H * nsd / ((3.0 * (double)mub + H) * (3.0 * (double)mub + H))) : T(0);
+    const T b0inv = plastic ? (T)(3.0 * (double)mub * inv_h) : T(0);
+    const T cH = plastic ? (T)(2.0 * fd * H * nsd * inv_h * inv_h) : T(0);
     const T KJ2 = K * J * J, KJ21 = K * (J * J - T(1));
     const T w1 = b0inv - beta1;
 #pragma unroll

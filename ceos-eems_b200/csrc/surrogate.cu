@@ -167,6 +167,219 @@ __global__ void __launch_bounds__(128) layer_gemm_kernel(LayerArgs A) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// The same 128-wide layer GEMMs on the 5th-generation tensor cores (tcgen05, sm_100a).
+// CTA = 128 threads, 128 samples x 128 outputs: D[n][m] = sum_k in[n][k] W[m][k] with
+//   A = in  (M = 128 samples x K = 128, K-major),  B = W (N = 128 outputs x K = 128, K-major),
+// both staged in shared memory in the canonical K-major layout without swizzle (8-row x 16-byte
+// core matrices; the two 8-element K halves of one MMA step 128 bytes apart, 8-row groups 2048
+// bytes apart), one thread issuing the 8 tcgen05.mma of K = 16 (BF16 in, FP32 accumulate in
+// tensor memory) and committing them to an mbarrier, then each warp reading its 32 TMEM lanes
+// (samples) with tcgen05.ld and running the layer's epilogue on 8 outputs at a time.
+// ---------------------------------------------------------------------------------------------
+constexpr int kUmmaRows = 128;                 // samples per CTA (M) and outputs (N)
+constexpr int kUmmaOpBytes = 128 * 128 * 2;    // one 128 x 128 BF16 operand
+constexpr unsigned long long kUmmaWaitNs = 100ull * 1000 * 1000;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: K-major, no swizzle, leading byte offset 128 (the next 8 K
+// elements), stride byte offset 2048 (the next 8 rows), descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)(128 >> 4) << 16;
+    d |= (uint64_t)(2048 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;  // base offset 0, layout type 0 (no swizzle)
+}
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, N = 128, M = 128.
+constexpr uint32_t kUmmaIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 >> 3) << 17) |
+                                ((uint32_t)(128 >> 4) << 24);
+
+__device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_addr(dst)), "l"(src),
+                 "r"(valid ? 16 : 0));
+}
+
+template <int EPI>
+__device__ __forceinline__ void layer_epilogue8(const LayerArgs& A, int n, int m0, const float* v) {
+    const size_t o = (size_t)n * kH + m0;
+    auto st_bf8 = [](__nv_bfloat16* dst, const float* x) {
+        uint4 u;
+        u.x = pack2(__float2bfloat16_rn(x[0]), __float2bfloat16_rn(x[1]));
+        u.y = pack2(__float2bfloat16_rn(x[2]), __float2bfloat16_rn(x[3]));
+        u.z = pack2(__float2bfloat16_rn(x[4]), __float2bfloat16_rn(x[5]));
+        u.w = pack2(__float2bfloat16_rn(x[6]), __float2bfloat16_rn(x[7]));
+        *reinterpret_cast<uint4*>(dst) = u;
+    };
+    auto ld8 = [](const float* src, float* x) {
+        const float4 a = *reinterpret_cast<const float4*>(src), b = *reinterpret_cast<const float4*>(src + 4);
+        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+    };
+    auto st8 = [](float* dst, const float* x) {
+        *reinterpret_cast<float4*>(dst) = make_float4(x[0], x[1], x[2], x[3]);
+        *reinterpret_cast<float4*>(dst + 4) = make_float4(x[4], x[5], x[6], x[7]);
+    };
+    float a[8], b[8];
+    if constexpr (EPI == kFwd) {
+        float z[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) z[j] = v[j] + A.bias[m0 + j];
+        st8(A.Z + o, z);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = softplus_f(z[j]);
+        st_bf8(A.outb + o, a);
+        if (A.last) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) b[j] = sigmoid_f(z[j]) * A.w5[m0 + j];
+            st_bf8(A.outb2 + o, b);
+        }
+    } else if constexpr (EPI == kBwd) {
+        float z[8];
+        ld8(A.Z + o, z);
+        st8(A.G + o, v);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = sigmoid_f(z[j]) * v[j];
+        st_bf8(A.outb + o, a);
+    } else if constexpr (EPI == kFwdT) {
+        float z[8];
+        ld8(A.Z + o, z);
+        st8(A.Zd + o, v);
+        if (A.last) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const float sg = sigmoid_f(z[j]);
+                a[j] = sg * v[j];
+                b[j] = sg * (1.f - sg) * v[j] * A.w5[m0 + j];
+            }
+            st8(A.outf + o, a);
+            st_bf8(A.outb2 + o, b);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) a[j] = sigmoid_f(z[j]) * v[j];
+            st_bf8(A.outb + o, a);
+        }
+    } else {
+        float z[8], zd[8], g[8];
+        ld8(A.Z + o, z);
+        ld8(A.Zd + o, zd);
+        ld8(A.G + o, g);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float sg = sigmoid_f(z[j]);
+            a[j] = sg * v[j] + sg * (1.f - sg) * zd[j] * g[j];
+        }
+        st_bf8(A.outb + o, a);
+    }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(128, 1) layer_umma_kernel(LayerArgs A, int* err) {
+    extern __shared__ __align__(1024) unsigned char sm_raw[];
+    unsigned char* As = sm_raw;                    // activations: [row group][k chunk][row][16 B]
+    unsigned char* Bs = sm_raw + kUmmaOpBytes;     // weights, same layout
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int n0 = blockIdx.x * kUmmaRows;
+    // stage both operands: consecutive threads fill consecutive 16-byte rows of one core matrix
+    for (int c = tid; c < 128 * 16; c += 128) {
+        const int r8 = c & 7, q = (c >> 3) & 15, g = c >> 7, r = 8 * g + r8;
+        const int off = g * 2048 + q * 128 + r8 * 16;
+        const bool valid = n0 + r < A.n;
+        cp_async16_zfill(As + off, A.in + (size_t)(valid ? n0 + r : 0) * kH + q * 8, valid);
+        cp_async16_zfill(Bs + off, A.W + (size_t)r * kH + q * 8, true);
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+    if (warp == 0) {  // 128 TMEM columns of 32-bit accumulators for the 128 outputs
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;\n" ::"r"(smem_addr(&tmem_base)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        s_fail = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(&mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // generic-proxy writes -> tensor core reads
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    if (tid == 0) {
+        const uint32_t a0 = smem_addr(As), b0 = smem_addr(Bs);
+#pragma unroll
+        for (int s = 0; s < kH / 16; ++s) {  // K = 16 per instruction: two 128-byte K chunks
+            const uint64_t ad = umma_desc(a0 + 256 * s), bd = umma_desc(b0 + 256 * s);
+            const uint32_t acc = s > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                ::"r"(tmem), "l"(ad), "l"(bd), "r"(kUmmaIdesc), "r"(acc));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                     ::"r"(smem_addr(&mbar)) : "memory");
+    }
+    // wait for the MMAs (phase 0 of the barrier), bounded
+    {
+        const unsigned long long t0 = [] { unsigned long long t; asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t)); return t; }();
+        uint32_t done = 0;
+        while (!done) {
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}\n"
+                : "=r"(done) : "r"(smem_addr(&mbar)) : "memory");
+            if (!done) {
+                unsigned long long t;
+                asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+                if (t - t0 > kUmmaWaitNs) {
+                    atomicOr(&s_fail, 1);
+                    break;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (s_fail) {
+        if (tid == 0) atomicOr(err, 1);
+    } else {
+        const int n = n0 + 32 * warp + lane;   // TMEM lane = sample row; warp w reads lanes 32w..32w+31
+#pragma unroll 1
+        for (int c = 0; c < kH / 32; ++c) {
+            uint32_t r[32];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + 32 * c;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            if (n < A.n) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float v[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) v[q] = __uint_as_float(r[8 * j + q]);
+                    layer_epilogue8<EPI>(A, n, 32 * c + 8 * j, v);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;\n" ::"r"(tmem));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Stress seed: delta_1 = sigma(z1) G_1 (FP32), g = W1^T delta_1 (FP32 master W1), residuals,
 // loss and u = dL/dg (rounded into the padded BF16 tangent input).
 // ---------------------------------------------------------------------------------------------
@@ -676,8 +889,10 @@ struct Sur {
     __nv_bfloat16** Aptr = nullptr;  // device array of the 4 a_l pointers
     double* loss = nullptr;
     int* ctr = nullptr;  // [2] Adam step, batch offset
+    int gemm_path = 0;   // 128-wide layer GEMMs: 0 mma.sync (CUDA-core warps), 1 tcgen05 (TMEM accumulators)
+    int* err = nullptr;  // set by a tensor-core GEMM whose MMA completion wait exceeded its bound
     ~Sur() {
-        void* p[] = {theta, grad, m1, m2, hp, WT, box, Wb1, Wb, WbT, X0, U0, Hb, Hd, Db, Ab, Z, Zd, G, Hd4, T, w6, Aptr, loss, ctr, Sw, s0tab};
+        void* p[] = {theta, grad, m1, m2, hp, WT, box, Wb1, Wb, WbT, X0, U0, Hb, Hd, Db, Ab, Z, Zd, G, Hd4, T, w6, Aptr, loss, ctr, Sw, s0tab, err};
         for (void* q : p)
             if (q) cudaFree(q);
         if (stream) cudaStreamDestroy(stream);
@@ -723,6 +938,15 @@ __global__ void pack_inputs_kernel(int n, const float* X, __nv_bfloat16* X0) {
     X0[i] = __float2bfloat16_rn(k < kIn ? X[(size_t)s * kIn + k] : 0.f);
 }
 
+// One 128-wide layer GEMM (K = 128) on the selected path.
+template <int EPI>
+void launch_layer(Sur* s, const LayerArgs& L, int n, cudaStream_t st) {
+    if (s->gemm_path == 1)
+        layer_umma_kernel<EPI><<<(n + kUmmaRows - 1) / kUmmaRows, 128, 2 * kUmmaOpBytes, st>>>(L, s->err);
+    else
+        layer_gemm_kernel<kH, EPI><<<(n + kTileN - 1) / kTileN, 128, 0, st>>>(L);
+}
+
 // One gradient evaluation over n <= cap samples already on the device (X [n][7], T [n][6]):
 // accumulates dL/dtheta into s->grad and the loss into s->loss.
 int grad_device(Sur* s, int n, const float* dX) {
@@ -747,7 +971,7 @@ int grad_device(Sur* s, int n, const float* dX) {
         } else {
             L.W = s->Wb + (size_t)(l - 1) * kH * kH;
             L.in = s->Hb + (l - 1) * BH;
-            layer_gemm_kernel<kH, kFwd><<<nb, 128, 0, st>>>(L);
+            launch_layer<kFwd>(s, L, n, st);
         }
     }
     // backward primal: G_{l} = W_{l+1}^T delta_{l+1}, delta_l
@@ -758,7 +982,7 @@ int grad_device(Sur* s, int n, const float* dX) {
         L.G = s->G + l * BH;
         L.outb = s->Db + l * BH;
         L.last = 0;
-        layer_gemm_kernel<kH, kBwd><<<nb, 128, 0, st>>>(L);
+        launch_layer<kBwd>(s, L, n, st);
     }
     seed_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, s->theta, s->Z, s->G, s->T, s->w6, s->Sw, 1.f / n, s->U0,
                                                  s->loss);
@@ -777,7 +1001,7 @@ int grad_device(Sur* s, int n, const float* dX) {
         } else {
             L.W = s->Wb + (size_t)(l - 1) * kH * kH;
             L.in = s->Hd + (l - 1) * BH;
-            layer_gemm_kernel<kH, kFwdT><<<nb, 128, 0, st>>>(L);
+            launch_layer<kFwdT>(s, L, n, st);
         }
     }
     // backward tangent: a_l from W_{l+1}^T a_{l+1}
@@ -789,7 +1013,7 @@ int grad_device(Sur* s, int n, const float* dX) {
         L.G = s->G + l * BH;
         L.outb = s->Ab + l * BH;
         L.last = 0;
-        layer_gemm_kernel<kH, kBwdT><<<nb, 128, 0, st>>>(L);
+        launch_layer<kBwdT>(s, L, n, st);
     }
     // weight gradients
     GradArgs G{};
@@ -857,6 +1081,16 @@ extern "C" int ceos_sur_create(int batch_max, int device, void** handle) {
     al((void**)&s->Aptr, sizeof(void*) * 4);
     al((void**)&s->loss, sizeof(double));
     al((void**)&s->ctr, sizeof(int) * 2);
+    al((void**)&s->err, sizeof(int));
+    if (ok)
+        ok = cudaFuncSetAttribute(layer_umma_kernel<kFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kUmmaOpBytes) ==
+                 cudaSuccess &&
+             cudaFuncSetAttribute(layer_umma_kernel<kBwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kUmmaOpBytes) ==
+                 cudaSuccess &&
+             cudaFuncSetAttribute(layer_umma_kernel<kFwdT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kUmmaOpBytes) ==
+                 cudaSuccess &&
+             cudaFuncSetAttribute(layer_umma_kernel<kBwdT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kUmmaOpBytes) ==
+                 cudaSuccess;
     if (ok) {
         __nv_bfloat16* ap[4] = {s->Ab, s->Ab + BH, s->Ab + 2 * BH, s->Ab + 3 * BH};
         ok = cudaMemcpy(s->Aptr, ap, sizeof(ap), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -867,6 +1101,18 @@ extern "C" int ceos_sur_create(int batch_max, int device, void** handle) {
 }
 
 extern "C" int ceos_sur_n_params(void) { return kNParams; }
+
+namespace {
+// A tensor-core layer GEMM whose MMA completion wait gave up leaves its outputs unwritten.
+int gemm_error(Sur* s) {
+    int e = 0;
+    CKS(cudaMemcpy(&e, s->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!e) return 0;
+    CKS(cudaMemset(s->err, 0, sizeof(int)));
+    s->msg = "tensor-core layer GEMM: the MMA completion wait exceeded its bound";
+    return CEOS_E_CUDA;
+}
+}  // namespace
 
 extern "C" int ceos_sur_set_params(void* handle, const float* theta) {
     Sur* s = static_cast<Sur*>(handle);
@@ -937,7 +1183,7 @@ extern "C" int ceos_sur_gradient(void* handle, int n, const float* x, const floa
     cudaFree(dX);
     if (rc) return rc;
     CKS(e);
-    return 0;
+    return gemm_error(s);
 }
 
 // Adam training on n samples (x [n][7], t [n][6], w [6], sample weights sw [n] or NULL): epochs
@@ -1022,7 +1268,15 @@ extern "C" int ceos_sur_train(void* handle, int n, const float* x, const float* 
     cudaFree(dX);
     cudaFree(dTall);
     cudaFree(dXall);
-    return rc;
+    return rc ? rc : gemm_error(s);
+}
+
+// Select the 128-wide layer GEMMs of training: 0 mma.sync, 1 tcgen05 tensor cores.
+extern "C" int ceos_sur_set_gemm(void* handle, int path) {
+    Sur* s = static_cast<Sur*>(handle);
+    if (!s || path < 0 || path > 1) return CEOS_E_ARG;
+    s->gemm_path = path;
+    return 0;
 }
 
 namespace {

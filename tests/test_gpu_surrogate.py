@@ -1,5 +1,7 @@
-"""Surrogate kernels on the GPU against the FP64 oracle: the BF16 tensor-core training gradient
-(oracle with the same BF16 rounding points: 2e-3; plain FP64: 3e-2 relative in norm), the FP32
+"""Surrogate kernels on the GPU against the FP64 oracle: the BF16 tensor-core training gradient, with
+the 128-wide layer GEMMs on tcgen05 (TMEM accumulators) and on mma.sync (oracle with the same BF16
+rounding points: 2e-3; plain FP64: 3e-2 relative in norm; 700 samples, so the last 128-sample tile
+is partial), the FP32
 inference of stress and tangent (1e-4 relative), the training-box flag, and a training run on
 an analytic energy."""
 import numpy as np
@@ -20,9 +22,11 @@ def _problem(n=700, seed=3):
     return th, x, t, w
 
 
-def test_training_gradient_matches_oracle():
+@pytest.mark.parametrize("gemm", ["mma", "tcgen05"])
+def test_training_gradient_matches_oracle(gemm):
     th, x, t, w = _problem()
     s = SG.Surrogate(batch_max=1024)
+    s.set_gemm(gemm)
     s.set_params(th)
     th32 = s.params().astype(np.float64)
     sw = np.random.default_rng(4).uniform(0.2, 3.0, len(x)).astype(np.float32)  # per-sample weights
@@ -111,3 +115,19 @@ def test_reference_state_is_stress_free_and_tangent_unchanged():
     np.testing.assert_array_equal(C_a, C_b)                           # the tangent is untouched
     assert np.abs((S_a - S_b) - S_I).max() <= 1e-4 * np.abs(S_I).max()
     s.close()
+
+
+def test_tcgen05_and_mma_gradients_agree():
+    """The two GEMM paths see the same BF16 operands and accumulate in FP32: their gradients differ only
+    by summation order and the BF16 rounding it can flip (1e-3 relative in norm)."""
+    th, x, t, w = _problem(n=1024, seed=8)
+    out = {}
+    for gemm in ("mma", "tcgen05"):
+        s = SG.Surrogate(batch_max=1024)
+        s.set_gemm(gemm)
+        s.set_params(th)
+        out[gemm] = s.gradient(x, t, w)
+        s.close()
+    (la, ga), (lb, gb) = out["mma"], out["tcgen05"]
+    assert abs(la - lb) <= 1e-5 * la
+    assert np.linalg.norm(ga - gb) <= 1e-3 * np.linalg.norm(ga)
