@@ -119,7 +119,7 @@ def reference_periodic_T(X, tol=1e-6):
     (T [3 n_nodes x n_red] sparse, the 24 full vertex dofs that the analysis fixes, :874-897 with
     ModFEMAnalysis.f90:1526-1535).
 
-    One branch of the reference is restated by its evident intent: for the YpZm edge (:773-783) the
+    One branch of the reference is restated by its evident intent: for the YpZm edge (:775-783) the
     reference zeroes only two of the node's diagonal entries and records Xp(n) instead of YpZm(n) in
     NulCols; here the YpZm node is tied like the YmZp and YpZp edges."""
     n = X.shape[0]
