@@ -819,27 +819,22 @@ CEOS_D void convert_rows(const ElemArgs<float>& a, int n0, int n1, double* stage
         const int m = __ldg(a.nup + n);
         const int rel = (int)(__ldg(a.csr_rs + n) - base) + head;
         const uint32_t bb = (uint32_t)__ldg(a.rs + n);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const int rowoff = rel + (k == 0 ? 0 : (k == 1 ? 3 + 3 * m : 5 + 6 * m));
-            for (int j = lane; j <= m; j += 32) {
-                const float4 v = __ldcg(reinterpret_cast<const float4*>(a.kblk + (size_t)((bb + j) & mask) * 12 + 4 * k));
-                if (j == 0) {  // diagonal block: entries l = k..2 of row k
-                    double* d = stage + rowoff;
-                    if (k == 0) { d[0] = v.x; d[1] = v.y; d[2] = v.z; }
-                    else if (k == 1) { d[0] = v.y; d[1] = v.z; }
-                    else { d[0] = v.z; }
-                } else {
-                    double* d = stage + rowoff + (3 - k) + 3 * (j - 1);
-                    d[0] = v.x; d[1] = v.y; d[2] = v.z;
-                }
-            }
-        }
-        __syncwarp();
+        // lane q handles block row (j = q / 3, k = q % 3): reads it, re-zeroes it, writes its FP64 values
         for (int q = lane; q < 3 * (m + 1); q += 32) {
             const int j = q / 3, k = q - 3 * j;
-            __stcg(reinterpret_cast<float4*>(a.kblk + (size_t)((bb + j) & mask) * 12 + 4 * k),
-                   make_float4(0.f, 0.f, 0.f, 0.f));
+            float4* src = reinterpret_cast<float4*>(a.kblk + (size_t)((bb + j) & mask) * 12 + 4 * k);
+            const float4 v = __ldcg(src);
+            __stcg(src, make_float4(0.f, 0.f, 0.f, 0.f));
+            const int rowoff = rel + (k == 0 ? 0 : (k == 1 ? 3 + 3 * m : 5 + 6 * m));
+            if (j == 0) {  // diagonal block: entries l = k..2 of row k
+                double* d = stage + rowoff;
+                if (k == 0) { d[0] = v.x; d[1] = v.y; d[2] = v.z; }
+                else if (k == 1) { d[0] = v.y; d[1] = v.z; }
+                else { d[0] = v.z; }
+            } else {
+                double* d = stage + rowoff + (3 - k) + 3 * (j - 1);
+                d[0] = v.x; d[1] = v.y; d[2] = v.z;
+            }
         }
     }
     __syncthreads();
@@ -870,19 +865,23 @@ __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<
     const int lane = t & 31, warp = t >> 5;
     constexpr int NB = 8 * kTileE;
 
-    auto fetch = [&]() -> int {
-        const unsigned k = atomicAdd(a.ticket, 1u);
+    auto item_at = [&](unsigned k) -> int {
         const long long pos = (long long)a.q_begin + k;
         return pos < a.q_end ? __ldg(a.queue + pos) : kEndItem;
     };
+    // Tickets run one item ahead of use: while an item is processed, the ticket after the next one is
+    // already requested, so the atomic's latency is hidden behind the work.  A CTA holds at most three
+    // tickets (current, next, requested); each waits only for earlier queue positions.
     int slot = 0;
     if (t == 0) {
-        s_item[0] = fetch();
+        s_item[0] = item_at(atomicAdd(a.ticket, 1u));
+        s_item[1] = item_at(atomicAdd(a.ticket, 1u));
         s_abort = 0;
     }
     if (t < kTileE) s.status[t] = 0;
     __syncthreads();
     int cur = s_item[0];
+    int next = s_item[1];
     int buf = 0;  // the connectivity and node data of `cur` (a tile) are staged in buffer buf
     if (cur >= 0) {
         prefetch_conn(a, cur * kTileE, s.node, s.ranks, t);
@@ -893,10 +892,8 @@ __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<
         cp_commit();
     }
     while (cur != kEndItem) {
-        slot ^= 1;
-        if (t == 0) s_item[slot] = fetch();
-        __syncthreads();
-        const int next = s_item[slot];
+        unsigned requested = 0;
+        if (t == 0) requested = atomicAdd(a.ticket, 1u);
         if (cur >= 0) {
             // ---------------- element tile ----------------
             const int e0 = cur * kTileE;
@@ -960,7 +957,11 @@ __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<
                 st_release_u32(a.conv_done + (-cur - 1), a.epoch);
             }
         }
+        if (t == 0) s_item[slot] = item_at(requested);
+        __syncthreads();
         cur = next;
+        next = s_item[slot];
+        slot ^= 1;
     }
     cp_wait_all();
 }

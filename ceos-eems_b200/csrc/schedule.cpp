@@ -9,8 +9,10 @@
 //    slots, blocks [minb(t) - R, maxb(t) - R), must have been converted: tile_wait[t] lists the items
 //    that hold them.  Occupants further back were converted before those by the same rule (the
 //    tiles that wrote the previous occupants waited for them, and the items converting the previous
-//    occupants waited for those tiles).  R is the smallest power of two for which every item a tile
-//    waits for is queued before the tile (at most the power of two >= n_blocks, which never wraps).
+//    occupants waited for those tiles).  R is a power of two for which every item a tile waits for
+//    is queued before the tile (at most the power of two >= n_blocks, which never wraps): the
+//    smallest such R0, enlarged up to 4 R0 so that those items are normally two grids of queue
+//    positions ahead of the tile.
 // Every wait of the kernel therefore targets an earlier queue position, and the earliest unfinished
 // queue entry never waits for anything unfinished: the queue always drains.
 #include "schedule.h"
@@ -114,15 +116,14 @@ int plan_schedule(int n_nodes, int n_elem, const int* conn0, const long long* rs
             out.err = "schedule: conversion item queued before its tiles";
             return CEOS_E_MESH;
         }
-    // ring size
+    // ring size: the smallest power of two R0 for which every item a tile waits for is queued before the
+    // tile; then, up to 4 R0, a larger ring that keeps those items at least two grids of queue positions
+    // ahead of the tile, so that a tile rarely waits for a conversion that has only just started
     long long span = 1LL << 16;
     for (int t = 0; t < T; ++t) span = std::max(span, tmaxb[t] - tminb[t]);
-    long long R = 1;
-    while (R < span) R <<= 1;
     long long Rmax = 1;
     while (Rmax < n_blocks) Rmax <<= 1;
-    out.tile_wait.assign(T, TileWait{0, 0});
-    for (;; R <<= 1) {
+    auto fill_waits = [&](long long R, long long dist) {
         bool ok = true;
         for (int t = 0; t < T && ok; ++t) {
             const long long hi = tmaxb[t] - R;
@@ -134,9 +135,20 @@ int plan_schedule(int n_nodes, int n_elem, const int* conn0, const long long* rs
             const int x = (int)(std::upper_bound(item_b0.begin(), item_b0.end(), lo) - item_b0.begin()) - 1;
             const int y = (int)(std::upper_bound(item_b0.begin(), item_b0.end(), hi - 1) - item_b0.begin());
             out.tile_wait[t] = TileWait{x, y};
-            for (int j = x; j < y && ok; ++j) ok = pos_item[j] < pos_tile[t];
+            for (int j = x; j < y && ok; ++j) ok = pos_item[j] + dist < pos_tile[t];
         }
-        if (ok || R >= Rmax) break;
+        return ok;
+    };
+    out.tile_wait.assign(T, TileWait{0, 0});
+    long long R0 = 1;
+    while (R0 < span) R0 <<= 1;
+    while (R0 < Rmax && !fill_waits(R0, 0)) R0 <<= 1;
+    const long long dist = 2LL * std::max(1, slack);
+    long long R = R0;
+    while (R < Rmax && R < 4 * R0 && !fill_waits(R, dist)) R <<= 1;
+    if (!fill_waits(R, 0)) {  // a larger ring is never needed for correctness; keep the minimal one then
+        R = R0;
+        fill_waits(R, 0);
     }
     out.ring_blocks = std::min(R, Rmax);
     return 0;

