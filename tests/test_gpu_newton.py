@@ -13,9 +13,11 @@ count per increment.  Checked here:
   in 50 increments): GPU counts = oracle counts per increment and final U within 1e-8 (1e-7 for J2);
   norms within 1e-6 relative above round-off over the whole visco history and over the J2 increments
   up to first yield (after it the first tangent of an increment is taken at points on their yield
-  surface, where its elastic/plastic branch depends on round-off).  FP64 element loop with the device Newton at relative 1e-8; the
-  mixed-precision loop with the device Newton at relative 1e-6 (its FP32 element forces put a
-  floor near 1e-7 under the residual) against the oracle at the same tolerance.
+  surface, where its elastic/plastic branch depends on round-off).  FP64 element loop with the
+  device Newton at relative 1e-8; the mixed-precision loop with the device Newton at relative 1e-5
+  against the oracle at the same tolerance: its FP32 element forces put a floor of a few 1e-6 of the
+  first residual under the residual (the bulk term lambda ln J with lambda = 99 mu amplifies the FP32
+  rounding of F), so 1e-6 is out of its reach.
 """
 import numpy as np
 import pytest
@@ -121,7 +123,7 @@ def test_newton_history_mixed_matches_oracle(config, nx):
     X, conn, bc, model, params, pe = (_config2 if config == "c2" else _config3)(nx)
     g = G.ElementLoop(X, conn, model, params, per_element=pe, precision=G.MIXED)
     o = O.Model(X, conn, [model], params, per_element=pe)
-    rg = g.analysis(bc, tol=1e-6, itmax=20, norm_mode=0, device_solver=True)
-    ro = o.analysis(bc, tol=1e-6, itmax=20, norm_mode=0)
+    rg = g.analysis(bc, tol=1e-5, itmax=20, norm_mode=0, device_solver=True)
+    ro = o.analysis(bc, tol=1e-5, itmax=20, norm_mode=0)
     g.close()
     _compare(rg, ro, norm_rtol=1e-4, u_tol=1e-5)
