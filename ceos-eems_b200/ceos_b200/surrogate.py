@@ -67,8 +67,8 @@ class Surrogate:
             raise CeosError(rc, buf.value.decode())
 
     def set_gemm(self, path):
-        """128-wide layer GEMMs of training: "tcgen05" (tensor cores, TMEM accumulators) or "mma"
-        (mma.sync on warps)."""
+        """128-wide layer GEMMs of training: "tcgen05" (tensor cores, TMEM accumulators; the default)
+        or "mma" (mma.sync on warps)."""
         self._check(self._L.ceos_sur_set_gemm(self._h, {"mma": 0, "tcgen05": 1}[path]))
 
     def set_params(self, theta):

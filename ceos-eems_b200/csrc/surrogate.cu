@@ -889,7 +889,7 @@ struct Sur {
     __nv_bfloat16** Aptr = nullptr;  // device array of the 4 a_l pointers
     double* loss = nullptr;
     int* ctr = nullptr;  // [2] Adam step, batch offset
-    int gemm_path = 0;   // 128-wide layer GEMMs: 0 mma.sync (CUDA-core warps), 1 tcgen05 (TMEM accumulators)
+    int gemm_path = 1;   // 128-wide layer GEMMs: 1 tcgen05 (TMEM accumulators, default), 0 mma.sync on warps
     int* err = nullptr;  // set by a tensor-core GEMM whose MMA completion wait exceeded its bound
     ~Sur() {
         void* p[] = {theta, grad, m1, m2, hp, WT, box, Wb1, Wb, WbT, X0, U0, Hb, Hd, Db, Ab, Z, Zd, G, Hd4, T, w6, Aptr, loss, ctr, Sw, s0tab, err};
@@ -1271,7 +1271,7 @@ extern "C" int ceos_sur_train(void* handle, int n, const float* x, const float* 
     return rc ? rc : gemm_error(s);
 }
 
-// Select the 128-wide layer GEMMs of training: 0 mma.sync, 1 tcgen05 tensor cores.
+// Select the 128-wide layer GEMMs of training: 1 tcgen05 tensor cores (the default), 0 mma.sync.
 extern "C" int ceos_sur_set_gemm(void* handle, int path) {
     Sur* s = static_cast<Sur*>(handle);
     if (!s || path < 0 || path > 1) return CEOS_E_ARG;

@@ -14,10 +14,11 @@ count per increment.  Checked here:
   norms within 1e-6 relative above round-off over the whole visco history and over the J2 increments
   up to first yield (after it the first tangent of an increment is taken at points on their yield
   surface, where its elastic/plastic branch depends on round-off).  FP64 element loop with the
-  device Newton at relative 1e-8; the mixed-precision loop with the device Newton at relative 1e-5
-  against the oracle at the same tolerance: its FP32 element forces put a floor of a few 1e-6 of the
-  first residual under the residual (the bulk term lambda ln J with lambda = 99 mu amplifies the FP32
-  rounding of F), so 1e-6 is out of its reach.
+  device Newton at relative 1e-8; the mixed-precision loop with the device Newton at relative 3e-5
+  against the oracle at the same tolerance: its FP32 element forces put a floor of 2e-6 (visco) to 5e-6
+  (J2) of the first residual under the residual (the bulk term lambda ln J with lambda = 99 mu
+  amplifies the FP32 rounding of F), so 1e-6 is out of its reach; at 3e-5 the floor lies 6x or more
+  below the criterion and the iterate before convergence 2.5x or more above it.
 """
 import numpy as np
 import pytest
@@ -123,7 +124,7 @@ def test_newton_history_mixed_matches_oracle(config, nx):
     X, conn, bc, model, params, pe = (_config2 if config == "c2" else _config3)(nx)
     g = G.ElementLoop(X, conn, model, params, per_element=pe, precision=G.MIXED)
     o = O.Model(X, conn, [model], params, per_element=pe)
-    rg = g.analysis(bc, tol=1e-5, itmax=20, norm_mode=0, device_solver=True)
-    ro = o.analysis(bc, tol=1e-5, itmax=20, norm_mode=0)
+    rg = g.analysis(bc, tol=3e-5, itmax=20, norm_mode=0, device_solver=True)
+    ro = o.analysis(bc, tol=3e-5, itmax=20, norm_mode=0)
     g.close()
-    _compare(rg, ro, norm_rtol=1e-4, u_tol=1e-5)
+    _compare(rg, ro, norm_rtol=1e-4, u_tol=1e-5, norm_steps=2 if config == "c3" else None)

@@ -9,8 +9,9 @@ Bars: max |GPU - oracle| / max |oracle| over every f_int and K entry; the stated
 times the error the mixed-precision path shows at this size (FP32 element arithmetic with
 element-local FP64 differences, FP64 det F / ln J / return mapping / accumulation).
 Also checked: the new state of every Gauss point against the oracle (1e-5 of each variable's
-largest magnitude; variables the model leaves at zero stay exactly zero), and for the J2 plate that
-every point is plastic in both.  Measured on a B200: J2 plate f_int 1.7e-5 (the interior forces of
+largest magnitude plus 1e-6 of the largest magnitude of any variable, which covers components that
+vanish analytically and carry FP32 round-off; variables the model leaves at zero stay exactly zero),
+and for the J2 plate that every point is plastic in both.  Measured on a B200: J2 plate f_int 1.7e-5 (the interior forces of
 the homogeneous tension cancel, so max |f_int| is a boundary force), K 1.1e-6."""
 import os
 import sys
@@ -57,7 +58,8 @@ def test_benchmark_mesh_evaluation_matches_fp64_oracle(name):
     scale = np.abs(st_o).max(axis=(0, 1))
     err = np.abs(st_g - st_o).max(axis=(0, 1))
     used = scale > 0
-    assert np.all(err[used] <= 1e-5 * scale[used]), (name, (err[used] / scale[used]).max())
+    bar = 1e-5 * scale + 1e-6 * scale.max()
+    assert np.all(err[used] <= bar[used]), (name, (err[used] / bar[used]).max())
     assert np.all(err[~used] == 0.0), name
     if name == "j2-plate":
         assert np.all(st_o[:, :, 6] > 0) and np.all(st_g[:, :, 6] > 0)  # every point plastic in both
