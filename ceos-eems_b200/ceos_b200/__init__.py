@@ -20,6 +20,7 @@ J2_SMALL, NH_Q1P0, SVK, CNH, VISCO_VAR, VISCO_PRONY, J2_FINITE = 2, 4, 5, 7, 12,
 FP64, MIXED = 0, 1
 OPT_STORE_STRESS = 1
 OPT_TIME_KERNELS = 2
+ASSEMBLY_TWO_PASS, ASSEMBLY_FUSED = 0, 1
 
 _lib = None
 
@@ -73,6 +74,7 @@ def lib():
         L.ceos_set_state.argtypes = [P, I, P]
         L.ceos_gp_stress.argtypes = [P, P]
         L.ceos_set_options.argtypes = [P, I]
+        L.ceos_set_assembly.argtypes = [P, I]
         L.ceos_set_committed_time.argtypes = [P, D]
         L.ceos_kernel_time.argtypes = [P, C.POINTER(C.c_float)]
         L.ceos_destroy.argtypes = [P]
@@ -119,6 +121,7 @@ class ElementLoop:
         self.n_dof = 3 * self.n_nodes
         self.model = model
         self.precision = precision
+        self.assembly = "two-pass"
         params = np.asarray(params, dtype=np.float64)
         if per_element:
             params = np.atleast_2d(params)
@@ -224,18 +227,29 @@ class ElementLoop:
     def store_stress(self, on=True):
         self.set_options(OPT_STORE_STRESS if on else 0)
 
+    def set_assembly(self, mode):
+        """Mixed-precision K assembly: "two-pass" (default; element loop into FP32 node-pair blocks,
+        then a conversion launch writes the FP64 CSR rows) or "fused" (one launch from a host-planned
+        queue, blocks in an L2-sized ring)."""
+        self.assembly = mode
+        _check(lib().ceos_set_assembly(self._h, {"two-pass": ASSEMBLY_TWO_PASS, "fused": ASSEMBLY_FUSED}[mode]))
+
     def launches_per_evaluation(self, tangent=True):
-        """Kernels that one device-resident evaluation launches: one (the fused element loop and CSR
-        assembly in mixed precision with a tangent, the element loop otherwise)."""
+        """Kernels that one device-resident evaluation launches: in mixed precision with a tangent two
+        (two-pass: element loop, conversion) or one (fused); the element loop otherwise."""
+        if self.precision == MIXED and tangent:
+            return 1 if self.assembly == "fused" else 2
         return 1
 
     def kernel_names(self):
         """Names of the kernels of one device-resident evaluation with a tangent."""
-        return ["element_assemble_kernel" if self.precision == MIXED else "element_loop_kernel"]
+        if self.precision != MIXED:
+            return ["element_loop_kernel"]
+        return ["element_assemble_kernel"] if self.assembly == "fused" else ["element_loop_kernel", "csr_convert_kernel"]
 
     def kernel_time_ms(self):
-        """(evaluation kernel ms, 0) of the last evaluation: the element loop with its K assembly is one
-        launch (the second entry was a separate K conversion kernel in earlier builds)."""
+        """(element loop ms, conversion ms) of the last evaluation; the conversion entry is 0 when one
+        launch does both (fused assembly) or there is no conversion (FP64)."""
         ms = (C.c_float * 2)()
         _check(lib().ceos_kernel_time(self._h, ms))
         return ms[0], ms[1]

@@ -77,10 +77,12 @@ void model_init_state(int model, double* st) {
 template <typename T>
 size_t elem_smem(const Handle* h) { return SmemLayout<T>(h->ns_used).total; }
 
-// One evaluation launch.  CEOS_MIXED with a tangent: the fused element loop + assembly over the
-// queue items of element slab `slab` (the whole queue when the host evaluates in one slab).
-// Otherwise: the element loop over elements [e0, e1) with the static tile schedule (K by FP64
-// atomics in CEOS_FP64 mode, no K without a tangent).
+// The launches of one evaluation range.  CEOS_MIXED with a tangent, two-pass assembly (default):
+// the element loop over elements [e0, e1) reducing FP32 node-pair blocks into the scratch, then
+// the conversion of the items of element slab `slab` (every item for slab -1).  Fused assembly:
+// one launch over the queue items of slab `slab` (the whole queue for slab -1).  Otherwise: the
+// element loop over [e0, e1) with the static tile schedule (K by FP64 atomics in CEOS_FP64 mode,
+// no K without a tangent).
 template <typename T, int MODEL>
 int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* dkval, cudaStream_t s, int e0, int e1,
                  int slab) {
@@ -115,6 +117,32 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
     const size_t smem = elem_smem<T>(h);
     const bool timed = (h->options & CEOS_OPT_TIME_KERNELS) && h->ev_k0;
     if constexpr (sizeof(T) == 4) {
+        if (dkval && h->assembly == CEOS_ASSEMBLY_TWO_PASS) {
+            a.e_begin = e0;
+            a.e_end = e1;
+            a.rs = h->d_blk0;
+            a.kblk = h->d_kblk;
+            a.ring_mask = h->scratch_mask;  // covers every block: no slot is shared
+            a.csr_rs = h->d_rs;
+            a.conv = static_cast<const int4*>(h->d_conv);
+            const int j0 = slab < 0 ? 0 : h->slab_conv[slab], j1 = slab < 0 ? h->n_conv : h->slab_conv[slab + 1];
+            CK(cudaFuncSetAttribute(element_loop_kernel<float, MODEL, SCATTER_RING>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            const int n_tiles = (e1 - e0 + kTileE - 1) / kTileE;
+            if (timed) CK(cudaEventRecord(h->ev_k0, s));
+            if (n_tiles > 0) {
+                element_loop_kernel<float, MODEL, SCATTER_RING><<<std::min(n_tiles, h->grid_cap), kThreads, smem, s>>>(a);
+                CK(cudaGetLastError());
+            }
+            if (timed) CK(cudaEventRecord(h->ev_k1, s));
+            if (j1 > j0) {
+                csr_convert_kernel<<<std::min(j1 - j0, h->conv_grid), kThreads, kStageRegion, s>>>(a, h->d_conv_order,
+                                                                                                 j0, j1);
+                CK(cudaGetLastError());
+            }
+            if (timed) CK(cudaEventRecord(h->ev_k2, s));
+            return 0;
+        }
         if (dkval) {
             a.e_begin = 0;
             a.e_end = h->n_elem;
@@ -189,11 +217,14 @@ int blocks_per_sm(K kernel, size_t smem) {
     return (e != cudaSuccess || per_sm < 1) ? 1 : per_sm;
 }
 
-// Resident CTAs per SM of the evaluation kernel of this handle (the fused kernel in mixed mode).
+// Resident CTAs per SM of the evaluation kernels of this handle (in mixed mode the fewer of the
+// two-pass element kernel and the fused kernel, which share one shared-memory layout).
 template <typename T, int MODEL>
 int model_blocks_per_sm(Handle* h) {
     const size_t smem = elem_smem<T>(h);
-    if constexpr (sizeof(T) == 4) return blocks_per_sm(element_assemble_kernel<MODEL>, smem);
+    if constexpr (sizeof(T) == 4)
+        return std::min(blocks_per_sm(element_assemble_kernel<MODEL>, smem),
+                        blocks_per_sm(element_loop_kernel<float, MODEL, SCATTER_RING>, smem));
     return blocks_per_sm(element_loop_kernel<T, MODEL>, smem);
 }
 
@@ -433,8 +464,8 @@ static int evaluate_prologue(Handle* h, double time, double* dfint, double* dkva
     if (dkval && h->precision == CEOS_FP64) CK(cudaMemsetAsync(dkval, 0, sizeof(double) * (size_t)h->nnz, s));
     if (dkval && h->precision == CEOS_MIXED) {
         ++h->epoch;  // the flags of this evaluation's tiles and conversion items
-        if (h->ring_dirty) {  // an aborted evaluation may have left partial sums in the ring
-            CK(cudaMemsetAsync(h->d_kblk, 0, (size_t)h->ring_blocks * 12 * sizeof(float), s));
+        if (h->ring_dirty) {  // an aborted evaluation may have left partial sums in the blocks
+            CK(cudaMemsetAsync(h->d_kblk, 0, (size_t)h->n_blocks * 12 * sizeof(float), s));
             h->ring_dirty = false;
         }
     }
@@ -445,8 +476,10 @@ static int evaluate_prologue(Handle* h, double time, double* dfint, double* dkva
 static int evaluate_range(Handle* h, double time, const double* dU, double* dfint, double* dkval, cudaStream_t s,
                           int e0, int e1, int slab) {
     const double dt = time - h->time_old;
-    return (h->precision == CEOS_FP64) ? launch_elem<double>(h, dt, dU, dfint, dkval, s, e0, e1, slab)
-                                       : launch_elem<float>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
+    const int rc = (h->precision == CEOS_FP64) ? launch_elem<double>(h, dt, dU, dfint, dkval, s, e0, e1, slab)
+                                               : launch_elem<float>(h, dt, dU, dfint, dkval, s, e0, e1, slab);
+    if (rc && dkval && h->precision == CEOS_MIXED) h->ring_dirty = true;  // blocks may be left unconverted
+    return rc;
 }
 
 int evaluate_device(Handle* h, double time, const double* dU, double* dfint, double* dkval, cudaStream_t s) {
@@ -500,7 +533,7 @@ static int ensure_copy_stream(Handle* h) {
 static int build_schedule(Handle* h) {
     SchedulePlan p;
     const int rc = plan_schedule(h->n_nodes, h->n_elem, h->conn0.data(), h->rs.data(), h->nup.data(), h->n_blocks,
-                                 h->slab_e, h->slab_node_end, kTileE, h->grid_cap, kStageDoubles, p);
+                                 h->slab_e, h->slab_node_end, kTileE, h->grid_cap, kStageDoubles, kConvNodes, p);
     if (rc) {
         h->msg = p.err;
         return rc;
@@ -523,8 +556,40 @@ static int build_schedule(Handle* h) {
     CK(cudaMalloc(&h->d_ticket, sizeof(unsigned)));
     CK(cudaMalloc(&h->d_sched_err, sizeof(int)));
     CK(cudaMemset(h->d_sched_err, 0, sizeof(int)));
-    CK(cudaMalloc(&h->d_kblk, (size_t)h->ring_blocks * 12 * sizeof(float)));
-    CK(cudaMemset(h->d_kblk, 0, (size_t)h->ring_blocks * 12 * sizeof(float)));
+    // two-pass assembly: the items of slab c are those whose last tile lies in slab c (their rows are
+    // final after slab c); listed slab by slab, in item order within a slab
+    {
+        std::vector<int> tile_slab(T, 0);
+        for (int c = 0; c < h->n_slabs; ++c)
+            for (int t = h->slab_e[c] / kTileE; t < (h->slab_e[c + 1] + kTileE - 1) / kTileE; ++t) tile_slab[t] = c;
+        std::vector<int> order;
+        order.reserve(J);
+        h->slab_conv.assign(h->n_slabs + 1, 0);
+        for (int c = 0; c < h->n_slabs; ++c) {
+            h->slab_conv[c] = (int)order.size();
+            for (int j = 0; j < (int)J; ++j)
+                if (tile_slab[p.conv[j].t1] == c) order.push_back(j);
+        }
+        h->slab_conv[h->n_slabs] = (int)order.size();
+        if (order.size() != J) {
+            h->msg = "schedule: conversion items not assigned to slabs";
+            return CEOS_E_MESH;
+        }
+        CK(cudaMalloc(&h->d_conv_order, J * sizeof(int)));
+        CK(cudaMemcpy(h->d_conv_order, order.data(), J * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    uint32_t pow2 = 1;
+    while ((long long)pow2 < h->n_blocks) pow2 <<= 1;
+    h->scratch_mask = pow2 - 1;
+    // every block has a slot of its own (two-pass); the fused ring uses slots [0, ring_blocks), and
+    // when ring_blocks exceeds n_blocks its slot index is the block index itself
+    CK(cudaMalloc(&h->d_kblk, (size_t)h->n_blocks * 12 * sizeof(float)));
+    CK(cudaMemset(h->d_kblk, 0, (size_t)h->n_blocks * 12 * sizeof(float)));
+    int per_sm = 1, sms = 148;
+    CK(cudaFuncSetAttribute(csr_convert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageRegion));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csr_convert_kernel, kThreads, kStageRegion));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    h->conv_grid = sms * std::max(1, per_sm);
     return 0;
 }
 }  // namespace ceos
@@ -803,6 +868,13 @@ extern "C" int ceos_set_options(void* handle, int options) {
     return 0;
 }
 
+extern "C" int ceos_set_assembly(void* handle, int mode) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || (mode != CEOS_ASSEMBLY_TWO_PASS && mode != CEOS_ASSEMBLY_FUSED)) return CEOS_E_ARG;
+    h->assembly = mode;  // both leave every block they use at zero after an evaluation
+    return 0;
+}
+
 extern "C" int ceos_kernel_time(void* handle, float* ms) {
     Handle* h = static_cast<Handle*>(handle);
     if (!h || !ms || !h->ev_k0) return CEOS_E_ARG;
@@ -943,7 +1015,7 @@ Handle::~Handle() {
     if (stream) cudaStreamSynchronize(stream);
     void* ptrs[] = {d_X, d_U, d_fint, d_kval, d_conn, d_rs, d_blk0, d_nup, d_ranks, d_elem_status, d_status_count,
                     d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress, d_kblk, d_queue, d_conv,
-                    d_tile_wait, d_flags, d_ticket, d_sched_err};
+                    d_tile_wait, d_flags, d_ticket, d_sched_err, d_conv_order};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (ev_k0) cudaEventDestroy(ev_k0);

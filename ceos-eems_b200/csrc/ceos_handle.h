@@ -38,8 +38,15 @@ struct Handle {
     int* d_mat_id = nullptr;
     void* d_state[2] = {nullptr, nullptr};
     void* d_gp_stress = nullptr;
-    float* d_kblk = nullptr;              // mixed mode: ring of FP32 node-pair blocks (ring_blocks of them)
+    float* d_kblk = nullptr;              // mixed mode: FP32 node-pair blocks, n_blocks of them (the fused
+                                          // assembly uses the first ring_blocks as its ring)
     long long n_blocks = 0;
+    int assembly = CEOS_ASSEMBLY_TWO_PASS;  // mixed mode with a tangent: two-pass or fused assembly
+    uint32_t scratch_mask = 0;            // two-pass: power of two minus one, >= every block index
+    std::vector<int> slab_conv;           // [n_slabs + 1] two-pass: conversion items of slab c are
+                                          // d_conv_order[slab_conv[c] .. slab_conv[c + 1])
+    int* d_conv_order = nullptr;
+    int conv_grid = 148;                  // CTAs of a conversion launch
     // fused assembly schedule (mixed mode with a tangent): a queue of element tiles and CSR
     // conversion items, split at the element slabs of the host-buffer evaluation
     std::vector<int> queue;               // >= 0 tile, < 0 conversion item -(j+1)

@@ -20,10 +20,13 @@
 // Warp-uniform roles (gp or b is the warp index) keep control flow convergent; the shared
 // layouts put the element index innermost so every shared access is conflict-free.
 //
-// Two kernels use these phases:
-//   element_loop_kernel<T, MODEL>: static tile schedule; K by FP64 atomics straight into the
-//     CSR values (CEOS_FP64), or no K (an evaluation without tangent);
-//   element_assemble_kernel<MODEL>: CEOS_MIXED with a tangent.  K accumulates in FP32 node-pair
+// Kernels using these phases:
+//   element_loop_kernel<T, MODEL, SCATTER>: static tile schedule.  SCATTER_CSR64: K by FP64
+//     atomics straight into the CSR values (CEOS_FP64), or no K (an evaluation without tangent).
+//     SCATTER_RING (CEOS_MIXED with a tangent, two-pass assembly): K by 16-byte FP32 vector
+//     reductions into node-pair blocks (3 rows x 4 floats per node pair) in a scratch array that
+//     holds every block; csr_convert_kernel then turns finished blocks into the FP64 CSR rows.
+//   element_assemble_kernel<MODEL>: CEOS_MIXED with a tangent, fused assembly.  K accumulates in FP32 node-pair
 //     blocks (3 rows x 4 floats per node pair) by 16-byte vector reductions, and the same launch
 //     turns finished blocks into the FP64 CSR rows.  The blocks live in a ring of 2^k blocks
 //     (block b in slot b & mask) sized to stay in L2, so the FP32 accumulation never travels to
@@ -84,9 +87,9 @@ struct ElemArgs {
     uint8_t* elem_status;   // [n_elem]
     int* status_count;      // failed elements
     T* gp_stress;           // [6][8][n_elem] or nullptr
-    // ---- fused assembly (element_assemble_kernel) ----
-    float* kblk;            // ring of FP32 node-pair blocks, 12 floats each, zero between evaluations
-    uint32_t ring_mask;     // block b lives in slot b & ring_mask
+    // ---- mixed-precision K assembly (two-pass element pass and conversion; fused kernel) ----
+    float* kblk;            // FP32 node-pair blocks, 12 floats each, zero between evaluations
+    uint32_t ring_mask;     // block b lives in slot b & ring_mask (two-pass: every block its own slot)
     const long long* csr_rs;   // [n_nodes] CSR position of row 3n (0-based)
     const int* queue;       // work items: >= 0 element tile, < 0 conversion item -(j+1)
     int q_begin, q_end;     // this launch's part of the queue
@@ -128,8 +131,12 @@ struct SmemLayout {
     }
 };
 // The conversion of a run of CSR rows stages its FP64 values in the g and ds regions (unused
-// between tiles), so an item holds at most this many K values.
-constexpr int kStageDoubles = (int)((sizeof(float) * 8 * 8 * kTileE * 4 + sizeof(float) * 8 * 7 * kTileE * 4) / 8) - 2;
+// between tiles), followed by a table of its nodes (first block, first K value, upper neighbours),
+// so an item holds at most kConvNodes nodes and kStageDoubles K values.
+constexpr int kConvNodes = 256;
+constexpr int kStageRegion = (int)(sizeof(float) * 8 * 8 * kTileE * 4 + sizeof(float) * 8 * 7 * kTileE * 4);
+constexpr int kStageDoubles = (kStageRegion - 3 * kConvNodes * (int)sizeof(int)) / 8 - 2;
+static_assert((kStageDoubles + 2) * 8 + 3 * kConvNodes * (int)sizeof(int) <= kStageRegion, "conversion staging");
 
 template <typename T>
 struct SmemPtrs {
@@ -753,9 +760,10 @@ CEOS_D void phase_b(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp
 }
 
 // ---------------------------------------------------------------------------------------------
-// Static schedule: FP64 mode (K by FP64 atomics) and evaluations without a tangent
+// Static schedule: FP64 mode (K by FP64 atomics), evaluations without a tangent, and the element
+// pass of the two-pass mixed-precision assembly (K blocks into the scratch, SCATTER_RING)
 // ---------------------------------------------------------------------------------------------
-template <typename T, int MODEL>
+template <typename T, int MODEL, int SCATTER = SCATTER_CSR64>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop_kernel(ElemArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SmemLayout<T> L(a.ns_used);
@@ -797,8 +805,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
             cp_commit();
         }
         tile_status(a, s, e0, t);
-        phase_b<T, MODEL, SCATTER_CSR64>(a, s, e0, warp, lane, s.node + buf * NB, s.rs + buf * NB, s.nup + buf * NB,
-                                         s.ranks + buf * NB);
+        phase_b<T, MODEL, SCATTER>(a, s, e0, warp, lane, s.node + buf * NB, s.rs + buf * NB, s.nup + buf * NB,
+                                   s.ranks + buf * NB);
     }
     cp_wait_all();
 }
@@ -807,39 +815,72 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
 // Fused schedule (CEOS_MIXED with a tangent): element tiles and CSR conversion items
 // ---------------------------------------------------------------------------------------------
 
-// Conversion item: the CSR rows of nodes [n0, n1) from their ring blocks.  The FP64 values are
-// staged in shared memory so that the K rows (contiguous from csr_rs[n0]) are written with
-// 16-byte streaming stores; the ring blocks are re-zeroed for their next occupant.
-CEOS_D void convert_rows(const ElemArgs<float>& a, int n0, int n1, double* stage, int t) {
-    const int lane = t & 31, warp = t >> 5;
-    const long long base = a.csr_rs[n0];
+// Conversion item: the CSR rows of nodes [n0, n1) (at most kConvNodes) from their ring blocks.
+// The blocks of consecutive nodes are consecutive, [blk0[n0], blk0[n1-1] + 1 + nup[n1-1]), and so
+// are their K values, from csr_rs[n0].  A table of the item's nodes is read first (one load per
+// node); then every thread takes whole blocks and issues the loads of all three rows of its blocks
+// before it uses any, so that an item costs a few memory latencies rather than one per node.  The
+// FP64 values are staged in shared memory and the K run is written with 16-byte streaming stores;
+// the ring blocks are re-zeroed for their next occupant.
+template <int kU>  // blocks in flight per thread
+CEOS_D void convert_rows(const ElemArgs<float>& a, int n0, int n1, double* stage, int* info, int t) {
+    int* fb = info;                   // first block of the node, relative to the item's first block
+    int* fk = info + kConvNodes;      // stage index of the node's first K value
+    int* fm = info + 2 * kConvNodes;  // upper neighbours of the node
+    const long long base = __ldg(a.csr_rs + n0);
     const int head = (int)(base & 1);  // stage index of K[base + p] is p + head (16-byte pairs)
+    const uint32_t b0 = (uint32_t)__ldg(a.rs + n0);
+    const int nn = n1 - n0;
+    for (int i = t; i < nn; i += kThreads) {
+        fb[i] = (int)((uint32_t)__ldg(a.rs + n0 + i) - b0);
+        fk[i] = (int)(__ldg(a.csr_rs + n0 + i) - base) + head;
+        fm[i] = __ldg(a.nup + n0 + i);
+    }
+    __syncthreads();
+    const int nblk = fb[nn - 1] + 1 + fm[nn - 1];
     const uint32_t mask = a.ring_mask;
-    for (int n = n0 + warp; n < n1; n += kThreads / 32) {
-        const int m = __ldg(a.nup + n);
-        const int rel = (int)(__ldg(a.csr_rs + n) - base) + head;
-        const uint32_t bb = (uint32_t)__ldg(a.rs + n);
-        // lane q handles block row (j = q / 3, k = q % 3): reads it, re-zeroes it, writes its FP64 values
-        for (int q = lane; q < 3 * (m + 1); q += 32) {
-            const int j = q / 3, k = q - 3 * j;
-            float4* src = reinterpret_cast<float4*>(a.kblk + (size_t)((bb + j) & mask) * 12 + 4 * k);
-            const float4 v = __ldcg(src);
-            __stcg(src, make_float4(0.f, 0.f, 0.f, 0.f));
-            const int rowoff = rel + (k == 0 ? 0 : (k == 1 ? 3 + 3 * m : 5 + 6 * m));
+    for (int q0 = t; q0 < nblk; q0 += kU * kThreads) {
+        float4 v[kU][3];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int q = q0 + u * kThreads;
+            if (q < nblk) {
+                const float4* src = reinterpret_cast<const float4*>(a.kblk + (size_t)((b0 + (uint32_t)q) & mask) * 12);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) v[u][k] = __ldcg(src + k);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int q = q0 + u * kThreads;
+            if (q >= nblk) continue;
+            float4* src = reinterpret_cast<float4*>(a.kblk + (size_t)((b0 + (uint32_t)q) & mask) * 12);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) __stcg(src + k, make_float4(0.f, 0.f, 0.f, 0.f));
+            int lo = 0, hi = nn - 1;  // the node of block q: the last i with fb[i] <= q
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (fb[mid] <= q) lo = mid;
+                else hi = mid - 1;
+            }
+            const int j = q - fb[lo], m = fm[lo], rel = fk[lo];
+            const int r1 = rel + 3 + 3 * m, r2 = r1 + 2 + 3 * m;  // rows 3n+1 and 3n+2
             if (j == 0) {  // diagonal block: entries l = k..2 of row k
-                double* d = stage + rowoff;
-                if (k == 0) { d[0] = v.x; d[1] = v.y; d[2] = v.z; }
-                else if (k == 1) { d[0] = v.y; d[1] = v.z; }
-                else { d[0] = v.z; }
+                stage[rel] = v[u][0].x; stage[rel + 1] = v[u][0].y; stage[rel + 2] = v[u][0].z;
+                stage[r1] = v[u][1].y; stage[r1 + 1] = v[u][1].z;
+                stage[r2] = v[u][2].z;
             } else {
-                double* d = stage + rowoff + (3 - k) + 3 * (j - 1);
-                d[0] = v.x; d[1] = v.y; d[2] = v.z;
+                double* d0 = stage + rel + 3 + 3 * (j - 1);
+                double* d1 = stage + r1 + 2 + 3 * (j - 1);
+                double* d2 = stage + r2 + 1 + 3 * (j - 1);
+                d0[0] = v[u][0].x; d0[1] = v[u][0].y; d0[2] = v[u][0].z;
+                d1[0] = v[u][1].x; d1[1] = v[u][1].y; d1[2] = v[u][1].z;
+                d2[0] = v[u][2].x; d2[1] = v[u][2].y; d2[2] = v[u][2].z;
             }
         }
     }
     __syncthreads();
-    const long long end = a.csr_rs[n1 - 1] + 6 + 9LL * __ldg(a.nup + n1 - 1);
-    const int L = (int)(end - base);
+    const int L = fk[nn - 1] - head + 6 + 9 * fm[nn - 1];
     double* K = a.kval + base - head;  // 16-byte aligned: base - head is even
     const int npairs = (L + head + 1) >> 1;
     for (int i = t; i < npairs; i += kThreads) {
@@ -853,6 +894,21 @@ CEOS_D void convert_rows(const ElemArgs<float>& a, int n0, int n1, double* stage
     }
 }
 
+// Conversion pass of the two-pass assembly: CTA k converts the items order[j0 + k], order[j0 + k +
+// gridDim.x], ... < j1 (conversion items of one element slab, or all of them).  The element pass
+// before it in stream order has completed every reduction into their blocks.  Dynamic shared
+// memory: kStageRegion bytes (the staging of one item and its node table).
+__global__ void __launch_bounds__(kThreads) csr_convert_kernel(ElemArgs<float> a, const int* order, int j0, int j1) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* stage = reinterpret_cast<double*>(smem_raw);
+    int* info = reinterpret_cast<int*>(stage + kStageDoubles + 2);
+    for (int j = j0 + (int)blockIdx.x; j < j1; j += (int)gridDim.x) {
+        const int4 c = __ldg(a.conv + __ldg(order + j));
+        convert_rows<2>(a, c.x, c.y, stage, info, (int)threadIdx.x);
+        __syncthreads();  // the staging is read out before the next item writes it
+    }
+}
+
 template <int MODEL>
 __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<float> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -861,6 +917,7 @@ __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<
     const SmemLayout<float> L(a.ns_used);
     const SmemPtrs<float> s(smem_raw, L);
     double* stage = reinterpret_cast<double*>(smem_raw + L.g);  // g and ds are contiguous
+    int* conv_info = reinterpret_cast<int*>(stage + kStageDoubles + 2);
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     constexpr int NB = 8 * kTileE;
@@ -950,7 +1007,7 @@ __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<
                                      s.st, t);
                 cp_commit();
             }
-            convert_rows(a, c.x, c.y, stage, t);
+            convert_rows<1>(a, c.x, c.y, stage, conv_info, t);  // one block in flight: no spills here
             __syncthreads();
             if (t == 0) {
                 __threadfence();

@@ -1,8 +1,8 @@
 // schedule.cpp -- work queue of the fused element loop + CSR assembly (see schedule.h).
 //
 //  - Tiles: tile t = elements [t*tile_elems, (t+1)*tile_elems).
-//  - Conversion items: runs of consecutive nodes whose CSR rows hold at most stage_max - 1 values,
-//    cut at the node prefixes the host-buffer slabs finish.  Item j waits for the tiles [t0, t1]
+//  - Conversion items: runs of at most max_nodes consecutive nodes whose CSR rows hold at most
+//    stage_max - 1 values, cut at the node prefixes the host-buffer slabs finish.  Item j waits for the tiles [t0, t1]
 //    that contain its nodes, and is queued `slack` tiles after t1 (so those tiles are normally
 //    done when it starts) but never after the end of t1's slab.
 //  - Ring: block b occupies slot b & (R - 1).  Before tile t reduces, the previous occupants of its
@@ -25,10 +25,11 @@ namespace ceos {
 
 int plan_schedule(int n_nodes, int n_elem, const int* conn0, const long long* rs, const int* nup, long long n_blocks,
                   const std::vector<int>& slab_e, const std::vector<int>& slab_node_end, int tile_elems, int slack,
-                  long long stage_max, SchedulePlan& out) {
+                  long long stage_max, int max_nodes, SchedulePlan& out) {
     const int E = n_elem, N = n_nodes;
     const int n_slabs = (int)slab_node_end.size();
-    if (E < 1 || N < 1 || tile_elems < 1 || (int)slab_e.size() != n_slabs + 1 || slab_e[n_slabs] != E) {
+    if (E < 1 || N < 1 || tile_elems < 1 || max_nodes < 1 || (int)slab_e.size() != n_slabs + 1 ||
+        slab_e[n_slabs] != E) {
         out.err = "schedule: bad arguments";
         return CEOS_E_ARG;
     }
@@ -77,7 +78,7 @@ int plan_schedule(int n_nodes, int n_elem, const int* conn0, const long long* rs
                 out.err = "schedule: the CSR rows of node " + std::to_string(n + 1) + " exceed the staging buffer";
                 return CEOS_E_MESH;
             }
-            if (n > n0 && (cut[n] || len + ln > stage_max - 1)) {
+            if (n > n0 && (cut[n] || len + ln > stage_max - 1 || n - n0 >= max_nodes)) {
                 push(n0, n);
                 n0 = n;
                 len = 0;
@@ -162,11 +163,12 @@ int plan_schedule(int n_nodes, int n_elem, const int* conn0, const long long* rs
 // slab_q [n_slabs + 1]; counts [n_queue, n_conv, n_tiles].
 extern "C" int ceos_test_plan_schedule(int n_nodes, int n_elem, const int* conn0, const long long* rs, const int* nup,
                                        long long n_blocks, int n_slabs, const int* slab_e, const int* slab_node_end,
-                                       int tile_elems, int slack, long long stage_max, int* queue, int* conv,
-                                       int* wait, int* slab_q, int* counts, long long* ring_blocks) {
+                                       int tile_elems, int slack, long long stage_max, int max_nodes, int* queue,
+                                       int* conv, int* wait, int* slab_q, int* counts, long long* ring_blocks) {
     ceos::SchedulePlan p;
     std::vector<int> se(slab_e, slab_e + n_slabs + 1), sn(slab_node_end, slab_node_end + n_slabs);
-    const int rc = ceos::plan_schedule(n_nodes, n_elem, conn0, rs, nup, n_blocks, se, sn, tile_elems, slack, stage_max, p);
+    const int rc = ceos::plan_schedule(n_nodes, n_elem, conn0, rs, nup, n_blocks, se, sn, tile_elems, slack, stage_max, max_nodes,
+                                        p);
     if (rc) return rc;
     std::copy(p.queue.begin(), p.queue.end(), queue);
     for (size_t j = 0; j < p.conv.size(); ++j) {

@@ -31,10 +31,10 @@ struct SchedulePlan {
 // Tiles are tile_elems consecutive elements.  Node n owns the node-pair blocks
 // [bb(n), bb(n) + 1 + nup[n]) with bb(n) = n + (rs[n] - 6n)/9 (rs[n]: CSR position of row 3n).
 // slab_e [n_slabs + 1] are element boundaries (multiples of tile_elems, last = n_elem); after slab
-// c the rows of nodes [0, slab_node_end[c]) are final.  An item holds at most stage_max K values.
-// Returns 0 or a negative code with out.err set.
+// c the rows of nodes [0, slab_node_end[c]) are final.  An item holds at most stage_max - 1 K values
+// and at most max_nodes nodes.  Returns 0 or a negative code with out.err set.
 int plan_schedule(int n_nodes, int n_elem, const int* conn0, const long long* rs, const int* nup, long long n_blocks,
                   const std::vector<int>& slab_e, const std::vector<int>& slab_node_end, int tile_elems, int slack,
-                  long long stage_max, SchedulePlan& out);
+                  long long stage_max, int max_nodes, SchedulePlan& out);
 
 }  // namespace ceos

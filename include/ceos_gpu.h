@@ -122,11 +122,17 @@ int ceos_set_state(void* handle, int which, const double* in);
 int ceos_gp_stress(void* handle, double* out);
 enum { CEOS_OPT_STORE_STRESS = 1, CEOS_OPT_TIME_KERNELS = 2 };
 int ceos_set_options(void* handle, int options);
-/* With CEOS_OPT_TIME_KERNELS set, CUDA events bracket the kernel of every evaluation; this
- * returns its device time (ms) for the last evaluation (synchronizes): ms[0] the element loop
- * with its K assembly (one launch: in CEOS_MIXED the FP32 node-pair blocks become FP64 CSR rows
- * inside the same launch), ms[1] = 0. */
+/* With CEOS_OPT_TIME_KERNELS set, CUDA events bracket the kernels of every evaluation; this
+ * returns their device time (ms) for the last evaluation (synchronizes): ms[0] the element loop,
+ * ms[1] the conversion of the FP32 node-pair blocks into the FP64 CSR rows (CEOS_MIXED two-pass
+ * assembly; 0 when one launch does both or there is no conversion). */
 int ceos_kernel_time(void* handle, float* ms);
+/* CEOS_MIXED K assembly: CEOS_ASSEMBLY_TWO_PASS (default) runs the element loop, reducing FP32
+ * node-pair blocks into a scratch array that holds all of them, then a conversion launch writes
+ * the FP64 CSR rows; CEOS_ASSEMBLY_FUSED runs both in one launch from a host-planned queue, with
+ * the blocks in a ring sized for L2.  Both give the same K up to the FP32 summation order. */
+enum { CEOS_ASSEMBLY_TWO_PASS = 0, CEOS_ASSEMBLY_FUSED = 1 };
+int ceos_set_assembly(void* handle, int mode);
 int ceos_set_committed_time(void* handle, double t);
 
 /* Release every device buffer and the stream. */

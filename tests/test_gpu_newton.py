@@ -14,11 +14,15 @@ count per increment.  Checked here:
   norms within 1e-6 relative above round-off over the whole visco history and over the J2 increments
   up to first yield (after it the first tangent of an increment is taken at points on their yield
   surface, where its elastic/plastic branch depends on round-off).  FP64 element loop with the
-  device Newton at relative 1e-8; the mixed-precision loop with the device Newton at relative 3e-5
-  against the oracle at the same tolerance: its FP32 element forces put a floor of 2e-6 (visco) to 5e-6
-  (J2) of the first residual under the residual (the bulk term lambda ln J with lambda = 99 mu
-  amplifies the FP32 rounding of F), so 1e-6 is out of its reach; at 3e-5 the floor lies 6x or more
-  below the criterion and the iterate before convergence 2.5x or more above it.
+  device Newton at relative 1e-8.  The mixed-precision loop with the device Newton runs against the
+  oracle under the reference's absolute criterion (norm_mode 1): its FP32 element forces put an
+  absolute floor under the residual (about 1.2e-7 for the visco cube, 4.5e-4 for the J2 plate, where
+  the bulk term lambda ln J with lambda = 99 mu amplifies the FP32 rounding of F).  A relative
+  criterion puts that floor close to tol * R0 in the increments around the load reversals of the
+  cyclic shear, where R0 is small, and the count there depends on round-off; an absolute tolerance
+  10-20x above the floor (1e-5 visco, 1e-2 J2) does not.  Norms are compared within 1e-4 relative
+  plus three times the floor; U within 1e-4 of max |U| (each run stops somewhere below the
+  criterion).
 """
 import numpy as np
 import pytest
@@ -63,16 +67,16 @@ def test_device_newton_golden_mean_dilatation(golden_nh):
     _golden_run(golden_nh, G.NH_Q1P0, [mat["C10"], mat["BulkModulus"]], 1e-4, 1.0)
 
 
-def _compare(rg, ro, norm_rtol=1e-6, u_tol=1e-8, norm_steps=None):
+def _compare(rg, ro, norm_rtol=1e-6, u_tol=1e-8, norm_steps=None, norm_atol=0.0):
     """Equal iteration counts and cut-backs per increment, final U within u_tol; the norm histories of
-    the first norm_steps increments (all when None) within norm_rtol above round-off."""
+    the first norm_steps increments (all when None) within norm_rtol (plus norm_atol) above round-off."""
     assert rg["rc"] == 0 and ro["rc"] == 0, (rg["rc"], ro["rc"])
     np.testing.assert_array_equal(rg["iters"], ro["iters"])
     np.testing.assert_array_equal(rg["cutbacks"], ro["cutbacks"])
     assert len(rg["norms"]) == len(ro["norms"])
     n = len(ro["norms"]) if norm_steps is None else int(np.sum(ro["iters"][:norm_steps] + 1))
     big = ro["norms"][:n] > 1e-6 * ro["norms"].max()
-    np.testing.assert_allclose(rg["norms"][:n][big], ro["norms"][:n][big], rtol=norm_rtol)
+    np.testing.assert_allclose(rg["norms"][:n][big], ro["norms"][:n][big], rtol=norm_rtol, atol=norm_atol)
     assert np.abs(rg["U"] - ro["U"]).max() <= u_tol * np.abs(ro["U"]).max()
 
 
@@ -124,7 +128,10 @@ def test_newton_history_mixed_matches_oracle(config, nx):
     X, conn, bc, model, params, pe = (_config2 if config == "c2" else _config3)(nx)
     g = G.ElementLoop(X, conn, model, params, per_element=pe, precision=G.MIXED)
     o = O.Model(X, conn, [model], params, per_element=pe)
-    rg = g.analysis(bc, tol=3e-5, itmax=20, norm_mode=0, device_solver=True)
-    ro = o.analysis(bc, tol=3e-5, itmax=20, norm_mode=0)
+    tol, floor = (1e-5, 1.2e-7) if config == "c2" else (1e-2, 4.5e-4)
+    rg = g.analysis(bc, tol=tol, itmax=20, norm_mode=1, device_solver=True)
+    ro = o.analysis(bc, tol=tol, itmax=20, norm_mode=1)
     g.close()
-    _compare(rg, ro, norm_rtol=1e-4, u_tol=1e-5, norm_steps=2 if config == "c3" else None)
+    # U: each run stops somewhere below the residual criterion, which fixes U only to about
+    # tol / stiffness: 1e-4 of max |U| (measured difference 1.8e-5 on the visco cube)
+    _compare(rg, ro, norm_rtol=1e-4, u_tol=1e-4, norm_steps=2 if config == "c3" else None, norm_atol=3 * floor)

@@ -1,7 +1,8 @@
 """The host-buffer call (ceos_evaluate) computes in element slabs and copies every finished node-row
 prefix to the host while later slabs run.  Its f_int and K equal those of the single-launch device
 call (ceos_evaluate_device) up to the summation order of the atomics, for a sweep numbering (rows
-finish slab by slab) and for a scrambled one (rows finish only at the end)."""
+finish slab by slab) and for a scrambled one (rows finish only at the end); in mixed precision with
+both K assemblies (two-pass: element loop then conversion per slab; fused: one launch per slab)."""
 import numpy as np
 import pytest
 
@@ -24,12 +25,15 @@ def _mesh(n, scramble):
 
 
 @pytest.mark.parametrize("n,scramble", [(32, False), (40, True)])
-@pytest.mark.parametrize("precision,rtol", [(G.FP64, 1e-12), (G.MIXED, 2e-5)])
-def test_slab_pipelined_host_call_equals_device_call(n, scramble, precision, rtol):
+@pytest.mark.parametrize("precision,rtol,assembly", [(G.FP64, 1e-12, None), (G.MIXED, 2e-5, "two-pass"),
+                                                     (G.MIXED, 2e-5, "fused")])
+def test_slab_pipelined_host_call_equals_device_call(n, scramble, precision, rtol, assembly):
     import torch
     X, conn = _mesh(n, scramble)
     g = G.ElementLoop(X, conn, G.CNH, CNH_P, precision=precision)
     try:
+        if assembly:
+            g.set_assembly(assembly)
         # a smooth deformation (|grad u| <= 0.2) plus a small nodal jitter
         x, y, z = X[:, 0], X[:, 1], X[:, 2]
         rng = np.random.default_rng(2)

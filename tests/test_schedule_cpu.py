@@ -69,7 +69,7 @@ def slabs(n_elem, conn0, n_nodes, ns):
     return np.array(se, np.int32), np.array(sn, np.int32)
 
 
-def plan(f, X, conn, ns=1, slack=296, stage_max=7678):
+def plan(f, X, conn, ns=1, slack=296, stage_max=7294, max_nodes=256):
     conn0 = np.ascontiguousarray(conn - 1, np.int32)
     N, E = X.shape[0], conn0.shape[0]
     rs, nup, up, n_blocks = pattern(N, conn0)
@@ -83,12 +83,12 @@ def plan(f, X, conn, ns=1, slack=296, stage_max=7678):
     ring = C.c_longlong(0)
     p = lambda a: a.ctypes.data_as(C.c_void_p)
     rc = f(N, E, p(conn0), p(rs), p(nup), C.c_longlong(n_blocks), ns, p(se), p(sn), TILE, slack,
-           C.c_longlong(stage_max), p(queue), p(conv), p(wait), p(slab_q), p(counts), C.byref(ring))
+           C.c_longlong(stage_max), max_nodes, p(queue), p(conv), p(wait), p(slab_q), p(counts), C.byref(ring))
     assert rc == 0
     nq, nc = counts[0], counts[1]
     return {"queue": queue[:nq], "conv": conv[:4 * nc].reshape(nc, 4), "wait": wait.reshape(T, 2), "slab_q": slab_q,
             "R": ring.value, "conn0": conn0, "rs": rs, "nup": nup, "up": up, "n_blocks": n_blocks, "se": se, "sn": sn,
-            "T": T, "N": N, "E": E, "stage_max": stage_max}
+            "T": T, "N": N, "E": E, "stage_max": stage_max, "max_nodes": max_nodes}
 
 
 def tile_blocks(P, t):
@@ -118,12 +118,14 @@ def check_plan(P, seed=0):
             assert pos_item[-v - 1] < 0
             pos_item[-v - 1] = k
     assert (pos_tile >= 0).all() and (pos_item >= 0).all()
-    # items: contiguous node runs covering every node, rows within the staging buffer
+    # items: contiguous node runs covering every node, rows within the staging buffer, nodes within
+    # the item's node table
     assert conv[0, 0] == 0 and conv[-1, 1] == P["N"] and (conv[1:, 0] == conv[:-1, 1]).all()
     rs, nup = P["rs"], P["nup"]
     for n0, n1, t0, t1 in conv:
         L = (rs[n1 - 1] + 6 + 9 * nup[n1 - 1]) - rs[n0]
         assert L <= P["stage_max"] - 1
+        assert 1 <= n1 - n0 <= P["max_nodes"]
     # tiles containing each node
     node_tiles = [[] for _ in range(P["N"])]
     for e, el in enumerate(P["conn0"]):
@@ -213,7 +215,7 @@ def test_schedule_waits_ring_and_drain(planner, case, ns):
         Xn[perm] = X
         X, conn = Xn, (perm[conn - 1] + 1)[rng.permutation(conn.shape[0])].astype(np.int32)
     # a small staging buffer (many conversion items) and a short slack (a small ring)
-    P = plan(planner, X, conn, ns=ns, slack=3, stage_max=600)
+    P = plan(planner, X, conn, ns=ns, slack=3, stage_max=600, max_nodes=24)
     check_plan(P, seed=ns)
 
 
