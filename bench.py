@@ -468,7 +468,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=None, help="mesh size (96 for j2-plate: nx x nx x nx/2; 64 for visco)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--assembly", default="two-pass", choices=["two-pass", "fused"],
+    ap.add_argument("--assembly", default="two-pass", choices=["two-pass", "fused", "banded"],
                     help="mixed-precision K assembly of the element-loop workloads")
     ap.add_argument("--ref-sample-gps", type=int, default=600000,
                     help="Gauss points per step of the reference arm's bounded sample")

@@ -20,7 +20,8 @@ J2_SMALL, NH_Q1P0, SVK, CNH, VISCO_VAR, VISCO_PRONY, J2_FINITE = 2, 4, 5, 7, 12,
 FP64, MIXED = 0, 1
 OPT_STORE_STRESS = 1
 OPT_TIME_KERNELS = 2
-ASSEMBLY_TWO_PASS, ASSEMBLY_FUSED = 0, 1
+ASSEMBLY_TWO_PASS, ASSEMBLY_FUSED, ASSEMBLY_BANDED = 0, 1, 2
+_ASSEMBLY = {"two-pass": ASSEMBLY_TWO_PASS, "fused": ASSEMBLY_FUSED, "banded": ASSEMBLY_BANDED}
 
 _lib = None
 
@@ -75,6 +76,7 @@ def lib():
         L.ceos_gp_stress.argtypes = [P, P]
         L.ceos_set_options.argtypes = [P, I]
         L.ceos_set_assembly.argtypes = [P, I]
+        L.ceos_launch_count.argtypes = [P, I, ip]
         L.ceos_set_committed_time.argtypes = [P, D]
         L.ceos_kernel_time.argtypes = [P, C.POINTER(C.c_float)]
         L.ceos_destroy.argtypes = [P]
@@ -229,17 +231,17 @@ class ElementLoop:
 
     def set_assembly(self, mode):
         """Mixed-precision K assembly: "two-pass" (default; element loop into FP32 node-pair blocks,
-        then a conversion launch writes the FP64 CSR rows) or "fused" (one launch from a host-planned
-        queue, blocks in an L2-sized ring)."""
+        then a conversion launch writes the FP64 CSR rows), "fused" (one launch from a host-planned
+        queue, blocks in an L2-sized ring) or "banded" (the two passes band by band on three streams,
+        blocks in a ring of a few bands)."""
+        _check(lib().ceos_set_assembly(self._h, _ASSEMBLY[mode]))
         self.assembly = mode
-        _check(lib().ceos_set_assembly(self._h, {"two-pass": ASSEMBLY_TWO_PASS, "fused": ASSEMBLY_FUSED}[mode]))
 
     def launches_per_evaluation(self, tangent=True):
-        """Kernels that one device-resident evaluation launches: in mixed precision with a tangent two
-        (two-pass: element loop, conversion) or one (fused); the element loop otherwise."""
-        if self.precision == MIXED and tangent:
-            return 1 if self.assembly == "fused" else 2
-        return 1
+        """Kernels that one device-resident evaluation launches under the current assembly."""
+        n = C.c_int(0)
+        _check(lib().ceos_launch_count(self._h, int(bool(tangent)), C.byref(n)))
+        return n.value
 
     def kernel_names(self):
         """Names of the kernels of one device-resident evaluation with a tangent."""

@@ -77,6 +77,21 @@ void model_init_state(int model, double* st) {
 template <typename T>
 size_t elem_smem(const Handle* h) { return SmemLayout<T>(h->ns_used).total; }
 
+// Streams and events of the banded assembly, created at its first evaluation.
+int ensure_band_streams(Handle* h) {
+    if (h->band_stream) return 0;
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CK(cudaStreamCreateWithFlags(&h->band_stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithPriority(&h->conv_stream, cudaStreamNonBlocking, hi));  // hi: the greatest priority
+    CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    h->ev_band.assign(h->n_bands, nullptr);
+    h->ev_bconv.assign(h->n_bands, nullptr);
+    for (auto& ev : h->ev_band) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    for (auto& ev : h->ev_bconv) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    return 0;
+}
+
 // The launches of one evaluation range.  CEOS_MIXED with a tangent, two-pass assembly (default):
 // the element loop over elements [e0, e1) reducing FP32 node-pair blocks into the scratch, then
 // the conversion of the items of element slab `slab` (every item for slab -1).  Fused assembly:
@@ -117,6 +132,65 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
     const size_t smem = elem_smem<T>(h);
     const bool timed = (h->options & CEOS_OPT_TIME_KERNELS) && h->ev_k0;
     if constexpr (sizeof(T) == 4) {
+        if (dkval && h->assembly == CEOS_ASSEMBLY_BANDED) {
+            // the whole mesh band by band (every band is a slab of its own; `slab` is not used):
+            // even element bands on s, odd ones on band_stream, conversions on conv_stream
+            a.rs = h->d_blk0;
+            a.kblk = h->d_kblk;
+            a.ring_mask = h->band_ring - 1;
+            a.csr_rs = h->d_rs;
+            a.conv = static_cast<const int4*>(h->d_bconv);
+            {
+                const int r = ensure_band_streams(h);
+                if (r) return r;
+            }
+            CK(cudaFuncSetAttribute(element_loop_kernel<float, MODEL, SCATTER_RING>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            if (timed) CK(cudaEventRecord(h->ev_k0, s));
+            CK(cudaEventRecord(h->ev_fork, s));
+            CK(cudaStreamWaitEvent(h->band_stream, h->ev_fork, 0));
+            CK(cudaStreamWaitEvent(h->conv_stream, h->ev_fork, 0));
+            if (h->copy_f) CK(cudaStreamWaitEvent(h->copy_stream, h->ev_fork, 0));
+            int n_done = 0;
+            for (int c = 0; c < h->n_bands; ++c) {
+                cudaStream_t st = (c & 1) ? h->band_stream : s;
+                // ring slots: every row below band_node_end[c - depth] is converted and zeroed
+                if (c >= h->band_depth) CK(cudaStreamWaitEvent(st, h->ev_bconv[c - h->band_depth], 0));
+                a.e_begin = h->band_e[c];
+                a.e_end = h->band_e[c + 1];
+                const int n_tiles = (a.e_end - a.e_begin + kTileE - 1) / kTileE;
+                element_loop_kernel<float, MODEL, SCATTER_RING><<<std::min(n_tiles, h->grid_cap), kThreads, smem, st>>>(a);
+                CK(cudaGetLastError());
+                CK(cudaEventRecord(h->ev_band[c], st));
+                // rows of band c: every band <= c has reduced (band c - 1 was waited for before the
+                // conversion of band c - 1, earlier in conv_stream)
+                CK(cudaStreamWaitEvent(h->conv_stream, h->ev_band[c], 0));
+                const int j0 = h->band_conv[c], j1 = h->band_conv[c + 1];
+                if (j1 > j0) {
+                    csr_convert_kernel<<<std::min(j1 - j0, h->conv_grid), kThreads, kStageRegion, h->conv_stream>>>(
+                        a, nullptr, j0, j1);
+                    CK(cudaGetLastError());
+                }
+                CK(cudaEventRecord(h->ev_bconv[c], h->conv_stream));
+                const int n_end = h->band_node_end[c];
+                if (h->copy_f && n_end > n_done) {  // host-buffer call: the finished rows go to the host now
+                    CK(cudaStreamWaitEvent(h->copy_stream, h->ev_bconv[c], 0));
+                    CK(cudaMemcpyAsync(h->copy_f + 3 * (size_t)n_done, dfint + 3 * (size_t)n_done,
+                                       3 * (size_t)(n_end - n_done) * sizeof(double), cudaMemcpyDeviceToHost,
+                                       h->copy_stream));
+                    const long long k0 = h->rs[n_done], k1 = n_end < h->n_nodes ? h->rs[n_end] : h->nnz;
+                    CK(cudaMemcpyAsync(h->copy_k + k0, dkval + k0, (size_t)(k1 - k0) * sizeof(double),
+                                       cudaMemcpyDeviceToHost, h->copy_stream));
+                }
+                n_done = n_end;
+            }
+            CK(cudaStreamWaitEvent(s, h->ev_bconv[h->n_bands - 1], 0));  // joins every band and conversion
+            if (timed) {
+                CK(cudaEventRecord(h->ev_k1, s));
+                CK(cudaEventRecord(h->ev_k2, s));
+            }
+            return 0;
+        }
         if (dkval && h->assembly == CEOS_ASSEMBLY_TWO_PASS) {
             a.e_begin = e0;
             a.e_end = e1;
@@ -465,7 +539,7 @@ static int evaluate_prologue(Handle* h, double time, double* dfint, double* dkva
     if (dkval && h->precision == CEOS_MIXED) {
         ++h->epoch;  // the flags of this evaluation's tiles and conversion items
         if (h->ring_dirty) {  // an aborted evaluation may have left partial sums in the blocks
-            CK(cudaMemsetAsync(h->d_kblk, 0, (size_t)h->n_blocks * 12 * sizeof(float), s));
+            CK(cudaMemsetAsync(h->d_kblk, 0, (size_t)h->kblk_slots * 12 * sizeof(float), s));
             h->ring_dirty = false;
         }
     }
@@ -520,8 +594,9 @@ static void plan_slab_bounds(Handle* h) {
 }
 
 static int ensure_copy_stream(Handle* h) {
-    if (h->n_slabs > 1 && !h->copy_stream) {
+    if (!h->copy_stream && (h->n_slabs > 1 || h->assembly == CEOS_ASSEMBLY_BANDED))
         CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    if (h->n_slabs > 1 && h->slab_ev.empty()) {
         h->slab_ev.assign(h->n_slabs, nullptr);
         for (auto& ev : h->slab_ev) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     }
@@ -581,15 +656,34 @@ static int build_schedule(Handle* h) {
     uint32_t pow2 = 1;
     while ((long long)pow2 < h->n_blocks) pow2 <<= 1;
     h->scratch_mask = pow2 - 1;
-    // every block has a slot of its own (two-pass); the fused ring uses slots [0, ring_blocks), and
-    // when ring_blocks exceeds n_blocks its slot index is the block index itself
-    CK(cudaMalloc(&h->d_kblk, (size_t)h->n_blocks * 12 * sizeof(float)));
-    CK(cudaMemset(h->d_kblk, 0, (size_t)h->n_blocks * 12 * sizeof(float)));
+    // the default two-pass assembly gives every block a slot of its own (ceos_set_assembly resizes)
+    h->kblk_slots = h->n_blocks;
+    CK(cudaMalloc(&h->d_kblk, (size_t)h->kblk_slots * 12 * sizeof(float)));
+    CK(cudaMemset(h->d_kblk, 0, (size_t)h->kblk_slots * 12 * sizeof(float)));
     int per_sm = 1, sms = 148;
     CK(cudaFuncSetAttribute(csr_convert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageRegion));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csr_convert_kernel, kThreads, kStageRegion));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
     h->conv_grid = sms * std::max(1, per_sm);
+    // banded two-pass assembly: bands of two waves of tiles
+    {
+        BandPlan bp;
+        const int band_elems = std::max(1, 2 * h->grid_cap) * kTileE;
+        const int brc = plan_bands(h->n_nodes, h->n_elem, h->conn0.data(), h->rs.data(), h->nup.data(), h->n_blocks,
+                                   band_elems, kTileE, kStageDoubles, kConvNodes, h->band_depth, bp);
+        if (brc) {
+            h->msg = bp.err;
+            return brc;
+        }
+        h->n_bands = (int)bp.node_end.size();
+        h->band_e = bp.band_e;
+        h->band_node_end = bp.node_end;
+        h->band_conv = bp.band_conv;
+        h->band_ring = (uint32_t)bp.ring_blocks;
+        const size_t nbc = bp.conv.size();
+        CK(cudaMalloc(&h->d_bconv, std::max<size_t>(nbc, 1) * sizeof(int4)));
+        if (nbc) CK(cudaMemcpy(h->d_bconv, bp.conv.data(), nbc * sizeof(int4), cudaMemcpyHostToDevice));
+    }
     return 0;
 }
 }  // namespace ceos
@@ -642,7 +736,15 @@ extern "C" int ceos_evaluate(void* handle, double time, const double* U, double*
     double* dk = kval ? h->d_kval : nullptr;
     int rc = evaluate_prologue(h, time, h->d_fint, dk, s);
     if (rc) return rc;
-    if (h->n_slabs == 1) {
+    if (kval && h->precision == CEOS_MIXED && h->assembly == CEOS_ASSEMBLY_BANDED) {
+        // the bands copy their finished rows to the host on copy_stream as they go
+        h->copy_f = fint;
+        h->copy_k = kval;
+        rc = evaluate_range(h, time, h->d_U, h->d_fint, dk, s, 0, h->n_elem, -1);
+        h->copy_f = h->copy_k = nullptr;
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(h->copy_stream));
+    } else if (h->n_slabs == 1) {
         rc = evaluate_range(h, time, h->d_U, h->d_fint, dk, s, 0, h->n_elem, -1);
         if (rc) return rc;
         CK(cudaMemcpyAsync(fint, h->d_fint, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -868,10 +970,48 @@ extern "C" int ceos_set_options(void* handle, int options) {
     return 0;
 }
 
+extern "C" int ceos_launch_count(void* handle, int tangent, int* n_launches) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !n_launches) return CEOS_E_ARG;
+    int n = 1;  // the element loop
+    if (tangent && h->precision == CEOS_MIXED) {
+        if (h->assembly == CEOS_ASSEMBLY_TWO_PASS) {
+            n = 1 + (h->n_conv > 0 ? 1 : 0);
+        } else if (h->assembly == CEOS_ASSEMBLY_BANDED) {
+            n = h->n_bands;
+            for (int c = 0; c < h->n_bands; ++c) n += h->band_conv[c + 1] > h->band_conv[c] ? 1 : 0;
+        }
+    }
+    *n_launches = n;
+    return 0;
+}
+
 extern "C" int ceos_set_assembly(void* handle, int mode) {
     Handle* h = static_cast<Handle*>(handle);
-    if (!h || (mode != CEOS_ASSEMBLY_TWO_PASS && mode != CEOS_ASSEMBLY_FUSED)) return CEOS_E_ARG;
-    h->assembly = mode;  // both leave every block they use at zero after an evaluation
+    if (!h || (mode != CEOS_ASSEMBLY_TWO_PASS && mode != CEOS_ASSEMBLY_FUSED && mode != CEOS_ASSEMBLY_BANDED))
+        return CEOS_E_ARG;
+    if (h->precision == CEOS_MIXED && h->d_kblk) {
+        // slots the mode uses: every block, or a power-of-two ring (a ring of at least n_blocks slots
+        // indexes blocks directly, so n_blocks of them suffice)
+        const long long ring = mode == CEOS_ASSEMBLY_FUSED ? (long long)h->ring_blocks : (long long)h->band_ring;
+        const long long need = mode == CEOS_ASSEMBLY_TWO_PASS ? h->n_blocks : std::min(ring, h->n_blocks);
+        if (need != h->kblk_slots) {  // the new slots exist before the old ones go: a failure changes nothing
+            CK(cudaSetDevice(h->device));
+            CK(cudaStreamSynchronize(h->stream));
+            float* fresh = nullptr;
+            CK(cudaMalloc(&fresh, (size_t)need * 12 * sizeof(float)));
+            if (cudaMemset(fresh, 0, (size_t)need * 12 * sizeof(float)) != cudaSuccess) {
+                cudaFree(fresh);
+                h->msg = "ceos_set_assembly: clearing the block slots failed";
+                return CEOS_E_CUDA;
+            }
+            cudaFree(h->d_kblk);
+            h->d_kblk = fresh;
+            h->kblk_slots = need;
+            h->ring_dirty = false;
+        }
+    }
+    h->assembly = mode;  // every mode leaves the slots it uses at zero after an evaluation
     return 0;
 }
 
@@ -1015,7 +1155,7 @@ Handle::~Handle() {
     if (stream) cudaStreamSynchronize(stream);
     void* ptrs[] = {d_X, d_U, d_fint, d_kval, d_conn, d_rs, d_blk0, d_nup, d_ranks, d_elem_status, d_status_count,
                     d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress, d_kblk, d_queue, d_conv,
-                    d_tile_wait, d_flags, d_ticket, d_sched_err, d_conv_order};
+                    d_tile_wait, d_flags, d_ticket, d_sched_err, d_conv_order, d_bconv};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (ev_k0) cudaEventDestroy(ev_k0);
@@ -1023,6 +1163,13 @@ Handle::~Handle() {
     if (ev_k2) cudaEventDestroy(ev_k2);
     for (cudaEvent_t ev : slab_ev)
         if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : ev_band)
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : ev_bconv)
+        if (ev) cudaEventDestroy(ev);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (band_stream) cudaStreamDestroy(band_stream);
+    if (conv_stream) cudaStreamDestroy(conv_stream);
     if (copy_stream) cudaStreamDestroy(copy_stream);
     if (stream) cudaStreamDestroy(stream);
 }

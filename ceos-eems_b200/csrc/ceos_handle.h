@@ -38,8 +38,9 @@ struct Handle {
     int* d_mat_id = nullptr;
     void* d_state[2] = {nullptr, nullptr};
     void* d_gp_stress = nullptr;
-    float* d_kblk = nullptr;              // mixed mode: FP32 node-pair blocks, n_blocks of them (the fused
-                                          // assembly uses the first ring_blocks as its ring)
+    float* d_kblk = nullptr;              // mixed mode: FP32 node-pair block slots, kblk_slots of them: every
+                                          // block (two-pass) or the ring of the fused / banded assembly
+    long long kblk_slots = 0;
     long long n_blocks = 0;
     int assembly = CEOS_ASSEMBLY_TWO_PASS;  // mixed mode with a tangent: two-pass or fused assembly
     uint32_t scratch_mask = 0;            // two-pass: power of two minus one, >= every block index
@@ -47,6 +48,19 @@ struct Handle {
                                           // d_conv_order[slab_conv[c] .. slab_conv[c + 1])
     int* d_conv_order = nullptr;
     int conv_grid = 148;                  // CTAs of a conversion launch
+    // banded two-pass assembly: element bands on two alternating streams, each band's conversion on
+    // a third; the blocks live in a ring of band_ring slots (see plan_bands, schedule.h)
+    int n_bands = 0;
+    std::vector<int> band_e, band_node_end, band_conv;
+    void* d_bconv = nullptr;              // int4 [band_conv[n_bands]] conversion items of the bands
+    uint32_t band_ring = 0;
+    int band_depth = 3;                   // element band c starts after the conversion of band c - depth
+    cudaStream_t band_stream = nullptr;   // odd element bands (even ones run on the caller's stream)
+    cudaStream_t conv_stream = nullptr;   // conversions, highest priority
+    cudaEvent_t ev_fork = nullptr;
+    std::vector<cudaEvent_t> ev_band, ev_bconv;
+    double* copy_f = nullptr;             // host-buffer call with the banded assembly: f_int and K rows
+    double* copy_k = nullptr;             // go to these host arrays band by band on copy_stream
     // fused assembly schedule (mixed mode with a tangent): a queue of element tiles and CSR
     // conversion items, split at the element slabs of the host-buffer evaluation
     std::vector<int> queue;               // >= 0 tile, < 0 conversion item -(j+1)

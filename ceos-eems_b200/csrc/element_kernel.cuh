@@ -895,15 +895,16 @@ CEOS_D void convert_rows(const ElemArgs<float>& a, int n0, int n1, double* stage
 }
 
 // Conversion pass of the two-pass assembly: CTA k converts the items order[j0 + k], order[j0 + k +
-// gridDim.x], ... < j1 (conversion items of one element slab, or all of them).  The element pass
-// before it in stream order has completed every reduction into their blocks.  Dynamic shared
-// memory: kStageRegion bytes (the staging of one item and its node table).
+// gridDim.x], ... < j1 (conversion items of one element slab, or all of them; items j themselves
+// when order is null, as for the bands of the banded assembly).  The element passes before it in
+// stream order have completed every reduction into their blocks.  Dynamic shared memory:
+// kStageRegion bytes (the staging of one item and its node table).
 __global__ void __launch_bounds__(kThreads) csr_convert_kernel(ElemArgs<float> a, const int* order, int j0, int j1) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* stage = reinterpret_cast<double*>(smem_raw);
     int* info = reinterpret_cast<int*>(stage + kStageDoubles + 2);
     for (int j = j0 + (int)blockIdx.x; j < j1; j += (int)gridDim.x) {
-        const int4 c = __ldg(a.conv + __ldg(order + j));
+        const int4 c = __ldg(a.conv + (order ? __ldg(order + j) : j));
         convert_rows<2>(a, c.x, c.y, stage, info, (int)threadIdx.x);
         __syncthreads();  // the staging is read out before the next item writes it
     }

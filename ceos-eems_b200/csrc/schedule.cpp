@@ -155,6 +155,90 @@ int plan_schedule(int n_nodes, int n_elem, const int* conn0, const long long* rs
     return 0;
 }
 
+int plan_bands(int n_nodes, int n_elem, const int* conn0, const long long* rs, const int* nup, long long n_blocks,
+               int band_elems, int tile_elems, long long stage_max, int max_nodes, int depth, BandPlan& out) {
+    const int E = n_elem, N = n_nodes;
+    if (E < 1 || N < 1 || tile_elems < 1 || band_elems < tile_elems || band_elems % tile_elems || max_nodes < 1 ||
+        depth < 1) {
+        out.err = "bands: bad arguments";
+        return CEOS_E_ARG;
+    }
+    const int nb = (E + band_elems - 1) / band_elems;
+    out.band_e.assign(nb + 1, 0);
+    for (int c = 0; c < nb; ++c) out.band_e[c] = c * band_elems;
+    out.band_e[nb] = E;
+    std::vector<long long> bb(N + 1);
+    for (int n = 0; n < N; ++n) bb[n] = (long long)n + (rs[n] - 6LL * n) / 9;
+    bb[N] = n_blocks;
+    // last band touching each node, and the largest block end each band touches
+    std::vector<int> last(N, -1);
+    std::vector<long long> maxb(nb, 0);
+    for (int c = 0; c < nb; ++c)
+        for (int e = out.band_e[c]; e < out.band_e[c + 1]; ++e)
+            for (int k = 0; k < 8; ++k) {
+                const int n = conn0[(size_t)8 * e + k];
+                last[n] = c;
+                maxb[c] = std::max(maxb[c], bb[n] + 1 + nup[n]);
+            }
+    for (int n = 0; n < N; ++n)
+        if (last[n] < 0) {
+            out.err = "bands: node " + std::to_string(n + 1) + " belongs to no element";
+            return CEOS_E_MESH;
+        }
+    // final prefixes: a running maximum over the last bands of the nodes in row order
+    out.node_end.assign(nb, 0);
+    {
+        int run = 0, n = 0;
+        for (int c = 0; c < nb; ++c) {
+            while (n < N && std::max(run, last[n]) <= c) run = std::max(run, last[n++]);
+            out.node_end[c] = n;
+        }
+        out.node_end[nb - 1] = N;
+    }
+    // conversion items: runs of at most max_nodes nodes and stage_max - 1 values, cut at the prefixes
+    out.conv.clear();
+    out.band_conv.assign(nb + 1, 0);
+    int n0 = 0;
+    for (int c = 0; c < nb; ++c) {
+        out.band_conv[c] = (int)out.conv.size();
+        const int n_end = out.node_end[c];
+        long long len = 0;
+        int a = n0;
+        for (int n = n0; n < n_end; ++n) {
+            const long long ln = 6 + 9LL * nup[n];
+            if (ln > stage_max - 1) {
+                out.err = "bands: the CSR rows of node " + std::to_string(n + 1) + " exceed the staging buffer";
+                return CEOS_E_MESH;
+            }
+            if (n > a && (len + ln > stage_max - 1 || n - a >= max_nodes)) {
+                out.conv.push_back(ConvItem{a, n, c, c});
+                a = n;
+                len = 0;
+            }
+            len += ln;
+        }
+        if (n_end > a) out.conv.push_back(ConvItem{a, n_end, c, c});
+        n0 = std::max(n0, n_end);
+    }
+    out.band_conv[nb] = (int)out.conv.size();
+    // ring: the largest span of live blocks [bb(node_end[c - depth]), M(c + 1))
+    long long Rmax = 1;
+    while (Rmax < n_blocks) Rmax <<= 1;
+    long long span = 1, M = 0;
+    std::vector<long long> Mk(nb);
+    for (int c = 0; c < nb; ++c) Mk[c] = M = std::max(M, maxb[c]);
+    for (int c = 0; c < nb; ++c) {
+        const long long lo = c - depth >= 0 ? bb[out.node_end[c - depth]] : 0;
+        const long long hi = Mk[std::min(c + 1, nb - 1)];
+        span = std::max(span, hi - lo);
+    }
+    out.max_span = span;
+    long long R = 1;
+    while (R < span + 1) R <<= 1;
+    out.ring_blocks = std::min(R, Rmax);
+    return 0;
+}
+
 }  // namespace ceos
 
 #ifdef CEOS_SCHEDULE_TEST
@@ -186,6 +270,36 @@ extern "C" int ceos_test_plan_schedule(int n_nodes, int n_elem, const int* conn0
     counts[1] = (int)p.conv.size();
     counts[2] = p.n_tiles;
     *ring_blocks = p.ring_blocks;
+    return 0;
+}
+#endif
+
+#ifdef CEOS_SCHEDULE_TEST
+// Flat entry for the CPU tests of the band plan.  Output arrays sized by the caller: band_e
+// [n_elem/band_elems + 2], node_end [n_elem/band_elems + 1], conv [4 n_nodes], band_conv
+// [n_elem/band_elems + 2]; counts [n_bands, n_conv]; ring [ring_blocks, max_span].
+extern "C" int ceos_test_plan_bands(int n_nodes, int n_elem, const int* conn0, const long long* rs, const int* nup,
+                                    long long n_blocks, int band_elems, int tile_elems, long long stage_max,
+                                    int max_nodes, int depth, int* band_e, int* node_end, int* conv, int* band_conv,
+                                    int* counts, long long* ring) {
+    ceos::BandPlan p;
+    const int rc = ceos::plan_bands(n_nodes, n_elem, conn0, rs, nup, n_blocks, band_elems, tile_elems, stage_max,
+                                    max_nodes, depth, p);
+    if (rc) return rc;
+    const int nb = (int)p.node_end.size();
+    std::copy(p.band_e.begin(), p.band_e.end(), band_e);
+    std::copy(p.node_end.begin(), p.node_end.end(), node_end);
+    std::copy(p.band_conv.begin(), p.band_conv.end(), band_conv);
+    for (size_t j = 0; j < p.conv.size(); ++j) {
+        conv[4 * j] = p.conv[j].n0;
+        conv[4 * j + 1] = p.conv[j].n1;
+        conv[4 * j + 2] = p.conv[j].t0;
+        conv[4 * j + 3] = p.conv[j].t1;
+    }
+    counts[0] = nb;
+    counts[1] = (int)p.conv.size();
+    ring[0] = p.ring_blocks;
+    ring[1] = p.max_span;
     return 0;
 }
 #endif

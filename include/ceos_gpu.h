@@ -130,9 +130,14 @@ int ceos_kernel_time(void* handle, float* ms);
 /* CEOS_MIXED K assembly: CEOS_ASSEMBLY_TWO_PASS (default) runs the element loop, reducing FP32
  * node-pair blocks into a scratch array that holds all of them, then a conversion launch writes
  * the FP64 CSR rows; CEOS_ASSEMBLY_FUSED runs both in one launch from a host-planned queue, with
- * the blocks in a ring sized for L2.  Both give the same K up to the FP32 summation order. */
-enum { CEOS_ASSEMBLY_TWO_PASS = 0, CEOS_ASSEMBLY_FUSED = 1 };
+ * the blocks in a ring sized for L2; CEOS_ASSEMBLY_BANDED runs the two passes band by band, element
+ * bands on two alternating streams and each band's conversion on a third, the blocks in a ring that
+ * holds the rows of a few bands.  All give the same K up to the FP32 summation order. */
+enum { CEOS_ASSEMBLY_TWO_PASS = 0, CEOS_ASSEMBLY_FUSED = 1, CEOS_ASSEMBLY_BANDED = 2 };
 int ceos_set_assembly(void* handle, int mode);
+/* Kernel launches of one device-resident evaluation (with or without a tangent) under the current
+ * assembly. */
+int ceos_launch_count(void* handle, int tangent, int* n_launches);
 int ceos_set_committed_time(void* handle, double t);
 
 /* Release every device buffer and the stream. */

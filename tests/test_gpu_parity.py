@@ -97,7 +97,7 @@ def test_evaluate_fp64(model, params, amp):
 @pytest.mark.parametrize("model,params,amp,tol", [
     (G.CNH, CNH_P, 0.08, 2e-5), (G.VISCO_PRONY, PRONY_P, 0.08, 2e-5), (G.J2_FINITE, J2F_P, 0.01, 5e-5),
     (G.VISCO_VAR, VV_P, 0.05, 2e-5), (G.NH_Q1P0, Q1P0_P, 0.08, 5e-5)])
-@pytest.mark.parametrize("assembly", ["two-pass", "fused"])
+@pytest.mark.parametrize("assembly", ["two-pass", "fused", "banded"])
 def test_evaluate_mixed(model, params, amp, tol, assembly):
     X, conn = meshgen.structured_box(6, 5, 4, jitter=0.05, seed=2)
     g, o = _pair(model, params, X, conn, precision=G.MIXED)

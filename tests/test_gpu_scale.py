@@ -1,8 +1,8 @@
 """Parity at the benchmark configurations' full size, against the FP64 oracle, through the C ABI.
 
 One mixed-precision evaluation of each element-loop benchmark mesh, after the same committed
-history as the benchmark, compared with the FP64 oracle at the same Gauss-point history, with both
-K assemblies (two-pass and fused):
+history as the benchmark, compared with the FP64 oracle at the same Gauss-point history, with the
+three K assemblies (two-pass, fused, banded: 24 and 14 bands on these meshes):
 - the finite-strain J2 plate, 96 x 96 x 48 Hexa8 (442,368 elements) with per-element E and
   sigma_y0, evaluated at 2.5 % uniaxial strain from 1.25 % committed (every point plastic);
 - the visco-Prony cube, 64^3 Hexa8 (262,144 elements), cyclic simple shear after two increments.
@@ -45,9 +45,12 @@ def test_benchmark_mesh_evaluation_matches_fp64_oracle(name):
     fg, kg, rc, nf = g.evaluate(w.t_eval, w.U_eval)  # two-pass assembly (the default)
     assert rc == 0 and nf == 0
     st_g = g.state(1)
-    g.set_assembly("fused")  # the same evaluation (nothing committed) with the fused assembly
-    fg2, kg2, rc2, _ = g.evaluate(w.t_eval, w.U_eval)
-    assert rc2 == 0
+    others = []
+    for mode in ("fused", "banded"):  # the same evaluation (nothing committed) with the other assemblies
+        g.set_assembly(mode)
+        fg2, kg2, rc2, _ = g.evaluate(w.t_eval, w.U_eval)
+        assert rc2 == 0
+        others.append((fg2, kg2))
     g.close()
     threads = os.cpu_count() or 1
     used = np.arange(1, w.X.shape[0] + 1)
@@ -55,7 +58,7 @@ def test_benchmark_mesh_evaluation_matches_fp64_oracle(name):
     fo, ko, rco = m.evaluate_sample(w.t_eval, U, w.n_elem, threads)
     assert rco == 0
     bf, bk = BARS[name]
-    for f_, k_ in ((fg, kg), (fg2, kg2)):
+    for f_, k_ in [(fg, kg)] + others:
         ef = np.abs(f_ - fo).max() / np.abs(fo).max()
         ek = np.abs(k_ - ko).max() / np.abs(ko).max()
         assert ef <= bf and ek <= bk, (name, ef, ek)

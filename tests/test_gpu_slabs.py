@@ -2,7 +2,9 @@
 prefix to the host while later slabs run.  Its f_int and K equal those of the single-launch device
 call (ceos_evaluate_device) up to the summation order of the atomics, for a sweep numbering (rows
 finish slab by slab) and for a scrambled one (rows finish only at the end); in mixed precision with
-both K assemblies (two-pass: element loop then conversion per slab; fused: one launch per slab)."""
+the three K assemblies (two-pass: element loop then conversion per slab; fused: one launch per slab;
+banded: element bands on two streams and each band's conversion on a third, rows copied band by band,
+two to four bands on these meshes)."""
 import numpy as np
 import pytest
 
@@ -26,7 +28,7 @@ def _mesh(n, scramble):
 
 @pytest.mark.parametrize("n,scramble", [(32, False), (40, True)])
 @pytest.mark.parametrize("precision,rtol,assembly", [(G.FP64, 1e-12, None), (G.MIXED, 2e-5, "two-pass"),
-                                                     (G.MIXED, 2e-5, "fused")])
+                                                     (G.MIXED, 2e-5, "fused"), (G.MIXED, 2e-5, "banded")])
 def test_slab_pipelined_host_call_equals_device_call(n, scramble, precision, rtol, assembly):
     import torch
     X, conn = _mesh(n, scramble)

@@ -225,3 +225,96 @@ def test_schedule_ring_stays_small_on_a_swept_mesh(planner):
     P = plan(planner, X, conn, ns=1, slack=8)
     assert P["R"] < P["n_blocks"] / 2
     check_plan(P)
+
+
+# ---- banded two-pass assembly (plan_bands) ----
+
+@pytest.fixture(scope="module")
+def band_planner(tmp_path_factory):
+    so = str(tmp_path_factory.mktemp("bands") / "libbands_test.so")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-DCEOS_SCHEDULE_TEST", SRC, "-o", so])
+    f = C.CDLL(so).ceos_test_plan_bands
+    f.restype = C.c_int
+    return f
+
+
+def plan_bands(f, X, conn, band_elems, depth=2, stage_max=7294, max_nodes=256):
+    conn0 = np.ascontiguousarray(conn - 1, np.int32)
+    N, E = X.shape[0], conn0.shape[0]
+    rs, nup, up, n_blocks = pattern(N, conn0)
+    nb_max = E // band_elems + 2
+    band_e = np.zeros(nb_max, np.int32)
+    node_end = np.zeros(nb_max, np.int32)
+    conv = np.zeros(4 * N, np.int32)
+    band_conv = np.zeros(nb_max, np.int32)
+    counts = np.zeros(2, np.int32)
+    ring = np.zeros(2, np.int64)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    rc = f(N, E, p(conn0), p(rs), p(nup), C.c_longlong(n_blocks), band_elems, TILE, C.c_longlong(stage_max), max_nodes,
+           depth, p(band_e), p(node_end), p(conv), p(band_conv), p(counts), p(ring))
+    assert rc == 0
+    nb, nc = counts
+    return {"band_e": band_e[:nb + 1], "node_end": node_end[:nb], "conv": conv[:4 * nc].reshape(nc, 4),
+            "band_conv": band_conv[:nb + 1], "R": int(ring[0]), "span": int(ring[1]), "conn0": conn0, "rs": rs,
+            "nup": nup, "n_blocks": n_blocks, "N": N, "E": E, "depth": depth, "stage_max": stage_max,
+            "max_nodes": max_nodes}
+
+
+def check_bands(P):
+    """Items cover every row once, band by band, with rows final after their band; at every moment of
+    the pipeline (element bands c and c + 1 running, conversions done up to band c - depth) the blocks
+    of the live rows occupy distinct ring slots."""
+    be, ne, conv, bc = P["band_e"], P["node_end"], P["conv"], P["band_conv"]
+    nb = len(ne)
+    assert be[0] == 0 and be[-1] == P["E"] and all(b % TILE == 0 for b in be[:-1])
+    assert (np.diff(ne) >= 0).all() and ne[-1] == P["N"]
+    rs, nup, conn0 = P["rs"], P["nup"], P["conn0"]
+    first, last = np.full(P["N"], nb), np.full(P["N"], -1)
+    for c in range(nb):
+        nodes = np.unique(conn0[be[c]:be[c + 1]])
+        first[nodes] = np.minimum(first[nodes], c)
+        last[nodes] = np.maximum(last[nodes], c)
+    lo = 0
+    for c in range(nb):
+        items = conv[bc[c]:bc[c + 1]]
+        if len(items):
+            assert items[0, 0] == lo and items[-1, 1] == ne[c] and (items[1:, 0] == items[:-1, 1]).all()
+        for n0, n1, _, _ in items:
+            assert 1 <= n1 - n0 <= P["max_nodes"]
+            assert rs[n1 - 1] + 6 + 9 * nup[n1 - 1] - rs[n0] <= P["stage_max"] - 1
+            assert last[n0:n1].max() <= c  # no later band touches these rows
+        lo = ne[c]
+    R = P["R"]
+    assert R & (R - 1) == 0
+    bb = np.arange(P["N"]) + (rs - 6 * np.arange(P["N"])) // 9
+    for c in range(nb):
+        low = ne[c - P["depth"]] if c - P["depth"] >= 0 else 0
+        live = [n for n in range(low, P["N"]) if first[n] <= min(c + 1, nb - 1)]
+        blocks = np.concatenate([np.arange(bb[n], bb[n] + 1 + nup[n]) for n in live]) if live else np.zeros(0, int)
+        slots = blocks % R
+        assert len(np.unique(slots)) == len(slots), c
+
+
+@pytest.mark.parametrize("case,band_elems", [("cube", 128), ("plate", 256), ("plate", 64), ("shuffled", 96)])
+def test_band_plan_items_and_ring(band_planner, case, band_elems):
+    if case == "cube":
+        X, conn = meshgen.structured_box(12, 12, 12, jitter=0.05, seed=0)
+    elif case == "plate":
+        X, conn = meshgen.structured_box(16, 16, 8, lx=2.0, ly=2.0, jitter=0.05, seed=0)
+    else:
+        X, conn = meshgen.structured_box(9, 8, 7, jitter=0.05, seed=1)
+        rng = np.random.default_rng(3)
+        perm = rng.permutation(X.shape[0])
+        Xn = np.empty_like(X)
+        Xn[perm] = X
+        X, conn = Xn, (perm[conn - 1] + 1)[rng.permutation(conn.shape[0])].astype(np.int32)
+    P = plan_bands(band_planner, X, conn, band_elems, stage_max=600, max_nodes=24)
+    check_bands(P)
+
+
+def test_band_ring_stays_small_on_a_swept_mesh(band_planner):
+    """On a mesh numbered along a sweep the band ring holds a few bands of node rows, not the mesh."""
+    X, conn = meshgen.structured_box(24, 24, 24, jitter=0.05, seed=0)
+    P = plan_bands(band_planner, X, conn, band_elems=24 * 24 * 2)
+    assert P["R"] <= P["n_blocks"] / 2
+    check_bands(P)
