@@ -295,8 +295,9 @@ def check_bands(P):
         assert len(np.unique(slots)) == len(slots), c
 
 
+@pytest.mark.parametrize("depth", [2, 3])
 @pytest.mark.parametrize("case,band_elems", [("cube", 128), ("plate", 256), ("plate", 64), ("shuffled", 96)])
-def test_band_plan_items_and_ring(band_planner, case, band_elems):
+def test_band_plan_items_and_ring(band_planner, case, band_elems, depth):
     if case == "cube":
         X, conn = meshgen.structured_box(12, 12, 12, jitter=0.05, seed=0)
     elif case == "plate":
@@ -308,13 +309,13 @@ def test_band_plan_items_and_ring(band_planner, case, band_elems):
         Xn = np.empty_like(X)
         Xn[perm] = X
         X, conn = Xn, (perm[conn - 1] + 1)[rng.permutation(conn.shape[0])].astype(np.int32)
-    P = plan_bands(band_planner, X, conn, band_elems, stage_max=600, max_nodes=24)
+    P = plan_bands(band_planner, X, conn, band_elems, depth=depth, stage_max=600, max_nodes=24)
     check_bands(P)
 
 
 def test_band_ring_stays_small_on_a_swept_mesh(band_planner):
     """On a mesh numbered along a sweep the band ring holds a few bands of node rows, not the mesh."""
     X, conn = meshgen.structured_box(24, 24, 24, jitter=0.05, seed=0)
-    P = plan_bands(band_planner, X, conn, band_elems=24 * 24 * 2)
+    P = plan_bands(band_planner, X, conn, band_elems=24 * 24 * 2, depth=3)
     assert P["R"] <= P["n_blocks"] / 2
     check_bands(P)
