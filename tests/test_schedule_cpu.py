@@ -314,8 +314,10 @@ def test_band_plan_items_and_ring(band_planner, case, band_elems, depth):
 
 
 def test_band_ring_stays_small_on_a_swept_mesh(band_planner):
-    """On a mesh numbered along a sweep the band ring holds a few bands of node rows, not the mesh."""
+    """On a mesh numbered along a sweep the band ring holds a few bands of node rows, not the mesh
+    (the live span; the ring is that span rounded up to a power of two)."""
     X, conn = meshgen.structured_box(24, 24, 24, jitter=0.05, seed=0)
     P = plan_bands(band_planner, X, conn, band_elems=24 * 24 * 2, depth=3)
-    assert P["R"] <= P["n_blocks"] / 2
+    rmax = 1 << int(np.ceil(np.log2(P["n_blocks"])))
+    assert P["span"] <= P["n_blocks"] / 2 and P["R"] < rmax
     check_bands(P)
