@@ -77,6 +77,7 @@ def lib():
         L.ceos_set_options.argtypes = [P, I]
         L.ceos_set_assembly.argtypes = [P, I]
         L.ceos_launch_count.argtypes = [P, I, ip]
+        L.ceos_test_stall_conversion.argtypes = [P, I, I]
         L.ceos_set_committed_time.argtypes = [P, D]
         L.ceos_kernel_time.argtypes = [P, C.POINTER(C.c_float)]
         L.ceos_destroy.argtypes = [P]
@@ -236,6 +237,11 @@ class ElementLoop:
         blocks in a ring of a few bands)."""
         _check(lib().ceos_set_assembly(self._h, _ASSEMBLY[mode]))
         self.assembly = mode
+
+    def test_stall_conversion(self, item, on=True):
+        """Failure-path test of the fused assembly: conversion item `item` waits for a flag that nothing
+        sets (its bounded wait runs out and the launch reports an error), or is restored (on=False)."""
+        _check(lib().ceos_test_stall_conversion(self._h, item, int(bool(on))))
 
     def launches_per_evaluation(self, tangent=True):
         """Kernels that one device-resident evaluation launches under the current assembly."""

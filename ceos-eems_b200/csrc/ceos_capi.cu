@@ -626,8 +626,10 @@ static int build_schedule(Handle* h) {
     CK(cudaMemcpy(h->d_conv, p.conv.data(), J * sizeof(int4), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&h->d_tile_wait, T * sizeof(int2)));
     CK(cudaMemcpy(h->d_tile_wait, p.tile_wait.data(), T * sizeof(int2), cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&h->d_flags, (T + J) * sizeof(unsigned)));
-    CK(cudaMemset(h->d_flags, 0, (T + J) * sizeof(unsigned)));
+    // tile and item flags, then one flag that nothing ever sets (ceos_test_stall_conversion)
+    CK(cudaMalloc(&h->d_flags, (T + J + 1) * sizeof(unsigned)));
+    CK(cudaMemset(h->d_flags, 0, (T + J + 1) * sizeof(unsigned)));
+    h->conv_host = p.conv;
     CK(cudaMalloc(&h->d_ticket, sizeof(unsigned)));
     CK(cudaMalloc(&h->d_sched_err, sizeof(int)));
     CK(cudaMemset(h->d_sched_err, 0, sizeof(int)));
@@ -967,6 +969,17 @@ extern "C" int ceos_set_options(void* handle, int options) {
         CK(cudaSetDevice(h->device));
         CK(cudaMalloc(&h->d_gp_stress, (size_t)6 * 8 * h->n_elem * h->elem_bytes()));
     }
+    return 0;
+}
+
+extern "C" int ceos_test_stall_conversion(void* handle, int item, int on) {
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || h->precision != CEOS_MIXED || item < 0 || item >= h->n_conv) return CEOS_E_ARG;
+    ConvItem c = h->conv_host[item];
+    if (on) c.t0 = c.t1 = h->n_tiles + h->n_conv;  // the tile-flag index of the sentinel flag
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(static_cast<int4*>(h->d_conv) + item, &c, sizeof(int4), cudaMemcpyHostToDevice));
     return 0;
 }
 

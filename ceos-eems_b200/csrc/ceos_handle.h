@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/ceos_gpu.h"
+#include "schedule.h"
 
 namespace ceos {
 
@@ -64,6 +65,7 @@ struct Handle {
     // fused assembly schedule (mixed mode with a tangent): a queue of element tiles and CSR
     // conversion items, split at the element slabs of the host-buffer evaluation
     std::vector<int> queue;               // >= 0 tile, < 0 conversion item -(j+1)
+    std::vector<ConvItem> conv_host;      // the planned conversion items (host copy)
     std::vector<int> slab_q;              // [n_slabs + 1] queue position where slab c starts
     int n_tiles = 0, n_conv = 0;
     uint32_t ring_blocks = 0;             // power of two; block b lives in slot b & (ring_blocks - 1)

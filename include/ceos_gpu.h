@@ -138,6 +138,10 @@ int ceos_set_assembly(void* handle, int mode);
 /* Kernel launches of one device-resident evaluation (with or without a tangent) under the current
  * assembly. */
 int ceos_launch_count(void* handle, int tangent, int* n_launches);
+/* Failure-path test of the fused assembly: on != 0 makes conversion item `item` wait for a flag that
+ * nothing sets, so its bounded wait (200 ms) runs out: the launch aborts, ceos_status reports
+ * CEOS_E_CUDA and the next evaluation clears the blocks; on = 0 restores the item. */
+int ceos_test_stall_conversion(void* handle, int item, int on);
 int ceos_set_committed_time(void* handle, double t);
 
 /* Release every device buffer and the stream. */
