@@ -67,8 +67,8 @@ class Surrogate:
             raise CeosError(rc, buf.value.decode())
 
     def set_gemm(self, path):
-        """128-wide layer GEMMs of training: "tcgen05" (tensor cores, TMEM accumulators; the default)
-        or "mma" (mma.sync on warps)."""
+        """128-wide layer GEMMs of training: "tcgen05" (the default: tensor cores, TMEM accumulators, the
+        four passes of 128 samples in one launch) or "mma" (mma.sync on warps, one launch per layer)."""
         self._check(self._L.ceos_sur_set_gemm(self._h, {"mma": 0, "tcgen05": 1}[path]))
 
     def set_params(self, theta):

@@ -10,9 +10,11 @@
 // Training fits the stress (a Sobolev loss on de/dx, L = (1/N) sum w_k (g_k - t_k)^2) by the
 // forward-over-reverse product d/dtheta (u.g), u = dL/dg, in four passes over the layers plus
 // the weight gradients, every 128-wide contraction on the tensor cores in BF16 with FP32
-// accumulation (mma.sync.m16n8k16): forward primal, backward primal (gives g and u), forward
-// tangent along u, backward tangent, then dW = a h^T + delta hdot^T.  FP32 master weights and
-// Adam; BF16 copies (and transposed copies) of W1..W4 are refreshed after every step.
+// accumulation: forward primal, backward primal (gives g and u), forward tangent along u,
+// backward tangent, then dW = a h^T + delta hdot^T.  The default path (tcgen05, TMEM
+// accumulators) runs the four passes of 128 samples in one CTA of one launch (grad_chain_kernel);
+// the mma.sync.m16n8k16 path launches one kernel per layer.  FP32 master weights and Adam; BF16
+// copies (and transposed copies) of W1..W4 are refreshed after every step.
 //
 // Inference (FP32, CUDA cores) gives S and the 6x6 tangent per point from one forward pass,
 // one backward pass and one forward pass of the Jacobians J_l = dz_l/dx accumulating
@@ -50,6 +52,11 @@ constexpr int kTab = 513;    // vf grid of the reference-state stress table
 
 __device__ __forceinline__ float softplus_f(float z) { return fmaxf(z, 0.f) + log1pf(expf(-fabsf(z))); }
 __device__ __forceinline__ float sigmoid_f(float z) { return 0.5f * (1.f + tanhf(0.5f * z)); }
+// Training epilogues: the same functions from the fast exponential and logarithm (relative error
+// about 1e-6, far below the BF16 rounding of the activations they produce); inference keeps the
+// accurate ones above.
+__device__ __forceinline__ float softplus_t(float z) { return fmaxf(z, 0.f) + __logf(1.f + __expf(-fabsf(z))); }
+__device__ __forceinline__ float sigmoid_t(float z) { return __fdividef(1.f, 1.f + __expf(-z)); }
 
 __device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], const uint32_t b[2]) {
     asm volatile(
@@ -60,6 +67,14 @@ __device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], const 
 }
 __device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
     return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+__device__ __forceinline__ uint4 pack_bf8(const float* x) {
+    uint4 u;
+    u.x = pack2(__float2bfloat16_rn(x[0]), __float2bfloat16_rn(x[1]));
+    u.y = pack2(__float2bfloat16_rn(x[2]), __float2bfloat16_rn(x[3]));
+    u.z = pack2(__float2bfloat16_rn(x[4]), __float2bfloat16_rn(x[5]));
+    u.w = pack2(__float2bfloat16_rn(x[6]), __float2bfloat16_rn(x[7]));
+    return u;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -81,7 +96,27 @@ struct LayerArgs {
     __nv_bfloat16* outb2;         // last layer: kFwd: delta_4 = sigma(z4) w5; kFwdT: a_4
     float* outf;                  // last layer kFwdT: hdot_4 in FP32 (for dw5)
     int last;                     // layer 4 (index 3)
+    unsigned char* smem_next;     // chain kernel: the next layer's activation operand in shared memory,
+                                  // written by the epilogue beside its global copy (null: global only)
+    int n0;                       // chain kernel: first sample of the CTA (row 0 of smem_next)
 };
+
+// The 16-byte row chunk of 8 consecutive outputs m0.. of sample n in the canonical K-major operand
+// layout (8-row x 16-byte core matrices, K chunks 128 bytes apart, 8-row groups 2048 bytes apart).
+__device__ __forceinline__ void st_next(const LayerArgs& A, int n, int m0, uint4 u) {
+    if (A.smem_next) {
+        const int r = n - A.n0;
+        *reinterpret_cast<uint4*>(A.smem_next + (r >> 3) * 2048 + (m0 >> 3) * 128 + (r & 7) * 16) = u;
+    }
+}
+// 8 BF16 outputs m0.. of sample n to global memory and, when they are the next layer's input, to its
+// shared-memory operand as well
+__device__ __forceinline__ void st_out8(const LayerArgs& A, __nv_bfloat16* dst, const float* x, int n, int m0,
+                                        bool next) {
+    const uint4 u = pack_bf8(x);
+    *reinterpret_cast<uint4*>(dst) = u;
+    if (next) st_next(A, n, m0, u);
+}
 
 template <int K, int EPI>
 __global__ void __launch_bounds__(128) layer_gemm_kernel(LayerArgs A) {
@@ -145,14 +180,14 @@ __global__ void __launch_bounds__(128) layer_gemm_kernel(LayerArgs A) {
                 if constexpr (EPI == kFwd) {
                     const float z = v + A.bias[m];
                     A.Z[o] = z;
-                    A.outb[o] = __float2bfloat16_rn(softplus_f(z));
-                    if (A.last) A.outb2[o] = __float2bfloat16_rn(sigmoid_f(z) * A.w5[m]);
+                    A.outb[o] = __float2bfloat16_rn(softplus_t(z));
+                    if (A.last) A.outb2[o] = __float2bfloat16_rn(sigmoid_t(z) * A.w5[m]);
                 } else if constexpr (EPI == kBwd) {
                     A.G[o] = v;
-                    A.outb[o] = __float2bfloat16_rn(sigmoid_f(A.Z[o]) * v);
+                    A.outb[o] = __float2bfloat16_rn(sigmoid_t(A.Z[o]) * v);
                 } else if constexpr (EPI == kFwdT) {
                     A.Zd[o] = v;
-                    const float s = sigmoid_f(A.Z[o]);
+                    const float s = sigmoid_t(A.Z[o]);
                     if (A.last) {
                         A.outf[o] = s * v;
                         A.outb2[o] = __float2bfloat16_rn(s * (1.f - s) * v * A.w5[m]);
@@ -160,7 +195,7 @@ __global__ void __launch_bounds__(128) layer_gemm_kernel(LayerArgs A) {
                         A.outb[o] = __float2bfloat16_rn(s * v);
                     }
                 } else {
-                    const float s = sigmoid_f(A.Z[o]);
+                    const float s = sigmoid_t(A.Z[o]);
                     A.outb[o] = __float2bfloat16_rn(s * v + s * (1.f - s) * A.Zd[o] * A.G[o]);
                 }
             }
@@ -201,17 +236,16 @@ __device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, boo
                  "r"(valid ? 16 : 0));
 }
 
+// The epilogue of 32 consecutive outputs m0..m0+31 of sample n: every FP32 input of the chunk (z,
+// zdot, G of the layer, as the pass needs) is loaded before any of it is used, so a chunk costs one
+// memory latency rather than one per group of 8 (the stores of a group could alias the loads of the
+// next, so the compiler cannot hoist them itself).
+template <int EPI>
+__device__ __forceinline__ void layer_epilogue32(const LayerArgs& A, int n, int m0, const float* v);
+
 template <int EPI>
 __device__ __forceinline__ void layer_epilogue8(const LayerArgs& A, int n, int m0, const float* v) {
     const size_t o = (size_t)n * kH + m0;
-    auto st_bf8 = [](__nv_bfloat16* dst, const float* x) {
-        uint4 u;
-        u.x = pack2(__float2bfloat16_rn(x[0]), __float2bfloat16_rn(x[1]));
-        u.y = pack2(__float2bfloat16_rn(x[2]), __float2bfloat16_rn(x[3]));
-        u.z = pack2(__float2bfloat16_rn(x[4]), __float2bfloat16_rn(x[5]));
-        u.w = pack2(__float2bfloat16_rn(x[6]), __float2bfloat16_rn(x[7]));
-        *reinterpret_cast<uint4*>(dst) = u;
-    };
     auto ld8 = [](const float* src, float* x) {
         const float4 a = *reinterpret_cast<const float4*>(src), b = *reinterpret_cast<const float4*>(src + 4);
         x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
@@ -227,20 +261,20 @@ __device__ __forceinline__ void layer_epilogue8(const LayerArgs& A, int n, int m
         for (int j = 0; j < 8; ++j) z[j] = v[j] + A.bias[m0 + j];
         st8(A.Z + o, z);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) a[j] = softplus_f(z[j]);
-        st_bf8(A.outb + o, a);
+        for (int j = 0; j < 8; ++j) a[j] = softplus_t(z[j]);
+        st_out8(A, A.outb + o, a, n, m0, !A.last);
         if (A.last) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) b[j] = sigmoid_f(z[j]) * A.w5[m0 + j];
-            st_bf8(A.outb2 + o, b);
+            for (int j = 0; j < 8; ++j) b[j] = sigmoid_t(z[j]) * A.w5[m0 + j];
+            st_out8(A, A.outb2 + o, b, n, m0, true);
         }
     } else if constexpr (EPI == kBwd) {
         float z[8];
         ld8(A.Z + o, z);
         st8(A.G + o, v);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) a[j] = sigmoid_f(z[j]) * v[j];
-        st_bf8(A.outb + o, a);
+        for (int j = 0; j < 8; ++j) a[j] = sigmoid_t(z[j]) * v[j];
+        st_out8(A, A.outb + o, a, n, m0, true);
     } else if constexpr (EPI == kFwdT) {
         float z[8];
         ld8(A.Z + o, z);
@@ -248,16 +282,16 @@ __device__ __forceinline__ void layer_epilogue8(const LayerArgs& A, int n, int m
         if (A.last) {
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const float sg = sigmoid_f(z[j]);
+                const float sg = sigmoid_t(z[j]);
                 a[j] = sg * v[j];
                 b[j] = sg * (1.f - sg) * v[j] * A.w5[m0 + j];
             }
             st8(A.outf + o, a);
-            st_bf8(A.outb2 + o, b);
+            st_out8(A, A.outb2 + o, b, n, m0, true);
         } else {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) a[j] = sigmoid_f(z[j]) * v[j];
-            st_bf8(A.outb + o, a);
+            for (int j = 0; j < 8; ++j) a[j] = sigmoid_t(z[j]) * v[j];
+            st_out8(A, A.outb + o, a, n, m0, true);
         }
     } else {
         float z[8], zd[8], g[8];
@@ -266,47 +300,118 @@ __device__ __forceinline__ void layer_epilogue8(const LayerArgs& A, int n, int m
         ld8(A.G + o, g);
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            const float sg = sigmoid_f(z[j]);
+            const float sg = sigmoid_t(z[j]);
             a[j] = sg * v[j] + sg * (1.f - sg) * zd[j] * g[j];
         }
-        st_bf8(A.outb + o, a);
+        st_out8(A, A.outb + o, a, n, m0, true);
     }
 }
 
 template <int EPI>
-__global__ void __launch_bounds__(128, 1) layer_umma_kernel(LayerArgs A, int* err) {
-    extern __shared__ __align__(1024) unsigned char sm_raw[];
-    unsigned char* As = sm_raw;                    // activations: [row group][k chunk][row][16 B]
-    unsigned char* Bs = sm_raw + kUmmaOpBytes;     // weights, same layout
-    __shared__ __align__(8) uint64_t mbar;
-    __shared__ uint32_t tmem_base;
-    __shared__ int s_fail;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int n0 = blockIdx.x * kUmmaRows;
-    // stage both operands: consecutive threads fill consecutive 16-byte rows of one core matrix
-    for (int c = tid; c < 128 * 16; c += 128) {
+__device__ __forceinline__ void layer_epilogue32(const LayerArgs& A, int n, int m0, const float* v) {
+    const size_t o = (size_t)n * kH + m0;
+    auto ld32 = [](const float* src, float* x) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float4 a = reinterpret_cast<const float4*>(src)[q];
+            x[4 * q] = a.x; x[4 * q + 1] = a.y; x[4 * q + 2] = a.z; x[4 * q + 3] = a.w;
+        }
+    };
+    auto st8 = [](float* dst, const float* x) {
+        *reinterpret_cast<float4*>(dst) = make_float4(x[0], x[1], x[2], x[3]);
+        *reinterpret_cast<float4*>(dst + 4) = make_float4(x[4], x[5], x[6], x[7]);
+    };
+    if constexpr (EPI == kFwd) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) layer_epilogue8<kFwd>(A, n, m0 + 8 * j, v + 8 * j);  // no loads but the bias
+    } else if constexpr (EPI == kBwd) {
+        float z[32];
+        ld32(A.Z + o, z);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float a[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) a[q] = sigmoid_t(z[8 * j + q]) * v[8 * j + q];
+            st8(A.G + o + 8 * j, v + 8 * j);
+            st_out8(A, A.outb + o + 8 * j, a, n, m0 + 8 * j, true);
+        }
+    } else if constexpr (EPI == kFwdT) {
+        float z[32];
+        ld32(A.Z + o, z);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float a[8], b[8];
+            st8(A.Zd + o + 8 * j, v + 8 * j);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float sg = sigmoid_t(z[8 * j + q]);
+                a[q] = sg * v[8 * j + q];
+                b[q] = A.last ? sg * (1.f - sg) * v[8 * j + q] * A.w5[m0 + 8 * j + q] : 0.f;
+            }
+            if (A.last) {
+                st8(A.outf + o + 8 * j, a);
+                st_out8(A, A.outb2 + o + 8 * j, b, n, m0 + 8 * j, true);
+            } else {
+                st_out8(A, A.outb + o + 8 * j, a, n, m0 + 8 * j, true);
+            }
+        }
+    } else {
+        float z[32], zd[32], g[32];
+        ld32(A.Z + o, z);
+        ld32(A.Zd + o, zd);
+        ld32(A.G + o, g);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float a[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = 8 * j + q;
+                const float sg = sigmoid_t(z[k]);
+                a[q] = sg * v[k] + sg * (1.f - sg) * zd[k] * g[k];
+            }
+            st_out8(A, A.outb + o + 8 * j, a, n, m0 + 8 * j, true);
+        }
+    }
+}
+
+// One 128-wide layer for the 128 samples n0.. of this CTA: stage the operands that are not in shared
+// memory yet (stage_a: the activations from A.in, stage_w: the weights from A.W), issue the MMAs from
+// one thread, wait for them (bounded; the MMA barrier completes once per layer, so the layer waits for
+// phase `phase`), start fetching the next layer's weights W_next into Bs (free once the MMAs are done),
+// run the epilogue from TMEM (which writes the next layer's activations into As when A.smem_next is
+// set).  Returns false, with every thread agreeing, when the wait ran out.  On return every thread has
+// finished with TMEM and its writes are visible to the CTA.
+constexpr int kChainThreads = 256;  // two threads per sample: warps w and w + 4 read the same TMEM lanes
+
+__device__ __forceinline__ void stage_weights(unsigned char* Bs, const __nv_bfloat16* W) {
+    for (int c = threadIdx.x; c < 128 * 16; c += kChainThreads) {
         const int r8 = c & 7, q = (c >> 3) & 15, g = c >> 7, r = 8 * g + r8;
-        const int off = g * 2048 + q * 128 + r8 * 16;
-        const bool valid = n0 + r < A.n;
-        cp_async16_zfill(As + off, A.in + (size_t)(valid ? n0 + r : 0) * kH + q * 8, valid);
-        cp_async16_zfill(Bs + off, A.W + (size_t)r * kH + q * 8, true);
+        cp_async16_zfill(Bs + g * 2048 + q * 128 + r8 * 16, W + (size_t)r * kH + q * 8, true);
     }
     asm volatile("cp.async.commit_group;\n" ::);
-    if (warp == 0) {  // 128 TMEM columns of 32-bit accumulators for the 128 outputs
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;\n" ::"r"(smem_addr(&tmem_base)));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+}
+
+template <int EPI>
+__device__ bool umma_layer(const LayerArgs& A, int n0, unsigned char* As, unsigned char* Bs, uint32_t tmem,
+                           uint64_t* mbar, uint32_t phase, int* s_fail, bool stage_a, bool stage_w,
+                           const __nv_bfloat16* W_next) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // staging: consecutive threads fill consecutive 16-byte rows of one core matrix
+    if (stage_a) {
+        for (int c = tid; c < 128 * 16; c += kChainThreads) {
+            const int r8 = c & 7, q = (c >> 3) & 15, g = c >> 7, r = 8 * g + r8;
+            const bool valid = n0 + r < A.n;
+            cp_async16_zfill(As + g * 2048 + q * 128 + r8 * 16, A.in + (size_t)(valid ? n0 + r : 0) * kH + q * 8,
+                             valid);
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
     }
-    if (tid == 0) {
-        s_fail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(&mbar)));
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
-    }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (stage_w) stage_weights(Bs, A.W);
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // also the weights prefetched by the previous layer
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // generic-proxy writes -> tensor core reads
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const uint32_t tmem = tmem_base;
     if (tid == 0) {
         const uint32_t a0 = smem_addr(As), b0 = smem_addr(Bs);
 #pragma unroll
@@ -319,22 +424,22 @@ __global__ void __launch_bounds__(128, 1) layer_umma_kernel(LayerArgs A, int* er
                 ::"r"(tmem), "l"(ad), "l"(bd), "r"(kUmmaIdesc), "r"(acc));
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
-                     ::"r"(smem_addr(&mbar)) : "memory");
+                     ::"r"(smem_addr(mbar)) : "memory");
     }
-    // wait for the MMAs (phase 0 of the barrier), bounded
-    {
-        const unsigned long long t0 = [] { unsigned long long t; asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t)); return t; }();
+    {  // wait for the MMAs, bounded
+        unsigned long long t0;
+        asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t0));
         uint32_t done = 0;
         while (!done) {
             asm volatile(
-                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                 "selp.u32 %0, 1, 0, p;\n\t}\n"
-                : "=r"(done) : "r"(smem_addr(&mbar)) : "memory");
+                : "=r"(done) : "r"(smem_addr(mbar)), "r"(phase) : "memory");
             if (!done) {
                 unsigned long long t;
                 asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
                 if (t - t0 > kUmmaWaitNs) {
-                    atomicOr(&s_fail, 1);
+                    atomicOr(s_fail, 1);
                     break;
                 }
             }
@@ -342,38 +447,56 @@ __global__ void __launch_bounds__(128, 1) layer_umma_kernel(LayerArgs A, int* er
     }
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     __syncthreads();
-    if (s_fail) {
-        if (tid == 0) atomicOr(err, 1);
-    } else {
-        const int n = n0 + 32 * warp + lane;   // TMEM lane = sample row; warp w reads lanes 32w..32w+31
+    if (*reinterpret_cast<volatile int*>(s_fail)) return false;
+    if (W_next) stage_weights(Bs, W_next);  // the MMAs have read Bs: fetch the next weights during the epilogue
+    // TMEM lane = sample row: warp w reads lanes 32 (w & 3) .. + 31 (its lane quadrant), columns
+    // 64 (w >> 2) .. + 63 (its half of the outputs)
+    const int quad = warp & 3, half = warp >> 2;
+    const int n = n0 + 32 * quad + lane;
 #pragma unroll 1
-        for (int c = 0; c < kH / 32; ++c) {
-            uint32_t r[32];
-            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + 32 * c;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-            if (n < A.n) {
+    for (int c = 2 * half; c < 2 * half + 2; ++c) {
+        uint32_t r[32];
+        const uint32_t taddr = tmem + ((uint32_t)(32 * quad) << 16) + 32 * c;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+              "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+              "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+              "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (n < A.n) {
+            float v[32];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    float v[8];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) v[q] = __uint_as_float(r[8 * j + q]);
-                    layer_epilogue8<EPI>(A, n, 32 * c + 8 * j, v);
-                }
-            }
+            for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
+            layer_epilogue32<EPI>(A, n, 32 * c, v);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();  // TMEM read out and the epilogue's global writes done before the next layer
+    return true;
+}
+
+// TMEM columns and the MMA barrier of a CTA running umma_layer: set up / released by warp 0 and
+// thread 0 (the caller syncs after setup).
+__device__ void umma_setup(uint32_t* tmem_base, uint64_t* mbar, int* s_fail) {
+    const int tid = threadIdx.x;
+    if ((tid >> 5) == 0) {  // 128 TMEM columns of 32-bit accumulators for the 128 outputs
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;\n" ::"r"(smem_addr(tmem_base)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        *s_fail = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    }
+}
+__device__ void umma_release(uint32_t tmem) {
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
-    if (warp == 0) {
+    if ((threadIdx.x >> 5) == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;\n" ::"r"(tmem));
     }
@@ -398,7 +521,7 @@ __global__ void seed_kernel(int n, const float* theta, const float* Z0, const fl
         const float ws = sw[s];  // per-sample weight
         float gk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         for (int m = 0; m < kH; ++m) {
-            const float d = sigmoid_f(Z0[(size_t)s * kH + m]) * G0[(size_t)s * kH + m];
+            const float d = sigmoid_t(Z0[(size_t)s * kH + m]) * G0[(size_t)s * kH + m];
 #pragma unroll
             for (int k = 0; k < 6; ++k) gk[k] += W1s[k * kH + m] * d;
         }
@@ -421,6 +544,204 @@ __global__ void seed_kernel(int n, const float* theta, const float* Z0, const fl
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
         atomicAdd(loss, tot * inv_n);
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The per-sample part of one gradient evaluation in one launch (tcgen05 path).  CTA = 128 threads
+// = 128 samples; everything up to the weight gradients is per sample, so a CTA runs it for its own
+// samples without waiting for any other CTA: forward primal, backward primal, stress seed, forward
+// tangent, backward tangent.  Layer 1 (7 inputs padded to 16) runs on the CUDA cores from the same
+// BF16 operands the tensor cores would read (products exact in FP32, FP32 sums); the twelve 128-wide
+// layers run as umma_layer, each reusing the CTA's TMEM columns and MMA barrier.  Intermediates go
+// to the same global arrays as the per-layer launches of the mma.sync path (the weight-gradient
+// kernels read them afterwards, and later layers of this CTA read them back through L2).
+// ---------------------------------------------------------------------------------------------
+struct ChainArgs {
+    int n;
+    size_t BH;                              // stride of the per-layer activation arrays (cap x 128)
+    const float* theta;                     // FP32 master parameters (biases, w5, W1 for the seed)
+    const __nv_bfloat16 *X0, *Wb1, *Wb, *WbT;
+    float *Z, *Zd, *G, *Hd4;
+    __nv_bfloat16 *Hb, *Hd, *Db, *Ab, *U0;
+    const float *T, *w6, *Sw;
+    float inv_n;
+    double* loss;
+};
+
+// Layer 1 for sample s: out[m] = sum_k W1b[m][k] in[s][k] (BF16 values, FP32 arithmetic), then the
+// pass's epilogue on 8 outputs at a time.
+template <int EPI>
+__device__ void layer1_sample(const LayerArgs& A, const float* W1f, int s, int m_begin, int m_end) {
+    if (s >= A.n) return;
+    float x[kInPad];
+    const uint4* src = reinterpret_cast<const uint4*>(A.in + (size_t)s * kInPad);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const uint4 u = src[h];
+        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            x[8 * h + 2 * q] = __bfloat162float(__ushort_as_bfloat16((unsigned short)(w[q] & 0xffffu)));
+            x[8 * h + 2 * q + 1] = __bfloat162float(__ushort_as_bfloat16((unsigned short)(w[q] >> 16)));
+        }
+    }
+#pragma unroll 1
+    for (int m0 = m_begin; m0 < m_end; m0 += 8) {
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            float acc = 0.f;
+#pragma unroll
+            for (int k = 0; k < kInPad; ++k) acc = fmaf(W1f[(m0 + j) * kInPad + k], x[k], acc);
+            v[j] = acc;
+        }
+        layer_epilogue8<EPI>(A, s, m0, v);
+    }
+}
+
+// Stress seed of sample s (seed_kernel's arithmetic): g = W1^T (sigma(z1) G_1) in FP32, residuals
+// against the targets, u = dL/dg into the padded BF16 tangent input; returns the sample's loss term.
+__device__ double seed_sample(const ChainArgs& C, const float* W1m, int s) {
+    if (s >= C.n) return 0.0;
+    const float ws = C.Sw[s];
+    float gk[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float* z0 = C.Z + (size_t)s * kH;
+    const float* g0 = C.G + (size_t)s * kH;
+    for (int m = 0; m < kH; ++m) {
+        const float d = sigmoid_t(z0[m]) * g0[m];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) gk[k] += W1m[k * kH + m] * d;
+    }
+    double part = 0.0;
+#pragma unroll
+    for (int k = 0; k < kInPad; ++k) {
+        float u = 0.f;
+        if (k < 6) {
+            const float r = gk[k] - C.T[(size_t)s * 6 + k];
+            part += (double)ws * C.w6[k] * r * r;
+            u = 2.f * ws * C.w6[k] * r * C.inv_n;
+        }
+        C.U0[(size_t)s * kInPad + k] = __float2bfloat16_rn(u);
+    }
+    return part;
+}
+
+__global__ void __launch_bounds__(kChainThreads, 1) grad_chain_kernel(ChainArgs C, int* err) {
+    extern __shared__ __align__(1024) unsigned char sm_raw[];
+    unsigned char* As = sm_raw;                 // activations operand
+    unsigned char* Bs = sm_raw + kUmmaOpBytes;  // weights operand
+    __shared__ float W1f[kH * kInPad];          // BF16 W1 (padded to 16 inputs) as floats, [m][k]
+    __shared__ float W1m[6 * kH];               // FP32 master W1 of the stress inputs, [k][m]
+    __shared__ double red[kChainThreads / 32];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int s_fail;
+    // thread t: sample n0 + (t & 127), output half t >> 7 (layer 1); the seed runs on t < 128
+    const int tid = threadIdx.x, n0 = blockIdx.x * kUmmaRows, s = n0 + (tid & 127);
+    const int m_begin = (tid >> 7) * (kH / 2), m_end = m_begin + kH / 2;
+    umma_setup(&tmem_base, &mbar, &s_fail);
+    for (int i = tid; i < kH * kInPad; i += kChainThreads) W1f[i] = __bfloat162float(C.Wb1[i]);
+    for (int i = tid; i < kH * kIn; i += kChainThreads) {
+        const int m = i / kIn, k = i - m * kIn;
+        if (k < 6) W1m[k * kH + m] = C.theta[oW1 + i];
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    uint32_t phase = 0;
+    bool ok = true;
+    LayerArgs L{};
+    L.n = C.n;
+    L.w5 = C.theta + oW5;
+    L.smem_next = As;  // every epilogue (and layer 1) leaves its output in As as the next layer's operand
+    L.n0 = n0;
+    // the weights of the 12 tensor-core layers in order; layer k fetches those of layer k + 1 into Bs
+    // while its epilogue runs, so only the first layer stages weights itself and no layer stages
+    // activations
+    auto W_of = [&](int k) -> const __nv_bfloat16* {
+        if (k >= 12) return nullptr;
+        const int q = k % 6;  // 0..2: W2..W4 (forward), 3..5: transposed W4..W2 (backward)
+        return q < 3 ? C.Wb + (size_t)q * kH * kH : C.WbT + (size_t)(5 - q) * kH * kH;
+    };
+    int k = 0;
+    // forward primal
+    L.in = C.X0;
+    L.bias = C.theta + layer_b(0);
+    L.Z = C.Z;
+    L.outb = C.Hb;
+    L.last = 0;
+    layer1_sample<kFwd>(L, W1f, s, m_begin, m_end);
+    __syncthreads();
+    for (int l = 1; l < 4 && ok; ++l, phase ^= 1) {
+        L.W = C.Wb + (size_t)(l - 1) * kH * kH;
+        L.in = C.Hb + (l - 1) * C.BH;
+        L.bias = C.theta + layer_b(l);
+        L.Z = C.Z + l * C.BH;
+        L.outb = C.Hb + l * C.BH;
+        L.outb2 = C.Db + 3 * C.BH;
+        L.last = l == 3;
+        ok = umma_layer<kFwd>(L, n0, As, Bs, tmem, &mbar, phase, &s_fail, false, k == 0, W_of(k + 1));
+        ++k;
+    }
+    // backward primal: G_l = W_{l+1}^T delta_{l+1}, delta_l
+    for (int l = 2; l >= 0 && ok; --l, phase ^= 1) {
+        L.W = C.WbT + (size_t)l * kH * kH;
+        L.in = C.Db + (l + 1) * C.BH;
+        L.Z = C.Z + l * C.BH;
+        L.G = C.G + l * C.BH;
+        L.outb = C.Db + l * C.BH;
+        L.last = 0;
+        ok = umma_layer<kBwd>(L, n0, As, Bs, tmem, &mbar, phase, &s_fail, false, k == 0, W_of(k + 1));
+        ++k;
+    }
+    if (ok) {
+        double part = tid < 128 ? seed_sample(C, W1m, s) : 0.0;
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if ((tid & 31) == 0) red[tid >> 5] = part;
+        __syncthreads();
+        if (tid == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < kChainThreads / 32; ++w) tot += red[w];
+            atomicAdd(C.loss, tot * C.inv_n);
+        }
+        // forward tangent along u
+        L.in = C.U0;
+        L.Z = C.Z;
+        L.Zd = C.Zd;
+        L.outb = C.Hd;
+        L.outb2 = C.Ab + 3 * C.BH;
+        L.outf = C.Hd4;
+        L.last = 0;
+        layer1_sample<kFwdT>(L, W1f, s, m_begin, m_end);
+        __syncthreads();
+    }
+    for (int l = 1; l < 4 && ok; ++l, phase ^= 1) {
+        L.W = C.Wb + (size_t)(l - 1) * kH * kH;
+        L.in = C.Hd + (l - 1) * C.BH;
+        L.Z = C.Z + l * C.BH;
+        L.Zd = C.Zd + l * C.BH;
+        L.outb = C.Hd + l * C.BH;
+        L.outb2 = C.Ab + 3 * C.BH;
+        L.outf = C.Hd4;
+        L.last = l == 3;
+        ok = umma_layer<kFwdT>(L, n0, As, Bs, tmem, &mbar, phase, &s_fail, false, k == 0, W_of(k + 1));
+        ++k;
+    }
+    // backward tangent: a_l from W_{l+1}^T a_{l+1}
+    for (int l = 2; l >= 0 && ok; --l, phase ^= 1) {
+        L.W = C.WbT + (size_t)l * kH * kH;
+        L.in = C.Ab + (l + 1) * C.BH;
+        L.Z = C.Z + l * C.BH;
+        L.Zd = C.Zd + l * C.BH;
+        L.G = C.G + l * C.BH;
+        L.outb = C.Ab + l * C.BH;
+        L.last = 0;
+        ok = umma_layer<kBwdT>(L, n0, As, Bs, tmem, &mbar, phase, &s_fail, false, k == 0, W_of(k + 1));
+        ++k;
+    }
+    if (!ok && tid == 0) atomicOr(err, 1);
+    umma_release(tmem);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -938,14 +1259,13 @@ __global__ void pack_inputs_kernel(int n, const float* X, __nv_bfloat16* X0) {
     X0[i] = __float2bfloat16_rn(k < kIn ? X[(size_t)s * kIn + k] : 0.f);
 }
 
-// One 128-wide layer GEMM (K = 128) on the selected path.
+// One 128-wide layer GEMM (K = 128) of the mma.sync path.
 template <int EPI>
 void launch_layer(Sur* s, const LayerArgs& L, int n, cudaStream_t st) {
-    if (s->gemm_path == 1)
-        layer_umma_kernel<EPI><<<(n + kUmmaRows - 1) / kUmmaRows, 128, 2 * kUmmaOpBytes, st>>>(L, s->err);
-    else
-        layer_gemm_kernel<kH, EPI><<<(n + kTileN - 1) / kTileN, 128, 0, st>>>(L);
+    layer_gemm_kernel<kH, EPI><<<(n + kTileN - 1) / kTileN, 128, 0, st>>>(L);
 }
+
+int weight_grads(Sur* s, int n, cudaStream_t st);
 
 // One gradient evaluation over n <= cap samples already on the device (X [n][7], T [n][6]):
 // accumulates dL/dtheta into s->grad and the loss into s->loss.
@@ -953,6 +1273,32 @@ int grad_device(Sur* s, int n, const float* dX) {
     cudaStream_t st = s->stream;
     const size_t BH = (size_t)s->cap * kH;
     pack_inputs_kernel<<<(n * kInPad + 255) / 256, 256, 0, st>>>(n, dX, s->X0);
+    if (s->gemm_path == 1) {  // tcgen05: the per-sample chain in one launch, then the weight gradients
+        ChainArgs C{};
+        C.n = n;
+        C.BH = BH;
+        C.theta = s->theta;
+        C.X0 = s->X0;
+        C.Wb1 = s->Wb1;
+        C.Wb = s->Wb;
+        C.WbT = s->WbT;
+        C.Z = s->Z;
+        C.Zd = s->Zd;
+        C.G = s->G;
+        C.Hd4 = s->Hd4;
+        C.Hb = s->Hb;
+        C.Hd = s->Hd;
+        C.Db = s->Db;
+        C.Ab = s->Ab;
+        C.U0 = s->U0;
+        C.T = s->T;
+        C.w6 = s->w6;
+        C.Sw = s->Sw;
+        C.inv_n = 1.f / n;
+        C.loss = s->loss;
+        grad_chain_kernel<<<(n + kUmmaRows - 1) / kUmmaRows, kChainThreads, 2 * kUmmaOpBytes, st>>>(C, s->err);
+        return weight_grads(s, n, st);
+    }
     const int nb = (n + kTileN - 1) / kTileN;
     LayerArgs L{};
     L.n = n;
@@ -1015,7 +1361,12 @@ int grad_device(Sur* s, int n, const float* dX) {
         L.last = 0;
         launch_layer<kBwdT>(s, L, n, st);
     }
-    // weight gradients
+    return weight_grads(s, n, st);
+}
+
+// dW_l = a_l h_{l-1}^T + delta_l hdot_{l-1}^T and the bias gradients, over all n samples.
+int weight_grads(Sur* s, int n, cudaStream_t st) {
+    const size_t BH = (size_t)s->cap * kH;
     GradArgs G{};
     G.n = n;
     for (int l = 0; l < 4; ++l) {
@@ -1083,14 +1434,8 @@ extern "C" int ceos_sur_create(int batch_max, int device, void** handle) {
     al((void**)&s->ctr, sizeof(int) * 2);
     al((void**)&s->err, sizeof(int));
     if (ok)
-        ok = cudaFuncSetAttribute(layer_umma_kernel<kFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kUmmaOpBytes) ==
-                 cudaSuccess &&
-             cudaFuncSetAttribute(layer_umma_kernel<kBwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kUmmaOpBytes) ==
-                 cudaSuccess &&
-             cudaFuncSetAttribute(layer_umma_kernel<kFwdT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kUmmaOpBytes) ==
-                 cudaSuccess &&
-             cudaFuncSetAttribute(layer_umma_kernel<kBwdT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kUmmaOpBytes) ==
-                 cudaSuccess;
+        ok = cudaFuncSetAttribute(grad_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kUmmaOpBytes) ==
+             cudaSuccess;
     if (ok) {
         __nv_bfloat16* ap[4] = {s->Ab, s->Ab + BH, s->Ab + 2 * BH, s->Ab + 3 * BH};
         ok = cudaMemcpy(s->Aptr, ap, sizeof(ap), cudaMemcpyHostToDevice) == cudaSuccess;

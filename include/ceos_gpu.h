@@ -224,8 +224,9 @@ int ceos_sur_material_device(void* handle, int n_elem, const double* F, long lon
  * stress: the undeformed state becomes stress-free, the tangent is unchanged. */
 int ceos_sur_set_reference(void* handle, double vf_lo, double vf_hi);
 int ceos_sur_message(void* handle, char* msg, int msg_len);
-/* The 128-wide layer GEMMs of training: path 1 (the default) tcgen05 tensor cores (128 samples x
- * 128 outputs per CTA, accumulators in tensor memory), path 0 mma.sync on warps. */
+/* The 128-wide layer GEMMs of training: path 1 (the default) tcgen05 tensor cores, the four passes of
+ * 128 samples in one CTA of one launch (accumulators in tensor memory), path 0 mma.sync on warps, one
+ * launch per layer.  Both give the same gradient up to FP32 summation order. */
 int ceos_sur_set_gemm(void* handle, int path);
 void ceos_sur_destroy(void* handle);
 
