@@ -75,7 +75,7 @@ void model_init_state(int model, double* st) {
     } while (0)
 
 template <typename T>
-size_t elem_smem(const Handle* h) { return SmemLayout<T>(h->ns_used).total; }
+size_t elem_smem(const Handle* h) { return SmemLayout<T>(h->ns_used, h->param_mode == 1 ? h->n_params : 0).total; }
 
 // Streams and events of the banded assembly, created at its first evaluation.
 int ensure_band_streams(Handle* h) {
@@ -121,6 +121,7 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
     a.st_new = reinterpret_cast<T*>(h->d_state[1 - h->cur_old]);
     a.ld = h->ld;
     a.ns_used = h->ns_used;
+    a.n_pe = h->param_mode == 1 ? h->n_params : 0;
     a.params = reinterpret_cast<const T*>(h->d_params);
     a.param_mode = h->param_mode;
     a.n_params = h->n_params;

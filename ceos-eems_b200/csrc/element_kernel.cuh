@@ -77,6 +77,7 @@ struct ElemArgs {
     T* st_new;
     int ld;                 // leading dimension of the state arrays (n_elem rounded up to 32)
     int ns_used;            // state variables the model reads and writes
+    int n_pe;               // per-element parameters staged per tile (n_params when param_mode 1, else 0)
     const T* params;        // see param_mode
     int param_mode;         // 0 uniform (pu[]); 1 per element params[k*n_elem+e]; 2 per material
     int n_params;
@@ -108,8 +109,8 @@ struct ElemArgs {
 // prefetched with cp.async while the current tile computes (software pipeline).
 template <typename T>
 struct SmemLayout {
-    size_t g, ds, st, x, u, xf, rs, nup, node, ranks, status, kd, total;
-    CEOS_HD explicit SmemLayout(int ns) {
+    size_t g, ds, st, x, u, xf, rs, nup, node, ranks, status, kd, pe, total;
+    CEOS_HD SmemLayout(int ns, int npe) {
         size_t o = 0;
         auto take = [&](size_t bytes) { size_t r = o; o += (bytes + 15) & ~size_t(15); return r; };
         g = take(sizeof(T) * 8 * 8 * kTileE * 4);        // [gp][node][e][4]: grad N (current)
@@ -127,6 +128,7 @@ struct SmemLayout {
         ranks = take(sizeof(uint32_t) * 2 * kTileE * 8); // [buf][e][8]
         status = take(sizeof(int) * kTileE);
         kd = take(sizeof(double) * kTileE);              // [e] Mean Dilatation: d2psi/dJbar2 / V0
+        pe = take(sizeof(T) * (size_t)(npe > 0 ? npe : 1) * kTileE);  // [k][e] per-element parameters
         total = o;
     }
 };
@@ -140,7 +142,7 @@ static_assert((kStageDoubles + 2) * 8 + 3 * kConvNodes * (int)sizeof(int) <= kSt
 
 template <typename T>
 struct SmemPtrs {
-    T *g, *ds, *st, *kd;
+    T *g, *ds, *st, *kd, *pe;
     double *x, *u;
     float* xf;
     long long* rs;
@@ -149,6 +151,7 @@ struct SmemPtrs {
     CEOS_D SmemPtrs(unsigned char* raw, const SmemLayout<T>& L)
         : g(reinterpret_cast<T*>(raw + L.g)), ds(reinterpret_cast<T*>(raw + L.ds)),
           st(reinterpret_cast<T*>(raw + L.st)), kd(reinterpret_cast<T*>(raw + L.kd)),
+          pe(reinterpret_cast<T*>(raw + L.pe)),
           x(reinterpret_cast<double*>(raw + L.x)), u(reinterpret_cast<double*>(raw + L.u)),
           xf(reinterpret_cast<float*>(raw + L.xf)), rs(reinterpret_cast<long long*>(raw + L.rs)),
           nup(reinterpret_cast<int*>(raw + L.nup)), node(reinterpret_cast<int*>(raw + L.node)),
@@ -279,7 +282,7 @@ CEOS_D void prefetch_conn(const ElemArgs<T>& a, int e0, int* node_s, uint32_t* r
 // tile whose node ids are already in node_s (async).
 template <typename T>
 CEOS_D void prefetch_nodes_state(const ElemArgs<T>& a, int e0, const int* node_s, double* xs, double* us,
-                                 long long* rs_s, int* nup_s, T* st_s, int t) {
+                                 long long* rs_s, int* nup_s, T* st_s, int t, T* pe_s) {
     const int lane = t & 31, n = t >> 5;
     if (e0 + lane < a.e_end) {
         const int node = node_s[n * kTileE + lane];
@@ -303,6 +306,14 @@ CEOS_D void prefetch_nodes_state(const ElemArgs<T>& a, int e0, const int* node_s
         for (int c = t; c < total; c += kThreads) {
             const int row = c / cpr, part = c - row * cpr;   // row = v*8 + gp
             cp_async16(st_s + row * kTileE + part * per_chunk, a.st_old + (size_t)row * a.ld + e0 + part * per_chunk);
+        }
+    }
+    // per-element parameters [k][e] (rows of params[k * n_elem + e], not 16-byte aligned in general)
+    for (int c = t; c < a.n_pe * kTileE; c += kThreads) {
+        const int k = c / kTileE, el = c - k * kTileE;
+        if (e0 + el < a.e_end) {
+            if constexpr (sizeof(T) == 4) cp_async4(pe_s + c, a.params + (size_t)k * a.n_elem + e0 + el);
+            else cp_async8(pe_s + c, a.params + (size_t)k * a.n_elem + e0 + el);
         }
     }
 }
@@ -401,7 +412,7 @@ CEOS_D void phase_a(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
         if (a.param_mode == 0) p[k] = a.pu[k];
-        else if (a.param_mode == 1) p[k] = a.params[(size_t)k * a.n_elem + e];
+        else if (a.param_mode == 1) p[k] = s.pe[k * kTileE + el];  // staged with the tile's state
         else p[k] = a.params[(size_t)__ldg(a.mat_id + e) * a.n_params + k];
     }
     StateIO<T> io{s.st + gp * kTileE + el, a.st_new, (size_t)8 * a.ld, (size_t)gp * a.ld + e};
@@ -766,7 +777,7 @@ CEOS_D void phase_b(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp
 template <typename T, int MODEL, int SCATTER = SCATTER_CSR64>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop_kernel(ElemArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const SmemLayout<T> L(a.ns_used);
+    const SmemLayout<T> L(a.ns_used, a.n_pe);
     const SmemPtrs<T> s(smem_raw, L);
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
@@ -781,7 +792,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
     if (t < kTileE) s.status[t] = 0;
     cp_wait_all();
     __syncthreads();
-    prefetch_nodes_state(a, a.e_begin + tile * kTileE, s.node, s.x, s.u, s.rs, s.nup, s.st, t);
+    prefetch_nodes_state(a, a.e_begin + tile * kTileE, s.node, s.x, s.u, s.rs, s.nup, s.st, t, s.pe);
     cp_commit();
 
     for (int it = 0; tile < n_tiles; ++it, tile += gridDim.x) {
@@ -801,7 +812,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
         __syncthreads();  // phase A results visible; x, u and state buffers are free
         if (next < n_tiles) {
             prefetch_nodes_state(a, e0n, s.node + (buf ^ 1) * NB, s.x, s.u, s.rs + (buf ^ 1) * NB,
-                                 s.nup + (buf ^ 1) * NB, s.st, t);
+                                 s.nup + (buf ^ 1) * NB, s.st, t, s.pe);
             cp_commit();
         }
         tile_status(a, s, e0, t);
@@ -915,7 +926,7 @@ __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item[2];
     __shared__ int s_abort;
-    const SmemLayout<float> L(a.ns_used);
+    const SmemLayout<float> L(a.ns_used, a.n_pe);
     const SmemPtrs<float> s(smem_raw, L);
     double* stage = reinterpret_cast<double*>(smem_raw + L.g);  // g and ds are contiguous
     int* conv_info = reinterpret_cast<int*>(stage + kStageDoubles + 2);
@@ -946,7 +957,7 @@ __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<
         cp_commit();
         cp_wait_all();
         __syncthreads();
-        prefetch_nodes_state(a, cur * kTileE, s.node, s.x, s.u, s.rs, s.nup, s.st, t);
+        prefetch_nodes_state(a, cur * kTileE, s.node, s.x, s.u, s.rs, s.nup, s.st, t, s.pe);
         cp_commit();
     }
     while (cur != kEndItem) {
@@ -974,7 +985,7 @@ __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<
             if (s_abort) break;
             if (next >= 0) {
                 prefetch_nodes_state(a, next * kTileE, s.node + nb * NB, s.x, s.u, s.rs + nb * NB, s.nup + nb * NB,
-                                     s.st, t);
+                                     s.st, t, s.pe);
                 cp_commit();
             }
             tile_status(a, s, e0, t);
@@ -1005,7 +1016,7 @@ __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<
             if (s_abort) break;
             if (next >= 0) {
                 prefetch_nodes_state(a, next * kTileE, s.node + buf * NB, s.x, s.u, s.rs + buf * NB, s.nup + buf * NB,
-                                     s.st, t);
+                                     s.st, t, s.pe);
                 cp_commit();
             }
             convert_rows<1>(a, c.x, c.y, stage, conv_info, t);  // one block in flight: no spills here
