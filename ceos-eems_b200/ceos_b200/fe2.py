@@ -16,6 +16,7 @@ def _setup():
     L.ceos_fe2_message.argtypes = [P, C.c_char_p, I]
     L.ceos_fe2_set_increments.argtypes = [P, I]
     L.ceos_fe2_set_allow_failures.argtypes = [P, I]
+    L.ceos_fe2_set_device_rounds.argtypes = [P, I]
     L.ceos_fe2_set_fractions.argtypes = [P, P]
     L.ceos_fe2_set_warm_start.argtypes = [P, I]
     L.ceos_fe2_set_solver_ctas.argtypes = [P, I]
@@ -69,6 +70,11 @@ class BatchedRVE:
         """RVEs that cannot converge come back as NaN (and newton_iters -1) instead of raising."""
         _check(lib().ceos_fe2_set_allow_failures(self._h, 1 if allow else 0))
         self._allow = allow
+
+    def set_device_rounds(self, on=True):
+        """Run every Newton round of a solve on the device (the default: one CUDA graph with a WHILE node,
+        launched once per solve), or (on=False) take the per-RVE decisions on the host between rounds."""
+        _check(lib().ceos_fe2_set_device_rounds(self._h, 1 if on else 0))
 
     def set_solver_ctas(self, n=0):
         """RVEs the MINRES kernel keeps in flight (0: as many as occupancy allows)."""

@@ -58,10 +58,23 @@ struct Fe2 {
     int* hp_need = nullptr;              // pinned [n_rve]
     int* hp_cgi = nullptr;               // pinned [n_rve]
     int* hp_status = nullptr;            // pinned [1] failed elements of the last assembly
+    // device-resident rounds (ceos_fe2_set_device_rounds): the whole continuation is one graph, a WHILE
+    // node whose body is one round (Fbar, assembly, failure flags, residual norms, the per-RVE decisions,
+    // operations, linear solve, Newton step); the decision kernel keeps each RVE's continuation state on
+    // the device and the last kernel of the body sets the loop condition
+    int device_rounds = 1;
+    cudaGraphExec_t g_rounds = nullptr;
+    int* d_rs_int = nullptr;      // [8][n_rve] phase, nit, halv, cuts, its, cg_tot, spare, spare
+    double* d_rs_dbl = nullptr;   // [6][n_rve] a_done, da, a_try, r0, racc, spare
+    double* d_Fp = nullptr;       // [n_rve*9] start of each RVE's path
+    double* d_Ft = nullptr;       // [n_rve*9] target Fbar
+    int* d_rctl = nullptr;        // [4] rounds run, RVEs still in Newton this round, abort flag, RVE that aborted
+    double* d_rpar = nullptr;     // [4] tol, force floor, max_newton, max_rounds (read by the round kernels)
     void drop_graphs() {
         if (g_assemble) cudaGraphExecDestroy(g_assemble);
         if (g_solve) cudaGraphExecDestroy(g_solve);
-        g_assemble = g_solve = nullptr;
+        if (g_rounds) cudaGraphExecDestroy(g_rounds);
+        g_assemble = g_solve = g_rounds = nullptr;
     }
     int warm = 0;                        // 1: continue every RVE from its last converged state
     std::vector<double> F_prev;          // [n_rve][9] Fbar of the last converged state (warm start)
@@ -116,7 +129,8 @@ struct Fe2 {
             if (q) cudaFreeHost(q);
         void* p[] = {d_node_off, d_red_off, d_ncell, d_rve_of_node, d_fmap, d_col, d_order, d_queue, d_Fbar, d_w,
                      d_u, d_rhs, d_dx, d_r64, d_y64, d_minv, d_rnorm, d_cg_iters, d_active, d_P, d_A, d_nn, d_Z, d_M, d_X9,
-                     d_rve_of_elem, d_fail, d_op, d_wc, d_eta, d_rcol, d_gcoord, d_rve_of_blk, d_kell};
+                     d_rve_of_elem, d_fail, d_op, d_wc, d_eta, d_rcol, d_gcoord, d_rve_of_blk, d_kell,
+                     d_rs_int, d_rs_dbl, d_Fp, d_Ft, d_rctl, d_rpar};
         for (void* q : p)
             if (q) cudaFree(q);
         if (loop) ceos_destroy(loop);
@@ -266,6 +280,135 @@ __global__ void rve_op_kernel(int n_rve, const int* red_off, const int* op, doub
         } else {
             wc[q] = w[q];
         }
+    }
+}
+
+// Load continuation of every RVE (the host-driven and the device-resident rounds use the same rules):
+// a Newton step is accepted when no element folds and the residual grows by at most kGrowth (never
+// beyond kDiverge x the residual at the start of the load step), otherwise halved up to kMaxHalvings
+// times; a load step that still fails, or does not converge in max_newton iterations, is cut back by
+// the golden ratio, at most kMaxCutbacks times.
+constexpr int kMaxHalvings = 6, kMaxCutbacks = 16;
+constexpr double kGrowth = 1.5, kDiverge = 1e3, kGolden = 0.6180339887498949;
+enum { kNewton = 0, kDone = 1, kFailed = 2 };
+
+// ---- device-resident rounds ----
+// state: si = [phase, nit, halv, cuts, its, cg_tot] x n_rve (ints), sd = [a_done, da, a_try, r0, racc] x
+// n_rve (doubles); par = {tol, force floor, max_newton, max_rounds}; ctl = {rounds run, RVEs in Newton
+// this round, abort, RVE that aborted}.
+
+// Fbar of this round's trial load level; clears the failed-element flags.
+__global__ void round_fbar_kernel(int n_rve, const double* Fp, const double* Ft, const double* sd, double* Fbar,
+                                  int* fail) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 9 * n_rve) return;
+    const int r = i / 9;
+    const double a = sd[2 * n_rve + r];
+    Fbar[i] = Fp[i] + a * (Ft[i] - Fp[i]);
+    if (i % 9 == 0) fail[r] = 0;
+}
+
+// Failed-element flags per RVE, only when the assembly reported failed elements.
+__global__ void round_fail_kernel(int n_elem, const int* status_count, const uint8_t* elem_status,
+                                  const int* rve_of_elem, int* fail) {
+    if (*status_count == 0) return;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n_elem && elem_status[e]) atomicOr(fail + rve_of_elem[e], 1);
+}
+
+// The per-RVE decision of one round (the host loop's rules, one thread per RVE): operation, whether
+// a linear solve is needed, and its forcing term.
+__global__ void round_decide_kernel(int n_rve, int allow_failures, const double* par, const double* rn_all,
+                                    const int* fail, int* si, double* sd, int* op, int* need, double* eta, int* ctl) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rve) return;
+    int* phase = si;
+    int* nit = si + n_rve;
+    int* halv = si + 2 * n_rve;
+    int* cuts = si + 3 * n_rve;
+    int* its = si + 4 * n_rve;
+    double* a_done = sd;
+    double* da = sd + n_rve;
+    double* a_try = sd + 2 * n_rve;
+    double* r0 = sd + 3 * n_rve;
+    double* racc = sd + 4 * n_rve;
+    const double tol = par[0], floor_ = par[1];
+    const int max_newton = (int)par[2];
+    op[r] = kOpNone;
+    need[r] = 0;
+    if (phase[r] != kNewton) return;
+    atomicAdd(ctl + 1, 1);
+    const double rn = rn_all[r];
+    const bool ok = !fail[r] && isfinite(rn);
+    bool cut = false, accepted = false;
+    if (nit[r] == 0) {  // start of a load step from the converged fluctuations
+        if (!ok) cut = true;
+        else { r0[r] = fmax(rn, 1e-300); accepted = true; }
+    } else if (ok && rn <= kGrowth * racc[r] && rn <= kDiverge * r0[r]) {
+        accepted = true;
+    } else if (halv[r] >= kMaxHalvings) {
+        cut = true;
+    } else {
+        op[r] = kOpBacktrack;
+        ++halv[r];
+    }
+    if (accepted) {
+        racc[r] = rn;
+        halv[r] = 0;
+        if (rn <= tol * r0[r] || rn <= floor_) {
+            a_done[r] = a_try[r];
+            op[r] = kOpSave;
+            nit[r] = 0;
+            if (a_done[r] >= 1.0) {
+                phase[r] = kDone;
+            } else {
+                da[r] = fmin(2.0 * da[r], 1.0 - a_done[r]);  // grow after a converged step
+                a_try[r] = 1.0 - (a_done[r] + da[r]) < 1e-12 ? 1.0 : a_done[r] + da[r];
+            }
+        } else if (nit[r] >= max_newton) {
+            cut = true;
+        } else {
+            // Eisenstat-Walker forcing: quadratic convergence without over-solving
+            const double rel = rn / r0[r];
+            eta[r] = fmin(1e-2, fmax(rel, 0.1 * tol / rel));
+            need[r] = 1;
+            ++nit[r];
+            ++its[r];
+        }
+    }
+    if (cut) {
+        if (++cuts[r] > kMaxCutbacks) {
+            if (!allow_failures) {
+                atomicCAS(ctl + 3, -1, r);
+                ctl[2] = 1;
+            }
+            // give up on this RVE: back to its last converged state, reported as failed
+            phase[r] = kFailed;
+            op[r] = kOpRestore;
+            a_try[r] = a_done[r];
+            return;
+        }
+        op[r] = kOpRestore;
+        da[r] *= kGolden;
+        a_try[r] = a_done[r] + da[r];
+        nit[r] = 0;
+        halv[r] = 0;
+    }
+}
+
+// End of a round: MINRES iterations of the solved RVEs, the round count, and the loop condition (another
+// round while some RVE was still in Newton, no abort, and the round cap is not reached).
+__global__ void round_finish_kernel(int n_rve, const int* need, const int* cg_iters, int* si, const double* par,
+                                    int* ctl, cudaGraphConditionalHandle cond) {
+    int* cg_tot = si + 5 * n_rve;
+    for (int r = threadIdx.x; r < n_rve; r += blockDim.x)
+        if (need[r]) cg_tot[r] += cg_iters[r];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int rounds = ++ctl[0];
+        const bool more = ctl[1] > 0 && ctl[2] == 0 && rounds < (int)par[3];
+        ctl[1] = 0;
+        cudaGraphSetConditional(cond, more ? 1u : 0u);
     }
 }
 
@@ -768,6 +911,82 @@ int capture(Fe2* f, int (*record)(Fe2*), cudaGraphExec_t* exec) {
     return 0;
 }
 
+// One device-resident round, recorded into the body of the WHILE node (no host buffers: everything
+// the round needs lives on the device).
+int record_round(Fe2* f, cudaGraphConditionalHandle cond) {
+    Handle* h = f->loop;
+    cudaStream_t s = h->stream;
+    const int nr = f->n_rve;
+    round_fbar_kernel<<<(9 * nr + 255) / 256, 256, 0, s>>>(nr, f->d_Fp, f->d_Ft, f->d_rs_dbl, f->d_Fbar, f->d_fail);
+    CKF(cudaGetLastError());
+    int rc = assemble(f);
+    if (rc) return rc;
+    round_fail_kernel<<<(h->n_elem + 255) / 256, 256, 0, s>>>(h->n_elem, h->d_status_count, h->d_elem_status,
+                                                              f->d_rve_of_elem, f->d_fail);
+    rve_norm_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_rhs, f->d_nn);
+    round_decide_kernel<<<(nr + 255) / 256, 256, 0, s>>>(nr, f->allow_failures, f->d_rpar, f->d_nn, f->d_fail,
+                                                         f->d_rs_int, f->d_rs_dbl, f->d_op, f->d_active, f->d_eta,
+                                                         f->d_rctl);
+    rve_op_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_op, f->d_w, f->d_dx, f->d_wc);
+    CKF(cudaGetLastError());
+    rc = run_solver(f, 1, f->d_rhs, f->d_dx, 2000, 3);  // RVEs without need[] skip the solve
+    if (rc) return rc;
+    rve_step_kernel<<<nr, 256, 0, s>>>(nr, f->d_red_off, f->d_active, f->d_dx, f->d_w);
+    round_finish_kernel<<<1, 256, 0, s>>>(nr, f->d_active, f->d_cg_iters, f->d_rs_int, f->d_rpar, f->d_rctl, cond);
+    CKF(cudaGetLastError());
+    return 0;
+}
+
+// The whole continuation as one graph: a WHILE node (condition 1 at every launch) around one round.
+int build_round_graph(Fe2* f) {
+    cudaStream_t s = f->loop->stream;
+    const int nr = f->n_rve;
+    if (!f->d_rs_int) {
+        CKF(cudaMalloc(&f->d_rs_int, sizeof(int) * 8 * (size_t)nr));
+        CKF(cudaMalloc(&f->d_rs_dbl, sizeof(double) * 6 * (size_t)nr));
+        CKF(cudaMalloc(&f->d_Fp, sizeof(double) * 9 * (size_t)nr));
+        CKF(cudaMalloc(&f->d_Ft, sizeof(double) * 9 * (size_t)nr));
+        CKF(cudaMalloc(&f->d_rctl, sizeof(int) * 4));
+        CKF(cudaMalloc(&f->d_rpar, sizeof(double) * 4));
+    }
+    cudaGraph_t g = nullptr;
+    CKF(cudaGraphCreate(&g, 0));
+    auto fail = [&](const char* what, cudaError_t e) {
+        f->msg = std::string(what) + ": " + cudaGetErrorString(e);
+        cudaGraphDestroy(g);
+        return CEOS_E_CUDA;
+    };
+    cudaGraphConditionalHandle cond;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return fail("cudaGraphConditionalHandleCreate", e);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+    if (e != cudaSuccess) return fail("cudaGraphAddNode (while)", e);
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return fail("cudaStreamBeginCaptureToGraph", e);
+    const int rc = record_round(f, cond);
+    cudaGraph_t out = nullptr;
+    e = cudaStreamEndCapture(s, &out);  // always ends the capture, also after an error
+    if (rc) {
+        cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail("cudaStreamEndCapture", e);
+    e = cudaGraphInstantiate(&f->g_rounds, g, 0);
+    if (e != cudaSuccess) {
+        f->g_rounds = nullptr;
+        return fail("cudaGraphInstantiate (rounds)", e);
+    }
+    cudaGraphDestroy(g);
+    return 0;
+}
+
 // Fibre area fraction of cell column (i, j) of an n^3 RVE: share of 16 x 16 sub-points of the
 // cell's cross-section strictly inside the fibre circle x^2 + y^2 < vf/pi about the RVE centre.
 double fibre_fraction(int n, int i, int j, double rad2) {
@@ -963,11 +1182,8 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
     // not converge in max_newton iterations, is cut back: the RVE returns to its converged
     // fluctuations and da shrinks by the golden ratio, as the reference's quasi-static driver
     // cuts back its load steps (ModFEMAnalysis.f90:1136-1374).
-    constexpr int kMaxHalvings = 6, kMaxCutbacks = 16;
-    // a looser growth test (4x) accepted steps whose linear solves then cost more in total
-    constexpr double kGrowth = 1.5, kDiverge = 1e3;
-    const double golden = 0.6180339887498949;
-    enum { kNewton = 0, kDone = 1, kFailed = 2 };
+    // (kMaxHalvings, kMaxCutbacks, kGrowth, kDiverge, kGolden at file scope; a looser growth test (4x)
+    // accepted steps whose linear solves then cost more in total)
     std::vector<int> phase(nr, kNewton), nit(nr, 0), halv(nr, 0), cuts(nr, 0), its(nr, 0), cg_tot(nr, 0);
     std::vector<int> op(nr), need(nr), fail(nr);
     std::vector<double> a_done(nr, 0.0), da(nr, 1.0 / std::max(1, f->n_sub)), a_try(nr), r0(nr, 1.0), racc(nr, 0.0),
@@ -982,7 +1198,52 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
     // a generous cap bounds the whole solve (RVEs still running then fail)
     const int max_rounds = 4 * (max_newton + kMaxHalvings + 2) * (kMaxCutbacks + 2 * std::max(1, f->n_sub) + 8);
     bool all_done = false;
-    for (int round = 0; round < max_rounds && !all_done; ++round) {
+    if (f->device_rounds) {
+        // every round on the device: upload the continuation state, one graph launch, read it back
+        if (!f->g_rounds) {
+            const int rc = build_round_graph(f);
+            if (rc) return rc;
+        }
+        std::vector<int> si(8 * (size_t)nr, 0);
+        std::vector<double> sd(6 * (size_t)nr, 0.0);
+        for (int r = 0; r < nr; ++r) {
+            si[r] = phase[r];
+            sd[r] = a_done[r];
+            sd[nr + r] = da[r];
+            sd[2 * nr + r] = a_try[r];
+            sd[3 * nr + r] = r0[r];
+            sd[4 * nr + r] = racc[r];
+        }
+        const double par[4] = {tol, f->force_floor, (double)max_newton, (double)max_rounds};
+        int ctl[4] = {0, 0, 0, -1};
+        CKF(cudaMemcpyAsync(f->d_rs_int, si.data(), sizeof(int) * si.size(), cudaMemcpyHostToDevice, s));
+        CKF(cudaMemcpyAsync(f->d_rs_dbl, sd.data(), sizeof(double) * sd.size(), cudaMemcpyHostToDevice, s));
+        CKF(cudaMemcpyAsync(f->d_Fp, Fp.data(), sizeof(double) * 9 * (size_t)nr, cudaMemcpyHostToDevice, s));
+        CKF(cudaMemcpyAsync(f->d_Ft, Fbar, sizeof(double) * 9 * (size_t)nr, cudaMemcpyHostToDevice, s));
+        CKF(cudaMemcpyAsync(f->d_rpar, par, sizeof(par), cudaMemcpyHostToDevice, s));
+        CKF(cudaMemcpyAsync(f->d_rctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
+        CKF(cudaGraphLaunch(f->g_rounds, s));
+        CKF(cudaMemcpyAsync(si.data(), f->d_rs_int, sizeof(int) * si.size(), cudaMemcpyDeviceToHost, s));
+        CKF(cudaMemcpyAsync(sd.data(), f->d_rs_dbl, sizeof(double) * sd.size(), cudaMemcpyDeviceToHost, s));
+        CKF(cudaMemcpyAsync(ctl, f->d_rctl, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+        CKF(cudaStreamSynchronize(s));
+        h->evaluated = true;
+        all_done = true;
+        for (int r = 0; r < nr; ++r) {
+            phase[r] = si[r];
+            its[r] = si[4 * nr + r];
+            cg_tot[r] = si[5 * nr + r];
+            a_done[r] = sd[r];
+            if (phase[r] == kNewton) all_done = false;
+        }
+        if (ctl[2]) {
+            f->msg = "RVE " + std::to_string(ctl[3]) + ": no convergence after " + std::to_string(kMaxCutbacks) +
+                     " load cut-backs (converged load level " + std::to_string(a_done[ctl[3]]) + ")";
+            return 1;
+        }
+        if (verbose) std::fprintf(stderr, "fe2: %d device-resident rounds\n", ctl[0]);
+    }
+    for (int round = 0; !f->device_rounds && round < max_rounds && !all_done; ++round) {
         for (int r = 0; r < nr; ++r)
             for (int k = 0; k < 9; ++k) {
                 const size_t i = 9 * (size_t)r + k;
@@ -1068,7 +1329,7 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
                     continue;
                 }
                 op[r] = kOpRestore;
-                da[r] *= golden;
+                da[r] *= kGolden;
                 a_try[r] = a_done[r] + da[r];
                 nit[r] = 0;
                 halv[r] = 0;
@@ -1277,7 +1538,18 @@ extern "C" int ceos_fe2_autotune(void* handle, const double* Fbar, int* threads,
 extern "C" int ceos_fe2_set_allow_failures(void* handle, int allow) {
     Fe2* f = static_cast<Fe2*>(handle);
     if (!f) return CEOS_E_ARG;
+    if ((allow ? 1 : 0) != f->allow_failures && f->g_rounds) {  // the round graph holds the flag
+        cudaGraphExecDestroy(f->g_rounds);
+        f->g_rounds = nullptr;
+    }
     f->allow_failures = allow ? 1 : 0;
+    return 0;
+}
+
+extern "C" int ceos_fe2_set_device_rounds(void* handle, int on) {
+    Fe2* f = static_cast<Fe2*>(handle);
+    if (!f) return CEOS_E_ARG;
+    f->device_rounds = on ? 1 : 0;
     return 0;
 }
 

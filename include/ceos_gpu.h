@@ -257,6 +257,13 @@ int ceos_fe2_set_increments(void* handle, int n_sub);
 /* allow != 0: an RVE that cannot converge gets NaN in P and A and newton_iters -1, and
  * ceos_fe2_solve returns 2 after finishing the others (default 0: the solve fails). */
 int ceos_fe2_set_allow_failures(void* handle, int allow);
+/* Device-resident continuation: on != 0 (the default) runs every Newton round of a solve on the
+ * device, one CUDA graph whose WHILE node repeats a round (Fbar of the trial load level, assembly,
+ * failure flags, residual norms, the per-RVE accept / halve / cut-back / converge decision, vector
+ * operations, the linear solve, the Newton step) until no RVE is left in Newton; the host launches it
+ * once per solve.  on = 0: the host takes the per-RVE decisions between rounds (two graph launches
+ * and a synchronisation per round). */
+int ceos_fe2_set_device_rounds(void* handle, int on);
 /* on != 0: each solve continues every RVE from the Fbar and fluctuation of its last converged
  * state (along the macro load path) instead of from Fbar = I (default 0). */
 int ceos_fe2_set_warm_start(void* handle, int on);

@@ -62,10 +62,12 @@ def test_uneven_family_converges():
     b.close()
 
 
-def test_warm_start_and_mask_follow_the_load_path():
+@pytest.mark.parametrize("device_rounds", [False, True])
+def test_warm_start_and_mask_follow_the_load_path(device_rounds):
     """Warm-started solves continue every RVE from its last converged state: after a solve at Fbar1,
     a solve at Fbar2 reaches the same equilibrium as a cold solve at Fbar2 in fewer Newton iterations;
-    a masked-out RVE keeps its state; a changed volume fraction restarts that RVE only."""
+    a masked-out RVE keeps its state; a changed volume fraction restarts that RVE only.  With
+    host-driven and with device-resident rounds."""
     n = np.array([3, 4], np.int32)
     vf = np.array([0.25, 0.3])
     G = fe2.sample_macro_F(2, seed=8, amp=0.08) - np.eye(3)
@@ -73,6 +75,7 @@ def test_warm_start_and_mask_follow_the_load_path():
     cold = fe2.BatchedRVE(n, vf)
     ref = cold.solve(F2)
     warm = fe2.BatchedRVE(n, vf)
+    warm.set_device_rounds(device_rounds)
     warm.set_warm_start(True)
     warm.solve(F1)
     out = warm.solve(F2)
@@ -121,3 +124,30 @@ def test_batched_rve_matches_reference_periodic_formulation():
         b.close()
         Pr = F2.RVEReference(n, vf).solve(Fb)
         assert np.abs(P - Pr).max() <= 1e-7 * np.abs(Pr).max(), (n, np.abs(P - Pr).max())
+
+
+def test_device_resident_rounds_match_host_rounds():
+    """The continuation run entirely on the device (one graph launch per solve: a WHILE node around the
+    round, the per-RVE accept / halve / cut-back / converge decisions in a kernel) reaches the same
+    equilibria as the host-driven rounds: P within 1e-7 of each other and of the FP64 oracle, the
+    same Newton iteration counts up to one (the FP32 atomic order of the stiffness fold differs between
+    the runs), on the oracle's small RVEs and on a config-4-like family that needs a load cut-back."""
+    for n, vf, Fb, check in (
+            (np.array([3, 4, 5, 3, 4], np.int32), np.array([0.3, 0.2, 0.35, 0.1, 0.4]),
+             fe2.sample_macro_F(5, seed=3, amp=0.1), True),
+            (*fe2.sample_rve_family(12, seed=4), fe2.sample_macro_F(12, seed=5), False)):
+        outs = []
+        for device_rounds in (False, True):
+            b = fe2.BatchedRVE(n, vf)
+            b.set_device_rounds(device_rounds)
+            outs.append(b.solve(Fb, tangent=device_rounds))
+            b.close()
+        host, dev = outs
+        scale = np.abs(host["P"]).max()
+        assert np.all(np.isfinite(dev["P"]))
+        assert np.abs(dev["P"] - host["P"]).max() <= 1e-7 * scale
+        assert np.abs(np.asarray(dev["newton_iters"]) - np.asarray(host["newton_iters"])).max() <= 1
+        if check:
+            for r in range(len(n)):
+                Po = F2.RVE(int(n[r]), float(vf[r])).solve(Fb[r])
+                assert np.abs(dev["P"][r] - Po).max() <= 1e-7 * np.abs(Po).max(), r
