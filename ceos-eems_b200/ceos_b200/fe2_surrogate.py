@@ -73,9 +73,12 @@ def rve_stresses(F, vf, n_cells=6, batch=4096, tangent=False, **rve_args):
 
 
 def fit(F, vf, P, epochs=150, batch=2048, lr0=3e-3, lr1=2e-5, seed=0, s_C=0.15, vf0=0.25, s_vf=0.15,
-        relative=0.2):
+        relative=0.2, box_margin=0.005):
     """Train a surrogate on the finite samples; the training box of the range check is the
-    component-wise extent of the training inputs.  relative > 0 weights every sample by
+    component-wise extent of the training inputs widened by box_margin of that extent on either side
+    (the sampled extremes fall just inside the sampling ranges: without a margin a macro point whose
+    fibre fraction lies 1e-6 beyond the smallest sampled one would be sent to an RVE solve for
+    nothing).  relative > 0 weights every sample by
     1 / (|S|^2 / mean|S|^2 + relative), so the loss measures relative stress error (small stresses of
     nearly isochoric states count as much as the large volumetric ones) with a floor.
     Returns (Surrogate, loss history, seconds)."""
@@ -89,7 +92,9 @@ def fit(F, vf, P, epochs=150, batch=2048, lr0=3e-3, lr1=2e-5, seed=0, s_C=0.15, 
     sur.set_params(init_params(seed))
     sur.set_scaling(s_C, s_W, vf0, s_vf)
     x = sur.inputs(C6, vf)
-    sur.set_scaling(s_C, s_W, vf0, s_vf, lo=x.min(axis=0), hi=x.max(axis=0))
+    lo, hi = x.min(axis=0), x.max(axis=0)
+    pad = box_margin * (hi - lo)
+    sur.set_scaling(s_C, s_W, vf0, s_vf, lo=lo - pad, hi=hi + pad)
     t, w = training_targets(F, P, s_C, s_W)
     sw = None
     if relative > 0:
