@@ -292,6 +292,71 @@ constexpr int kMaxHalvings = 6, kMaxCutbacks = 16;
 constexpr double kGrowth = 1.5, kDiverge = 1e3, kGolden = 0.6180339887498949;
 enum { kNewton = 0, kDone = 1, kFailed = 2 };
 
+// One RVE's continuation state and the decision of one round on it, shared by the host-driven and the
+// device-resident rounds.  rn: the RVE's residual norm after this round's assembly; ok: no element folded
+// and rn is finite.  Sets op (vector operation), need (a linear solve follows) and eta (its forcing
+// term); returns the flags kRejected (a halving), kCut (a load cut-back) and kExhausted (the cut-back
+// limit was passed: the RVE returns to its converged state and counts as failed).
+struct RveCont {
+    int phase, nit, halv, cuts, its;
+    double a_done, da, a_try, r0, racc;
+};
+enum { kRejected = 1, kCut = 2, kExhausted = 4 };
+__host__ __device__ inline int decide_rve(RveCont& c, double rn, bool ok, double tol, double floor_, int max_newton,
+                                          int& op, int& need, double& eta) {
+    op = kOpNone;
+    need = 0;
+    bool cut = false, accepted = false;
+    if (c.nit == 0) {  // start of a load step from the converged fluctuations
+        if (!ok) cut = true;
+        else { c.r0 = rn > 1e-300 ? rn : 1e-300; accepted = true; }
+    } else if (ok && rn <= kGrowth * c.racc && rn <= kDiverge * c.r0) {
+        accepted = true;
+    } else if (c.halv >= kMaxHalvings) {
+        cut = true;
+    } else {
+        op = kOpBacktrack;
+        ++c.halv;
+        return kRejected;
+    }
+    if (accepted) {
+        c.racc = rn;
+        c.halv = 0;
+        if (rn <= tol * c.r0 || rn <= floor_) {
+            c.a_done = c.a_try;
+            op = kOpSave;
+            c.nit = 0;
+            if (c.a_done >= 1.0) {
+                c.phase = kDone;
+            } else {
+                c.da = fmin(2.0 * c.da, 1.0 - c.a_done);  // grow after a converged step
+                c.a_try = 1.0 - (c.a_done + c.da) < 1e-12 ? 1.0 : c.a_done + c.da;
+            }
+        } else if (c.nit >= max_newton) {
+            cut = true;
+        } else {
+            // Eisenstat-Walker forcing: quadratic convergence without over-solving
+            const double rel = rn / c.r0;
+            eta = fmin(1e-2, fmax(rel, 0.1 * tol / rel));
+            need = 1;
+            ++c.nit;
+            ++c.its;
+        }
+    }
+    if (!cut) return 0;
+    op = kOpRestore;
+    if (++c.cuts > kMaxCutbacks) {  // give up on this RVE: back to its last converged state
+        c.phase = kFailed;
+        c.a_try = c.a_done;
+        return kExhausted;
+    }
+    c.da *= kGolden;
+    c.a_try = c.a_done + c.da;
+    c.nit = 0;
+    c.halv = 0;
+    return kCut;
+}
+
 // ---- device-resident rounds ----
 // state: si = [phase, nit, halv, cuts, its, cg_tot] x n_rve (ints), sd = [a_done, da, a_try, r0, racc] x
 // n_rve (doubles); par = {tol, force floor, max_newton, max_rounds}; ctl = {rounds run, RVEs in Newton
@@ -316,84 +381,39 @@ __global__ void round_fail_kernel(int n_elem, const int* status_count, const uin
     if (e < n_elem && elem_status[e]) atomicOr(fail + rve_of_elem[e], 1);
 }
 
-// The per-RVE decision of one round (the host loop's rules, one thread per RVE): operation, whether
-// a linear solve is needed, and its forcing term.
+// The per-RVE decision of one round (decide_rve, one thread per RVE): operation, whether a linear
+// solve is needed, and its forcing term.
 __global__ void round_decide_kernel(int n_rve, int allow_failures, const double* par, const double* rn_all,
                                     const int* fail, int* si, double* sd, int* op, int* need, double* eta, int* ctl) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_rve) return;
-    int* phase = si;
-    int* nit = si + n_rve;
-    int* halv = si + 2 * n_rve;
-    int* cuts = si + 3 * n_rve;
-    int* its = si + 4 * n_rve;
-    double* a_done = sd;
-    double* da = sd + n_rve;
-    double* a_try = sd + 2 * n_rve;
-    double* r0 = sd + 3 * n_rve;
-    double* racc = sd + 4 * n_rve;
-    const double tol = par[0], floor_ = par[1];
-    const int max_newton = (int)par[2];
     op[r] = kOpNone;
     need[r] = 0;
-    if (phase[r] != kNewton) return;
+    if (si[r] != kNewton) return;
     atomicAdd(ctl + 1, 1);
+    RveCont c{si[r], si[n_rve + r], si[2 * n_rve + r], si[3 * n_rve + r], si[4 * n_rve + r],
+              sd[r], sd[n_rve + r], sd[2 * n_rve + r], sd[3 * n_rve + r], sd[4 * n_rve + r]};
     const double rn = rn_all[r];
-    const bool ok = !fail[r] && isfinite(rn);
-    bool cut = false, accepted = false;
-    if (nit[r] == 0) {  // start of a load step from the converged fluctuations
-        if (!ok) cut = true;
-        else { r0[r] = fmax(rn, 1e-300); accepted = true; }
-    } else if (ok && rn <= kGrowth * racc[r] && rn <= kDiverge * r0[r]) {
-        accepted = true;
-    } else if (halv[r] >= kMaxHalvings) {
-        cut = true;
-    } else {
-        op[r] = kOpBacktrack;
-        ++halv[r];
+    int o = kOpNone, nd = 0;
+    double e = eta[r];
+    const int flags = decide_rve(c, rn, !fail[r] && isfinite(rn), par[0], par[1], (int)par[2], o, nd, e);
+    if ((flags & kExhausted) && !allow_failures) {
+        atomicCAS(ctl + 3, -1, r);
+        ctl[2] = 1;
     }
-    if (accepted) {
-        racc[r] = rn;
-        halv[r] = 0;
-        if (rn <= tol * r0[r] || rn <= floor_) {
-            a_done[r] = a_try[r];
-            op[r] = kOpSave;
-            nit[r] = 0;
-            if (a_done[r] >= 1.0) {
-                phase[r] = kDone;
-            } else {
-                da[r] = fmin(2.0 * da[r], 1.0 - a_done[r]);  // grow after a converged step
-                a_try[r] = 1.0 - (a_done[r] + da[r]) < 1e-12 ? 1.0 : a_done[r] + da[r];
-            }
-        } else if (nit[r] >= max_newton) {
-            cut = true;
-        } else {
-            // Eisenstat-Walker forcing: quadratic convergence without over-solving
-            const double rel = rn / r0[r];
-            eta[r] = fmin(1e-2, fmax(rel, 0.1 * tol / rel));
-            need[r] = 1;
-            ++nit[r];
-            ++its[r];
-        }
-    }
-    if (cut) {
-        if (++cuts[r] > kMaxCutbacks) {
-            if (!allow_failures) {
-                atomicCAS(ctl + 3, -1, r);
-                ctl[2] = 1;
-            }
-            // give up on this RVE: back to its last converged state, reported as failed
-            phase[r] = kFailed;
-            op[r] = kOpRestore;
-            a_try[r] = a_done[r];
-            return;
-        }
-        op[r] = kOpRestore;
-        da[r] *= kGolden;
-        a_try[r] = a_done[r] + da[r];
-        nit[r] = 0;
-        halv[r] = 0;
-    }
+    op[r] = o;
+    need[r] = nd;
+    eta[r] = e;
+    si[r] = c.phase;
+    si[n_rve + r] = c.nit;
+    si[2 * n_rve + r] = c.halv;
+    si[3 * n_rve + r] = c.cuts;
+    si[4 * n_rve + r] = c.its;
+    sd[r] = c.a_done;
+    sd[n_rve + r] = c.da;
+    sd[2 * n_rve + r] = c.a_try;
+    sd[3 * n_rve + r] = c.r0;
+    sd[4 * n_rve + r] = c.racc;
 }
 
 // End of a round: MINRES iterations of the solved RVEs, the round count, and the loop condition (another
@@ -1277,63 +1297,29 @@ extern "C" int ceos_fe2_solve(void* handle, const double* Fbar, double tol, int 
             need[r] = 0;
             if (phase[r] != kNewton) continue;
             all_done = false;
-            const bool ok = !fail[r] && std::isfinite(rn[r]);
-            bool cut = false, accepted = false;
-            if (nit[r] == 0) {  // start of a load step from the converged fluctuations
-                if (!ok) cut = true;
-                else { r0[r] = std::max(rn[r], 1e-300); accepted = true; }
-            } else if (ok && rn[r] <= kGrowth * racc[r] && rn[r] <= kDiverge * r0[r]) {
-                accepted = true;
-            } else if (halv[r] >= kMaxHalvings) {
-                cut = true;
-            } else {
-                op[r] = kOpBacktrack;
-                ++halv[r];
-                ++n_rej;
+            RveCont c{phase[r], nit[r], halv[r], cuts[r], its[r], a_done[r], da[r], a_try[r], r0[r], racc[r]};
+            const int flags = decide_rve(c, rn[r], !fail[r] && std::isfinite(rn[r]), tol, f->force_floor, max_newton,
+                                         op[r], need[r], eta[r]);
+            phase[r] = c.phase;
+            nit[r] = c.nit;
+            halv[r] = c.halv;
+            cuts[r] = c.cuts;
+            its[r] = c.its;
+            a_done[r] = c.a_done;
+            da[r] = c.da;
+            a_try[r] = c.a_try;
+            r0[r] = c.r0;
+            racc[r] = c.racc;
+            if (flags & kExhausted) {
+                f->msg = "RVE " + std::to_string(r) + ": no convergence after " + std::to_string(kMaxCutbacks) +
+                         " load cut-backs (converged load level " + std::to_string(a_done[r]) + ")";
+                if (!f->allow_failures) return st ? st : 1;
             }
-            if (accepted) {
-                racc[r] = rn[r];
-                halv[r] = 0;
-                if (rn[r] <= tol * r0[r] || rn[r] <= f->force_floor) {
-                    a_done[r] = a_try[r];
-                    op[r] = kOpSave;
-                    nit[r] = 0;
-                    if (a_done[r] >= 1.0) {
-                        phase[r] = kDone;
-                    } else {
-                        da[r] = std::min(2.0 * da[r], 1.0 - a_done[r]);  // grow after a converged step
-                        a_try[r] = 1.0 - (a_done[r] + da[r]) < 1e-12 ? 1.0 : a_done[r] + da[r];
-                    }
-                } else if (nit[r] >= max_newton) {
-                    cut = true;
-                } else {
-                    // Eisenstat-Walker forcing: quadratic convergence without over-solving
-                    const double rel = rn[r] / r0[r];
-                    eta[r] = std::min(1e-2, std::max(rel, 0.1 * tol / rel));
-                    need[r] = 1;
-                    ++nit[r];
-                    ++its[r];
-                    ++n_need;
-                    worst = std::max(worst, rel);
-                }
-            }
-            if (cut) {
-                if (++cuts[r] > kMaxCutbacks) {
-                    f->msg = "RVE " + std::to_string(r) + ": no convergence after " + std::to_string(kMaxCutbacks) +
-                             " load cut-backs (converged load level " + std::to_string(a_done[r]) + ")";
-                    if (!f->allow_failures) return st ? st : 1;
-                    // give up on this RVE: back to its last converged state, reported as failed
-                    phase[r] = kFailed;
-                    op[r] = kOpRestore;
-                    a_try[r] = a_done[r];
-                    continue;
-                }
-                op[r] = kOpRestore;
-                da[r] *= kGolden;
-                a_try[r] = a_done[r] + da[r];
-                nit[r] = 0;
-                halv[r] = 0;
-                ++n_cut;
+            n_rej += (flags & kRejected) ? 1 : 0;
+            n_cut += (flags & kCut) ? 1 : 0;
+            if (need[r]) {
+                ++n_need;
+                worst = std::max(worst, rn[r] / r0[r]);
             }
         }
         if (verbose)

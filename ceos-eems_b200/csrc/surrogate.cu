@@ -243,8 +243,11 @@ __device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, boo
 template <int EPI>
 __device__ __forceinline__ void layer_epilogue32(const LayerArgs& A, int n, int m0, const float* v);
 
+// The epilogue of 8 outputs of the forward passes (layer 1 on the CUDA cores, and the forward primal
+// groups of layer_epilogue32); the backward passes only run through layer_epilogue32.
 template <int EPI>
 __device__ __forceinline__ void layer_epilogue8(const LayerArgs& A, int n, int m0, const float* v) {
+    static_assert(EPI == kFwd || EPI == kFwdT, "forward passes only");
     const size_t o = (size_t)n * kH + m0;
     auto ld8 = [](const float* src, float* x) {
         const float4 a = *reinterpret_cast<const float4*>(src), b = *reinterpret_cast<const float4*>(src + 4);
@@ -268,14 +271,7 @@ __device__ __forceinline__ void layer_epilogue8(const LayerArgs& A, int n, int m
             for (int j = 0; j < 8; ++j) b[j] = sigmoid_t(z[j]) * A.w5[m0 + j];
             st_out8(A, A.outb2 + o, b, n, m0, true);
         }
-    } else if constexpr (EPI == kBwd) {
-        float z[8];
-        ld8(A.Z + o, z);
-        st8(A.G + o, v);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) a[j] = sigmoid_t(z[j]) * v[j];
-        st_out8(A, A.outb + o, a, n, m0, true);
-    } else if constexpr (EPI == kFwdT) {
+    } else {
         float z[8];
         ld8(A.Z + o, z);
         st8(A.Zd + o, v);
@@ -293,17 +289,6 @@ __device__ __forceinline__ void layer_epilogue8(const LayerArgs& A, int n, int m
             for (int j = 0; j < 8; ++j) a[j] = sigmoid_t(z[j]) * v[j];
             st_out8(A, A.outb + o, a, n, m0, true);
         }
-    } else {
-        float z[8], zd[8], g[8];
-        ld8(A.Z + o, z);
-        ld8(A.Zd + o, zd);
-        ld8(A.G + o, g);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const float sg = sigmoid_t(z[j]);
-            a[j] = sg * v[j] + sg * (1.f - sg) * zd[j] * g[j];
-        }
-        st_out8(A, A.outb + o, a, n, m0, true);
     }
 }
 
