@@ -262,3 +262,27 @@ def test_fem_system_of_equations_plugin():
     assert np.allclose(Rb[bc["presc"] - 1], -bc["presc_final"][:, 0])
     assert np.all(Rb[bc["fixed"] - 1] == 0.0)
     g.close()
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 1, 1), (11, 3, 1)])
+@pytest.mark.parametrize("assembly", ["two-pass", "fused", "banded"])
+def test_tiny_meshes_all_assemblies(shape, assembly):
+    """Edge cases of the tiling: a single element (one tile of 1, one conversion item), two elements,
+    and 33 elements (a full tile of 32 plus a tile of 1), with FP64 and with each mixed-precision K
+    assembly, against the FP64 oracle; the CSR pattern bit-exact."""
+    X, conn = meshgen.structured_box(*shape, jitter=0.05, seed=7)
+    U = smooth_u(X, 0.05, seed=3)
+    o = O.Model(X, conn, [G.CNH], CNH_P)
+    fo, ko, rco, _ = o.evaluate(0.0, U)
+    assert rco == 0
+    for precision, tol in ((G.FP64, 1e-12), (G.MIXED, 2e-5)):
+        g = G.ElementLoop(X, conn, G.CNH, CNH_P, precision=precision)
+        if precision == G.MIXED:
+            g.set_assembly(assembly)
+        fg, kg, rc, _ = g.evaluate(0.0, U)
+        rowmap, col = g.pattern()
+        g.close()
+        assert rc == 0
+        assert relerr(fg, fo) <= tol and relerr(kg, ko) <= tol, (precision, relerr(fg, fo), relerr(kg, ko))
+        orow, ocol, _ = O.pattern(X.shape[0], conn)
+        assert (rowmap == orow).all() and (col == ocol).all()
