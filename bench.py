@@ -224,6 +224,26 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+# B^T D B of one Hexa8 element in the node-pair form: 63 FMA per node and Gauss point for D B_b (54) and
+# sigma g_b (9), 27 per off-diagonal block and 18 per diagonal block per Gauss point (28 + 8 blocks), over
+# 8 Gauss points; the geometric dots g_a . sigma g_b (1,440 more) are left out of this floor
+FMA_PER_ELEMENT_BDB = 8 * (8 * 63 + 28 * 27 + 8 * 18)
+
+
+def fma_roofline(n_elem, element_ms, clocks, dev):
+    """The element loop's other bound: the FP32 FMAs of its B^T D B contraction per element pass against
+    the FP32 pipe's peak (128 FMA per clock per SM) at the SM clock sampled during the timed region."""
+    import torch
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz") or 1965.0
+    peak = sms * 128 * mhz * 1e6 / 1e12
+    achieved = FMA_PER_ELEMENT_BDB * n_elem / (element_ms * 1e-3) / 1e12
+    return {"bound": "fp32_fma", "unit": "TFMA/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
+            "fma_per_element": FMA_PER_ELEMENT_BDB, "floor_ms": FMA_PER_ELEMENT_BDB * n_elem / (peak * 1e12) * 1e3,
+            "what": "B^T D B contraction FMAs of one element pass / its CUDA-event time, against 128 FMA per clock "
+                    "per SM at the sampled SM clock (the Gauss-point update and phase-A geometry are extra work)"}
+
+
 def profile_traffic(workload, n_elem):
     """DRAM bytes of one evaluation (all its kernels) from the committed ncu summary, scaled by elements."""
     p = os.path.join(ROOT, "profiles", "element_loop_traffic.json")
@@ -387,6 +407,7 @@ def run_element_loop(args, w, config, world, rank, local_rank):
                          "peak_kind": peak_kind, "kernel": g.kernel_names(), "kernel_ms": k_mean + c_mean,
                          "algorithmic_bytes_per_launch": alg,
                          "kernel_split_ms": {"element_loop": k_mean, "conversion": c_mean},
+                         "compute": fma_roofline(w.n_elem, k_mean, clocks, dev),
                          "what": "algorithmic bytes of one evaluation / device time of all its kernels (the "
                                  "element loop and the K conversion, CUDA events on the launching stream)"},
             "clocks": clocks}
