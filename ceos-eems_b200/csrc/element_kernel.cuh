@@ -109,7 +109,7 @@ struct ElemArgs {
 // prefetched with cp.async while the current tile computes (software pipeline).
 template <typename T>
 struct SmemLayout {
-    size_t g, ds, st, x, u, xf, rs, nup, node, ranks, status, kd, pe, total;
+    size_t g, ds, st, x, u, rs, nup, node, ranks, status, kd, pe, total;
     CEOS_HD SmemLayout(int ns, int npe) {
         size_t o = 0;
         auto take = [&](size_t bytes) { size_t r = o; o += (bytes + 15) & ~size_t(15); return r; };
@@ -118,10 +118,6 @@ struct SmemLayout {
         st = take(sizeof(T) * (size_t)(ns > 0 ? ns : 1) * 8 * kTileE);  // [v][gp][e]: committed state
         x = take(sizeof(double) * 8 * kTileE * 3);     // [node][e][3] staged X (FP64)
         u = take(sizeof(double) * 8 * kTileE * 3);     // [node][e][3] staged U (FP64)
-        // FP32 mode: [node][e][dX 4 | dU 4], element-local differences in FP32.  It overlays the
-        // FP64 staging of x and u (12 KB >= 8 KB, contiguous): the staging of a tile is converted
-        // before the tile computes, and the next tile is staged only after phase A stopped reading.
-        xf = sizeof(T) == 4 ? x : take(16);
         rs = take(sizeof(long long) * 2 * 8 * kTileE);  // double-buffered [buf][node][e]
         nup = take(sizeof(int) * 2 * 8 * kTileE);
         node = take(sizeof(int) * 2 * 8 * kTileE);
@@ -144,7 +140,6 @@ template <typename T>
 struct SmemPtrs {
     T *g, *ds, *st, *kd, *pe;
     double *x, *u;
-    float* xf;
     long long* rs;
     int *nup, *node, *status;
     uint32_t* ranks;
@@ -153,7 +148,7 @@ struct SmemPtrs {
           st(reinterpret_cast<T*>(raw + L.st)), kd(reinterpret_cast<T*>(raw + L.kd)),
           pe(reinterpret_cast<T*>(raw + L.pe)),
           x(reinterpret_cast<double*>(raw + L.x)), u(reinterpret_cast<double*>(raw + L.u)),
-          xf(reinterpret_cast<float*>(raw + L.xf)), rs(reinterpret_cast<long long*>(raw + L.rs)),
+          rs(reinterpret_cast<long long*>(raw + L.rs)),
           nup(reinterpret_cast<int*>(raw + L.nup)), node(reinterpret_cast<int*>(raw + L.node)),
           status(reinterpret_cast<int*>(raw + L.status)), ranks(reinterpret_cast<uint32_t*>(raw + L.ranks)) {}
 };
@@ -322,24 +317,22 @@ CEOS_D void red_v4(float* p, float a, float b, float c, float d) {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
 }
 
-// FP32 mode: one FP64 -> FP32 conversion per (node, element), of the differences to the element's
-// node 0: X_n - X_0 and u_n - u_0 are formed in FP64, so the FP32 values keep their relative
-// precision at the element scale (absolute coordinates rounded to FP32 would perturb an element of
-// size h by ~6e-8 / h, which the bulk modulus of a nearly incompressible material amplifies in
-// f_int).  J_X and J_u are unchanged by the shift because sum_n dN_n/dxi = 0.  Contains barriers.
-CEOS_D void stage_local_differences(const SmemPtrs<float>& s, int warp, int lane) {
-    const int n = warp, el = lane;
+// FP32 mode: node n of element el as differences to the element's node 0, formed in FP64 from the
+// staged node data and then rounded: X_n - X_0 and u_n - u_0 keep their relative precision at the
+// element scale (absolute coordinates rounded to FP32 would perturb an element of size h by
+// ~6e-8 / h, which the bulk modulus of a nearly incompressible material amplifies in f_int).  J_X and
+// J_u are unchanged by the shift because sum_n dN_n/dxi = 0.  Each Gauss-point thread forms the
+// differences it reads, so the staging needs no conversion pass and no barrier.
+CEOS_D void local_node_f32(const SmemPtrs<float>& s, int n, int el, float X[3], float u[3]) {
     const double* xp = s.x + (n * kTileE + el) * 3;
     const double* up = s.u + (n * kTileE + el) * 3;
     const double* x0 = s.x + el * 3;
     const double* u0 = s.u + el * 3;
-    const float4 dx = make_float4((float)(xp[0] - x0[0]), (float)(xp[1] - x0[1]), (float)(xp[2] - x0[2]), 0.f);
-    const float4 du = make_float4((float)(up[0] - u0[0]), (float)(up[1] - u0[1]), (float)(up[2] - u0[2]), 0.f);
-    __syncthreads();  // every thread has read the FP64 staging that the FP32 tile overlays
-    float4* dst = reinterpret_cast<float4*>(s.xf + (n * kTileE + el) * 8);
-    dst[0] = dx;
-    dst[1] = du;
-    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        X[d] = n == 0 ? 0.f : (float)(xp[d] - x0[d]);
+        u[d] = n == 0 ? 0.f : (float)(up[d] - u0[d]);
+    }
 }
 
 // Phase A for thread (gp = warp, element = lane) of the tile at e0.
@@ -357,10 +350,7 @@ CEOS_D void phase_a(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp
     for (int n = 0; n < 8; ++n) {
         T X[3], u[3];
         if constexpr (sizeof(T) == 4) {
-            const float4* q = reinterpret_cast<const float4*>(s.xf + (n * kTileE + el) * 8);
-            const float4 xv = q[0], uv = q[1];
-            X[0] = xv.x; X[1] = xv.y; X[2] = xv.z;
-            u[0] = uv.x; u[1] = uv.y; u[2] = uv.z;
+            local_node_f32(s, n, el, X, u);
         } else {
             const double* xp = s.x + (n * kTileE + el) * 3;
             const double* up = s.u + (n * kTileE + el) * 3;
@@ -445,10 +435,9 @@ CEOS_D void phase_a(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp
                 for (int n = 0; n < 8; ++n) {
                     T X[3], x[3];
                     if constexpr (sizeof(T) == 4) {
-                        const float4* q = reinterpret_cast<const float4*>(s.xf + (n * kTileE + el) * 8);
-                        const float4 xv = q[0], uv = q[1];
-                        X[0] = xv.x; X[1] = xv.y; X[2] = xv.z;
-                        x[0] = xv.x + uv.x; x[1] = xv.y + uv.y; x[2] = xv.z + uv.z;
+                        float uf[3];
+                        local_node_f32(s, n, el, X, uf);
+                        x[0] = X[0] + uf[0]; x[1] = X[1] + uf[1]; x[2] = X[2] + uf[2];
                     } else {
                         const double* xp = s.x + (n * kTileE + el) * 3;
                         const double* up = s.u + (n * kTileE + el) * 3;
@@ -806,7 +795,6 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) element_loop
             prefetch_conn(a, e0n, s.node + (buf ^ 1) * NB, s.ranks + (buf ^ 1) * NB, t);
             cp_commit();
         }
-        if constexpr (sizeof(T) == 4) stage_local_differences(s, warp, lane);
         phase_a<T, MODEL>(a, s, e0, warp, lane);
         cp_wait_all();    // connectivity of the next tile has landed
         __syncthreads();  // phase A results visible; x, u and state buffers are free
@@ -973,7 +961,6 @@ __global__ void __launch_bounds__(kThreads, 2) element_assemble_kernel(ElemArgs<
                 prefetch_conn(a, next * kTileE, s.node + nb * NB, s.ranks + nb * NB, t);
                 cp_commit();
             }
-            stage_local_differences(s, warp, lane);
             phase_a<float, MODEL>(a, s, e0, warp, lane);
             if (warp == 0) {  // the ring slots of this tile must have been released by their last user
                 const int2 wr = __ldg(a.tile_wait + cur);

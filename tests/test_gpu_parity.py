@@ -2,7 +2,7 @@
 
 Bars (stated per test): the CSR pattern and slot map are bit-exact; in FP64 mode f_int and K
 agree with the oracle to 1e-12 relative (max-norm relative to the largest entry); in mixed
-mode to 2e-5; Newton histories match iteration counts exactly and norms to 1e-6 relative."""
+mode to per-model bars of 2e-6 to 3e-5 (f_int) and 1e-6 (K); Newton histories match iteration counts exactly and norms to 1e-6 relative."""
 import numpy as np
 import pytest
 
@@ -94,11 +94,16 @@ def test_evaluate_fp64(model, params, amp):
     g.close()
 
 
-@pytest.mark.parametrize("model,params,amp,tol", [
-    (G.CNH, CNH_P, 0.08, 2e-5), (G.VISCO_PRONY, PRONY_P, 0.08, 2e-5), (G.J2_FINITE, J2F_P, 0.01, 5e-5),
-    (G.VISCO_VAR, VV_P, 0.05, 2e-5), (G.NH_Q1P0, Q1P0_P, 0.08, 5e-5)])
+# Mixed-precision bars (f_int, K) about 3x the largest error measured on a B200 over both increments
+# and all three assemblies: f_int 5.6e-7 / 5.8e-7 / 9.2e-6 / 1.3e-6 / 1.8e-6 (CNH, Prony, finite J2,
+# variational visco, Q1P0), K at most 3.3e-7.  Finite J2 carries the largest f_int error: the return
+# mapping of a plastic Gauss point amplifies the FP32 rounding of F.
+@pytest.mark.parametrize("model,params,amp,ftol,ktol", [
+    (G.CNH, CNH_P, 0.08, 2e-6, 1e-6), (G.VISCO_PRONY, PRONY_P, 0.08, 2e-6, 1e-6),
+    (G.J2_FINITE, J2F_P, 0.01, 3e-5, 1e-6), (G.VISCO_VAR, VV_P, 0.05, 4e-6, 1e-6),
+    (G.NH_Q1P0, Q1P0_P, 0.08, 6e-6, 1e-6)])
 @pytest.mark.parametrize("assembly", ["two-pass", "fused", "banded"])
-def test_evaluate_mixed(model, params, amp, tol, assembly):
+def test_evaluate_mixed(model, params, amp, ftol, ktol, assembly):
     X, conn = meshgen.structured_box(6, 5, 4, jitter=0.05, seed=2)
     g, o = _pair(model, params, X, conn, precision=G.MIXED)
     g.set_assembly(assembly)
@@ -109,8 +114,8 @@ def test_evaluate_mixed(model, params, amp, tol, assembly):
         fg, kg, rc, _ = g.evaluate(t, U)
         fo, ko, _, _ = o.evaluate(t, U)
         assert rc == 0
-        assert relerr(fg, fo) <= tol
-        assert relerr(kg, ko) <= tol
+        assert relerr(fg, fo) <= ftol, ("fint", step)
+        assert relerr(kg, ko) <= ktol, ("K", step)
         g.commit(); o.commit(); g.set_committed_time(t); o.set_time_old(t)
     g.close()
 
@@ -269,13 +274,14 @@ def test_fem_system_of_equations_plugin():
 def test_tiny_meshes_all_assemblies(shape, assembly):
     """Edge cases of the tiling: a single element (one tile of 1, one conversion item), two elements,
     and 33 elements (a full tile of 32 plus a tile of 1), with FP64 and with each mixed-precision K
-    assembly, against the FP64 oracle; the CSR pattern bit-exact."""
+    assembly, against the FP64 oracle (mixed bars about 3x the errors measured on a B200: f_int
+    1.4e-6, K 3.3e-7); the CSR pattern bit-exact."""
     X, conn = meshgen.structured_box(*shape, jitter=0.05, seed=7)
     U = smooth_u(X, 0.05, seed=3)
     o = O.Model(X, conn, [G.CNH], CNH_P)
     fo, ko, rco, _ = o.evaluate(0.0, U)
     assert rco == 0
-    for precision, tol in ((G.FP64, 1e-12), (G.MIXED, 2e-5)):
+    for precision, ftol, ktol in ((G.FP64, 1e-12, 1e-12), (G.MIXED, 4e-6, 1e-6)):
         g = G.ElementLoop(X, conn, G.CNH, CNH_P, precision=precision)
         if precision == G.MIXED:
             g.set_assembly(assembly)
@@ -283,6 +289,6 @@ def test_tiny_meshes_all_assemblies(shape, assembly):
         rowmap, col = g.pattern()
         g.close()
         assert rc == 0
-        assert relerr(fg, fo) <= tol and relerr(kg, ko) <= tol, (precision, relerr(fg, fo), relerr(kg, ko))
+        assert relerr(fg, fo) <= ftol and relerr(kg, ko) <= ktol, (precision, relerr(fg, fo), relerr(kg, ko))
         orow, ocol, _ = O.pattern(X.shape[0], conn)
         assert (rowmap == orow).all() and (col == ocol).all()

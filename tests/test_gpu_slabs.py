@@ -27,9 +27,13 @@ def _mesh(n, scramble):
 
 
 @pytest.mark.parametrize("n,scramble", [(32, False), (40, True)])
-@pytest.mark.parametrize("precision,rtol,assembly", [(G.FP64, 1e-12, None), (G.MIXED, 2e-5, "two-pass"),
-                                                     (G.MIXED, 2e-5, "fused"), (G.MIXED, 2e-5, "banded")])
-def test_slab_pipelined_host_call_equals_device_call(n, scramble, precision, rtol, assembly):
+# f_int accumulates in FP64 in both modes (1e-12); mixed-precision K differs between the two calls only
+# by the order of the FP32 reductions: at most 2.7e-7 of the largest entry measured on a B200
+@pytest.mark.parametrize("precision,ftol,ktol,assembly", [(G.FP64, 1e-12, 1e-12, None),
+                                                          (G.MIXED, 1e-12, 1e-6, "two-pass"),
+                                                          (G.MIXED, 1e-12, 1e-6, "fused"),
+                                                          (G.MIXED, 1e-12, 1e-6, "banded")])
+def test_slab_pipelined_host_call_equals_device_call(n, scramble, precision, ftol, ktol, assembly):
     import torch
     X, conn = _mesh(n, scramble)
     g = G.ElementLoop(X, conn, G.CNH, CNH_P, precision=precision)
@@ -49,12 +53,12 @@ def test_slab_pipelined_host_call_equals_device_call(n, scramble, precision, rto
         g.evaluate_device(0.1, dU, df, dk)
         torch.cuda.synchronize()
         f_d, k_d = df.cpu().numpy(), dk.cpu().numpy()
-        assert np.abs(f_h - f_d).max() <= rtol * np.abs(f_d).max()
-        assert np.abs(k_h - k_d).max() <= rtol * np.abs(k_d).max()
+        assert np.abs(f_h - f_d).max() <= ftol * np.abs(f_d).max()
+        assert np.abs(k_h - k_d).max() <= ktol * np.abs(k_d).max()
         # every K entry was written by the host call: a second call into fresh zeros gives K again
         # (an entry the call skipped would stay 0; exact zero counts are not compared, since a sum of
         # FP32 contributions may cancel to 0.0 in one atomic order and not in another)
         f_h2, k_h2, _, _ = g.evaluate(0.1, U)
-        assert np.abs(k_h2 - k_d).max() <= rtol * np.abs(k_d).max()
+        assert np.abs(k_h2 - k_d).max() <= ktol * np.abs(k_d).max()
     finally:
         g.close()
