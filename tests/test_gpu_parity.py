@@ -120,6 +120,44 @@ def test_evaluate_mixed(model, params, amp, ftol, ktol, assembly):
     g.close()
 
 
+def test_block_slots_clean_across_evaluations_and_assemblies():
+    """Every mixed-precision assembly leaves its FP32 block slots at zero for the next evaluation.  A
+    sequence of evaluations on a mesh of two host-call slabs (32^3 elements) -- host-buffer and device
+    calls, one without a tangent, and switches to the fused and banded assemblies (which resize the
+    slots) and back -- gives the oracle's f_int and K at every evaluation with a tangent (bars of
+    test_evaluate_mixed for this model)."""
+    import torch
+    X, conn = meshgen.structured_box(32, 32, 32, jitter=0.05, seed=4)
+    g, o = _pair(G.CNH, CNH_P, X, conn, precision=G.MIXED)
+    U = smooth_u(X, 0.08, seed=5)
+    fo, ko, rco, _ = o.evaluate(0.0, U)
+    assert rco == 0
+    dU = torch.tensor(U, dtype=torch.float64, device="cuda")
+    steps = ["host", "host", "device", "no-tangent", "host", "fused", "two-pass", "device", "banded",
+             "two-pass", "host", "host"]
+    for k, step in enumerate(steps):
+        if step in ("fused", "banded", "two-pass"):
+            g.set_assembly(step)
+            step = "host"
+        if step == "no-tangent":
+            fg, kg, rc, _ = g.evaluate(0.0, U, tangent=False)
+            assert rc == 0 and kg is None
+            assert relerr(fg, fo) <= 2e-6, (k, "fint")
+            continue
+        if step == "device":
+            df = torch.zeros(g.n_dof, dtype=torch.float64, device="cuda")
+            dk = torch.zeros(g.nnz, dtype=torch.float64, device="cuda")
+            g.evaluate_device(0.0, dU, df, dk)
+            torch.cuda.synchronize()
+            fg, kg = df.cpu().numpy(), dk.cpu().numpy()
+        else:
+            fg, kg, rc, _ = g.evaluate(0.0, U)
+            assert rc == 0
+        assert relerr(fg, fo) <= 2e-6, (k, g.assembly, "fint")
+        assert relerr(kg, ko) <= 1e-6, (k, g.assembly, "K")
+    g.close()
+
+
 def test_mixed_near_incompressible_shear_patch():
     """Mixed precision on the benchmark's problem (visco-Prony, K = 100 mu, simple shear after two
     committed increments) on a 16^3 mesh: the interior nodal forces cancel, so f_int is small against
