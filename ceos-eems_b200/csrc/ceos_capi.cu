@@ -141,6 +141,8 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
             a.ring_mask = h->band_ring - 1;
             a.csr_rs = h->d_rs;
             a.conv = static_cast<const int4*>(h->d_bconv);
+            a.conv_meta = static_cast<const longlong2*>(h->d_bconv_meta);
+            a.sched_err = h->d_sched_err;
             {
                 const int r = ensure_band_streams(h);
                 if (r) return r;
@@ -168,7 +170,7 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
                 CK(cudaStreamWaitEvent(h->conv_stream, h->ev_band[c], 0));
                 const int j0 = h->band_conv[c], j1 = h->band_conv[c + 1];
                 if (j1 > j0) {
-                    csr_convert_kernel<<<std::min(j1 - j0, h->conv_grid), kThreads, kStageRegion, h->conv_stream>>>(
+                    csr_convert_kernel<<<std::min(j1 - j0, h->conv_grid), kThreads, kBulkSmem, h->conv_stream>>>(
                         a, nullptr, j0, j1);
                     CK(cudaGetLastError());
                 }
@@ -200,6 +202,8 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
             a.ring_mask = h->scratch_mask;  // covers every block: no slot is shared
             a.csr_rs = h->d_rs;
             a.conv = static_cast<const int4*>(h->d_conv);
+            a.conv_meta = static_cast<const longlong2*>(h->d_conv_meta);
+            a.sched_err = h->d_sched_err;
             const int j0 = slab < 0 ? 0 : h->slab_conv[slab], j1 = slab < 0 ? h->n_conv : h->slab_conv[slab + 1];
             CK(cudaFuncSetAttribute(element_loop_kernel<float, MODEL, SCATTER_RING>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -211,7 +215,7 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
             }
             if (timed) CK(cudaEventRecord(h->ev_k1, s));
             if (j1 > j0) {
-                csr_convert_kernel<<<std::min(j1 - j0, h->conv_grid), kThreads, kStageRegion, s>>>(a, h->d_conv_order,
+                csr_convert_kernel<<<std::min(j1 - j0, h->conv_grid), kThreads, kBulkSmem, s>>>(a, h->d_conv_order,
                                                                                                  j0, j1);
                 CK(cudaGetLastError());
             }
@@ -604,12 +608,35 @@ static int ensure_copy_stream(Handle* h) {
     return 0;
 }
 
+// Metadata of conversion items for csr_convert_kernel, two longlong2 per item: {first block, first K
+// position}, {first node | nodes << 32, blocks | K values << 32}, checked against the kernel's buffers.
+static int upload_conv_meta(Handle* h, const std::vector<ConvItem>& items, void** dst) {
+    std::vector<long long> m(4 * std::max<size_t>(items.size(), 1), 0);
+    auto bb = [&](int n) { return (long long)n + (h->rs[n] - 6LL * n) / 9; };
+    for (size_t j = 0; j < items.size(); ++j) {
+        const int n0 = items[j].n0, n1 = items[j].n1, last = n1 - 1;
+        const long long nblk = n1 > n0 ? bb(last) + 1 + h->nup[last] - bb(n0) : 0;
+        const long long nval = n1 > n0 ? h->rs[last] + 6 + 9LL * h->nup[last] - h->rs[n0] : 0;
+        if (n1 - n0 < 1 || n1 - n0 > kBulkNodes || nblk > kBulkBlocks || nval > kBulkStage - 1) {
+            h->msg = "conversion item " + std::to_string(j) + " exceeds the conversion buffers";
+            return CEOS_E_MESH;
+        }
+        m[4 * j] = bb(n0);
+        m[4 * j + 1] = h->rs[n0];
+        m[4 * j + 2] = (long long)n0 | ((long long)(n1 - n0) << 32);
+        m[4 * j + 3] = nblk | (nval << 32);
+    }
+    CK(cudaMalloc(dst, m.size() * sizeof(long long)));
+    CK(cudaMemcpy(*dst, m.data(), m.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    return 0;
+}
+
 // Work queue of the fused element loop + assembly (mixed mode): planned on the host
 // (plan_schedule, schedule.cpp), uploaded with the ring of node-pair blocks it sizes.
 static int build_schedule(Handle* h) {
     SchedulePlan p;
     const int rc = plan_schedule(h->n_nodes, h->n_elem, h->conn0.data(), h->rs.data(), h->nup.data(), h->n_blocks,
-                                 h->slab_e, h->slab_node_end, kTileE, h->grid_cap, kStageDoubles, kConvNodes, p);
+                                 h->slab_e, h->slab_node_end, kTileE, h->grid_cap, kBulkStage, kBulkNodes, p);
     if (rc) {
         h->msg = p.err;
         return rc;
@@ -625,6 +652,10 @@ static int build_schedule(Handle* h) {
     static_assert(sizeof(ConvItem) == sizeof(int4) && sizeof(TileWait) == sizeof(int2), "item layouts");
     CK(cudaMalloc(&h->d_conv, J * sizeof(int4)));
     CK(cudaMemcpy(h->d_conv, p.conv.data(), J * sizeof(int4), cudaMemcpyHostToDevice));
+    {
+        const int mrc = upload_conv_meta(h, p.conv, &h->d_conv_meta);
+        if (mrc) return mrc;
+    }
     CK(cudaMalloc(&h->d_tile_wait, T * sizeof(int2)));
     CK(cudaMemcpy(h->d_tile_wait, p.tile_wait.data(), T * sizeof(int2), cudaMemcpyHostToDevice));
     // tile and item flags, then one flag that nothing ever sets (ceos_test_stall_conversion)
@@ -664,8 +695,8 @@ static int build_schedule(Handle* h) {
     CK(cudaMalloc(&h->d_kblk, (size_t)h->kblk_slots * 12 * sizeof(float)));
     CK(cudaMemset(h->d_kblk, 0, (size_t)h->kblk_slots * 12 * sizeof(float)));
     int per_sm = 1, sms = 148;
-    CK(cudaFuncSetAttribute(csr_convert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageRegion));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csr_convert_kernel, kThreads, kStageRegion));
+    CK(cudaFuncSetAttribute(csr_convert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBulkSmem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csr_convert_kernel, kThreads, kBulkSmem));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
     h->conv_grid = sms * std::max(1, per_sm);
     // banded two-pass assembly: bands of two waves of tiles
@@ -673,7 +704,7 @@ static int build_schedule(Handle* h) {
         BandPlan bp;
         const int band_elems = std::max(1, 2 * h->grid_cap) * kTileE;
         const int brc = plan_bands(h->n_nodes, h->n_elem, h->conn0.data(), h->rs.data(), h->nup.data(), h->n_blocks,
-                                   band_elems, kTileE, kStageDoubles, kConvNodes, h->band_depth, bp);
+                                   band_elems, kTileE, kBulkStage, kBulkNodes, h->band_depth, bp);
         if (brc) {
             h->msg = bp.err;
             return brc;
@@ -686,6 +717,8 @@ static int build_schedule(Handle* h) {
         const size_t nbc = bp.conv.size();
         CK(cudaMalloc(&h->d_bconv, std::max<size_t>(nbc, 1) * sizeof(int4)));
         if (nbc) CK(cudaMemcpy(h->d_bconv, bp.conv.data(), nbc * sizeof(int4), cudaMemcpyHostToDevice));
+        const int mrc = upload_conv_meta(h, bp.conv, &h->d_bconv_meta);
+        if (mrc) return mrc;
     }
     return 0;
 }
@@ -702,13 +735,14 @@ extern "C" int ceos_evaluate_device(void* handle, double time, const double* U_d
 extern "C" int ceos_status(void* handle, int* n_failed) {
     Handle* h = static_cast<Handle*>(handle);
     if (!h) return CEOS_E_ARG;
-    if (h->d_sched_err) {  // a bounded wait of the fused assembly gave up: K is incomplete
+    if (h->d_sched_err) {  // a bounded wait of the K assembly gave up: K is incomplete
         int err = 0;
         CK(cudaMemcpy(&err, h->d_sched_err, sizeof(int), cudaMemcpyDeviceToHost));
         if (err) {
             CK(cudaMemset(h->d_sched_err, 0, sizeof(int)));
             h->ring_dirty = true;
-            h->msg = "fused assembly: a dependency wait exceeded its bound";
+            h->msg = "K assembly: a bounded wait exceeded its bound (a dependency wait of the fused assembly, or "
+                     "a block copy of the conversion pass)";
             return CEOS_E_CUDA;
         }
     }
@@ -1169,7 +1203,7 @@ Handle::~Handle() {
     if (stream) cudaStreamSynchronize(stream);
     void* ptrs[] = {d_X, d_U, d_fint, d_kval, d_conn, d_rs, d_blk0, d_nup, d_ranks, d_elem_status, d_status_count,
                     d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress, d_kblk, d_queue, d_conv,
-                    d_tile_wait, d_flags, d_ticket, d_sched_err, d_conv_order, d_bconv};
+                    d_tile_wait, d_flags, d_ticket, d_sched_err, d_conv_order, d_bconv, d_conv_meta, d_bconv_meta};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (ev_k0) cudaEventDestroy(ev_k0);

@@ -54,6 +54,7 @@ struct Handle {
     int n_bands = 0;
     std::vector<int> band_e, band_node_end, band_conv;
     void* d_bconv = nullptr;              // int4 [band_conv[n_bands]] conversion items of the bands
+    void* d_bconv_meta = nullptr;         // longlong2 [2 band_conv[n_bands]] their conversion-pass metadata
     uint32_t band_ring = 0;
     int band_depth = 3;                   // element band c starts after the conversion of band c - depth
     cudaStream_t band_stream = nullptr;   // odd element bands (even ones run on the caller's stream)
@@ -71,6 +72,7 @@ struct Handle {
     uint32_t ring_blocks = 0;             // power of two; block b lives in slot b & (ring_blocks - 1)
     int* d_queue = nullptr;
     void* d_conv = nullptr;               // int4 [n_conv] {first node, end node, first tile, last tile}
+    void* d_conv_meta = nullptr;          // longlong2 [2 n_conv] metadata of the items for the conversion pass
     void* d_tile_wait = nullptr;          // int2 [n_tiles] conversion items that last used the tile's slots
     unsigned* d_flags = nullptr;          // [n_tiles] tile done, [n_conv] conversion done (epoch values)
     unsigned* d_ticket = nullptr;         // work counter of the running launch

@@ -99,6 +99,8 @@ struct ElemArgs {
     unsigned* conv_done;    // [n_conv] = epoch once the item's rows are written and slots zeroed
     unsigned epoch;
     const int4* conv;       // [n_conv] {first node, end node, first tile, last tile} of an item
+    const longlong2* conv_meta;  // [2 n_conv] conversion pass: {first block, first K position},
+                                 // {first node | nodes << 32, blocks | K values << 32} of an item
     const int2* tile_wait;  // [n_tiles] items [x, y) that last used the ring slots of the tile
     int* sched_err;         // set when a wait exceeds its bound
 };
@@ -893,19 +895,238 @@ CEOS_D void convert_rows(const ElemArgs<float>& a, int n0, int n1, double* stage
     }
 }
 
-// Conversion pass of the two-pass assembly: CTA k converts the items order[j0 + k], order[j0 + k +
-// gridDim.x], ... < j1 (conversion items of one element slab, or all of them; items j themselves
-// when order is null, as for the bands of the banded assembly).  The element passes before it in
-// stream order have completed every reduction into their blocks.  Dynamic shared memory:
-// kStageRegion bytes (the staging of one item and its node table).
-__global__ void __launch_bounds__(kThreads) csr_convert_kernel(ElemArgs<float> a, const int* order, int j0, int j1) {
+// ---------------------------------------------------------------------------------------------
+// Conversion pass of the two-pass and banded assemblies (csr_convert_kernel)
+// ---------------------------------------------------------------------------------------------
+// Items of this pass hold at most kBulkNodes nodes and kBulkStage - 1 K values, so at most
+// kBulkBlocks node-pair blocks (blocks = nodes + sum of upper neighbours <= nodes + values / 9).
+// Shared memory: two block buffers | FP64 staging of one item | node table | two mbarriers.
+constexpr int kBulkNodes = 128;
+constexpr int kBulkStage = 3072;
+constexpr int kBulkBlocks = kBulkNodes + kBulkStage / 9 + 1;
+constexpr int kBulkRawBytes = kBulkBlocks * 48;
+constexpr int kBulkStageOff = 2 * kBulkRawBytes;
+constexpr int kBulkTableOff = kBulkStageOff + (kBulkStage + 2) * 8;
+constexpr int kBulkMbarOff = kBulkTableOff + 3 * kBulkNodes * 4;
+constexpr int kBulkSmem = kBulkMbarOff + 16;
+static_assert(kBulkRawBytes % 16 == 0 && kBulkStageOff % 16 == 0 && kBulkMbarOff % 8 == 0, "bulk copy alignment");
+static_assert(kBulkStage <= kStageDoubles && kBulkNodes <= kConvNodes, "items must also fit the fused staging");
+
+CEOS_D void mbar_init(uint64_t* m) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(m)) : "memory");
+}
+CEOS_D void mbar_expect_tx(uint64_t* m, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+}
+CEOS_D bool mbar_try_wait(uint64_t* m, unsigned parity) {
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(done) : "r"(smem_u32(m)), "r"(parity) : "memory");
+    return done != 0;
+}
+// Waits for phase `parity` of m for at most kWaitNs; false when the bound ran out.
+CEOS_D bool mbar_wait_bounded(uint64_t* m, unsigned parity) {
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(m, parity))
+        if (global_ns() - t0 > kWaitNs) return false;
+    return true;
+}
+// global -> shared bulk copy (no multicast) completing on mbarrier m; 16-byte aligned, size % 16 == 0
+CEOS_D void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* m) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m)) : "memory");
+}
+// shared -> global bulk copy in the thread's bulk group; 16-byte aligned, size % 16 == 0
+CEOS_D void bulk_store(void* dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n"
+                 ::"l"(dst), "r"(smem_u32(src)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+CEOS_D void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+CEOS_D void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+CEOS_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// Node table of an item, loaded one item ahead into registers: thread t < nodes holds node n0 + t.
+struct ConvRow {
+    long long blk, pos;  // first node-pair block and first K position of the node
+    int up;              // upper neighbours
+};
+
+// CTA k converts the items order[j0 + k], order[j0 + k + gridDim.x], ... < j1 (the conversion items of
+// one element slab, or all of them; items j themselves when order is null, as for the bands of the
+// banded assembly); the element passes before it in stream order have completed every reduction
+// into their blocks.  Software pipeline over the CTA's items, one item ahead:
+//   thread 0 fetches the next item's blocks (one contiguous run of 48-byte blocks, two runs where
+//   it wraps around the ring) into the other block buffer with bulk copies on an mbarrier, from the
+//   item's host-built metadata (no dependent loads);
+//   every thread keeps the next item's node table in registers while it converts the current one,
+//   waits for the current item's blocks, turns whole blocks into the FP64 staging (the node of a
+//   block by binary search in the table) and re-zeroes them in HBM;
+//   thread 0 writes the item's contiguous K run with one bulk store (16-byte aligned middle; the
+//   odd first and last values by plain stores), which drains while the next item converts.
+// Every wait is bounded: a copy that does not land within kWaitNs sets *sched_err (reported as
+// CEOS_E_CUDA, and the next evaluation clears the blocks) and the CTA stops after waiting, again
+// bounded, for the copies it still has in flight.
+__global__ void __launch_bounds__(kThreads, 3) csr_convert_kernel(ElemArgs<float> a, const int* order, int j0, int j1) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* stage = reinterpret_cast<double*>(smem_raw);
-    int* info = reinterpret_cast<int*>(stage + kStageDoubles + 2);
-    for (int j = j0 + (int)blockIdx.x; j < j1; j += (int)gridDim.x) {
-        const int4 c = __ldg(a.conv + (order ? __ldg(order + j) : j));
-        convert_rows<2>(a, c.x, c.y, stage, info, (int)threadIdx.x);
-        __syncthreads();  // the staging is read out before the next item writes it
+    float* raw0 = reinterpret_cast<float*>(smem_raw);
+    float* raw1 = reinterpret_cast<float*>(smem_raw + kBulkRawBytes);
+    double* stage = reinterpret_cast<double*>(smem_raw + kBulkStageOff);
+    int* fb = reinterpret_cast<int*>(smem_raw + kBulkTableOff);  // first block, relative to the item's
+    int* fk = fb + kBulkNodes;                                    // stage index of the first K value
+    int* fm = fk + kBulkNodes;                                    // upper neighbours
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + kBulkMbarOff);
+    __shared__ int s_fail;
+    __shared__ int s_issued[2];
+    const int t = threadIdx.x;
+    const int g = (int)gridDim.x;
+    int j = j0 + (int)blockIdx.x;
+    if (j >= j1) return;
+    const unsigned long long mask = a.ring_mask, ring = mask + 1ull;
+    struct Meta {
+        long long b0, base;
+        int n0, nn, nblk, nval;
+    };
+    auto meta = [&](int jj) {
+        const int id = order ? __ldg(order + jj) : jj;
+        const longlong2 p = __ldg(a.conv_meta + 2 * (size_t)id), q = __ldg(a.conv_meta + 2 * (size_t)id + 1);
+        return Meta{p.x, p.y, (int)(q.x & 0xffffffffLL), (int)(q.x >> 32), (int)(q.y & 0xffffffffLL), (int)(q.y >> 32)};
+    };
+    auto row = [&](const Meta& m) {
+        ConvRow r{0, 0, 0};
+        if (t < m.nn && m.nn <= kBulkNodes) {
+            r.blk = __ldg(a.rs + m.n0 + t);
+            r.pos = __ldg(a.csr_rs + m.n0 + t);
+            r.up = __ldg(a.nup + m.n0 + t);
+        }
+        return r;
+    };
+    auto in_bounds = [](const Meta& m) {
+        return m.nn >= 1 && m.nn <= kBulkNodes && m.nblk >= 1 && m.nblk <= kBulkBlocks && m.nval >= 6 &&
+               m.nval <= kBulkStage - 1;
+    };
+    // thread 0: bulk copies of the blocks of an item into buffer bf
+    auto issue = [&](const Meta& m, int bf) {
+        if (!in_bounds(m)) {
+            s_issued[bf] = 0;  // outside the planned bounds (the host checks them): never happens
+            return;
+        }
+        float* dst = bf ? raw1 : raw0;
+        mbar_expect_tx(mbar + bf, (unsigned)m.nblk * 48u);
+        const unsigned long long s0 = (unsigned long long)m.b0 & mask;
+        const unsigned long long na = (unsigned long long)m.nblk < ring - s0 ? (unsigned long long)m.nblk : ring - s0;
+        bulk_load(dst, a.kblk + s0 * 12, (unsigned)na * 48u, mbar + bf);
+        if (na < (unsigned long long)m.nblk) bulk_load(dst + na * 12, a.kblk, (unsigned)(m.nblk - (int)na) * 48u, mbar + bf);
+        s_issued[bf] = 1;
+    };
+    unsigned ph0 = 0, ph1 = 0;  // parity of the next phase of each buffer's mbarrier
+    int pend0 = 0, pend1 = 0;   // loads issued into each buffer and not yet landed (used by thread 0)
+    Meta mc = meta(j);                                   // current item
+    ConvRow rc = row(mc);                                // its node table
+    Meta mn = j + g < j1 ? meta(j + g) : Meta{0, 0, 0, 0, 0, 0};  // next item
+    if (t == 0) {
+        mbar_init(mbar);
+        mbar_init(mbar + 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        s_fail = 0;
+        issue(mc, 0);
+        pend0 = s_issued[0];
+    }
+    __syncthreads();
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = 0; j < j1; ++k, j += g) {
+        const int buf = k & 1;
+        const bool has_next = j + g < j1;
+        if (t == 0 && has_next) {  // the other buffer was last read before the end of the previous item
+            fence_proxy_async();
+            issue(mn, buf ^ 1);
+            if (buf) pend0 = s_issued[0];
+            else pend1 = s_issued[1];
+        }
+        // the current item's table into shared memory (the previous item stopped reading it before
+        // the end of its conversion); the next item's table and the one after's metadata are loaded
+        // now and used one item later
+        const int head = (int)(mc.base & 1);  // stage index of K[base + p] is p + head (16-byte pairs)
+        if (t < mc.nn && mc.nn <= kBulkNodes) {
+            fb[t] = (int)(rc.blk - mc.b0);
+            fk[t] = (int)(rc.pos - mc.base) + head;
+            fm[t] = rc.up;
+        }
+        const ConvRow rn = has_next ? row(mn) : ConvRow{0, 0, 0};
+        const Meta mnn = j + 2 * g < j1 ? meta(j + 2 * g) : Meta{0, 0, 0, 0, 0, 0};
+        if (s_issued[buf]) {
+            // the phase of a load that did not land stays current: the clean-up waits for it again
+            if (mbar_wait_bounded(mbar + buf, buf ? ph1 : ph0)) {
+                if (buf) {
+                    ph1 ^= 1u;
+                    pend1 = 0;
+                } else {
+                    ph0 ^= 1u;
+                    pend0 = 0;
+                }
+            } else {
+                atomicOr(&s_fail, 1);
+            }
+        } else if (t == 0) {
+            atomicOr(&s_fail, 2);
+        }
+        if (t == 0) bulk_wait_read_all();  // the previous item's K store has read the staging
+        __syncthreads();
+        if (s_fail) break;
+        const float* rb = buf ? raw1 : raw0;
+        const int nn = mc.nn, nblk = mc.nblk, L = mc.nval;
+        for (int q = t; q < nblk; q += kThreads) {
+            const float4* src = reinterpret_cast<const float4*>(rb + (size_t)q * 12);
+            const float4 v0 = src[0], v1 = src[1], v2 = src[2];
+            float4* gb = reinterpret_cast<float4*>(a.kblk + (size_t)(((unsigned long long)mc.b0 + q) & mask) * 12);
+            __stcg(gb, zero);  // re-zero the slot for the next evaluation
+            __stcg(gb + 1, zero);
+            __stcg(gb + 2, zero);
+            int lo = 0, hi = nn - 1;  // the node of block q: the last i with fb[i] <= q
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (fb[mid] <= q) lo = mid;
+                else hi = mid - 1;
+            }
+            const int jb = q - fb[lo], m = fm[lo], rel = fk[lo];
+            const int r1 = rel + 3 + 3 * m, r2 = r1 + 2 + 3 * m;  // rows 3n+1 and 3n+2
+            if (jb == 0) {  // diagonal block: entries l = k..2 of row k
+                stage[rel] = v0.x; stage[rel + 1] = v0.y; stage[rel + 2] = v0.z;
+                stage[r1] = v1.y; stage[r1 + 1] = v1.z;
+                stage[r2] = v2.z;
+            } else {
+                double* d0 = stage + rel + 3 + 3 * (jb - 1);
+                double* d1 = stage + r1 + 2 + 3 * (jb - 1);
+                double* d2 = stage + r2 + 1 + 3 * (jb - 1);
+                d0[0] = v0.x; d0[1] = v0.y; d0[2] = v0.z;
+                d1[0] = v1.x; d1[1] = v1.y; d1[2] = v1.z;
+                d2[0] = v2.x; d2[1] = v2.y; d2[2] = v2.z;
+            }
+        }
+        fence_proxy_async();  // staging writes (and block reads) ordered before the bulk copies that follow
+        __syncthreads();
+        double* K = a.kval + mc.base - head;  // 16-byte aligned: base - head is even
+        const int pa = (head + 1) & ~1, pb = (head + L) & ~1;
+        if (pb > pa) {
+            if (t == 0) bulk_store(K + pa, stage + pa, (unsigned)(pb - pa) * 8u);
+            if (t == 32 && head) __stcs(K + 1, stage[1]);
+            if (t == 64 && ((head + L) & 1)) __stcs(K + head + L - 1, stage[head + L - 1]);
+        } else {
+            for (int p = head + t; p < head + L; p += kThreads) __stcs(K + p, stage[p]);
+        }
+        mc = mn;
+        rc = rn;
+        mn = mnn;
+    }
+    if (t == 0) {
+        if (s_fail) {
+            if (a.sched_err) atomicOr(a.sched_err, 1);
+            // copies still in flight into this CTA's shared memory: wait for them, bounded
+            if (pend0) (void)mbar_wait_bounded(mbar, ph0);
+            if (pend1) (void)mbar_wait_bounded(mbar + 1, ph1);
+        }
+        bulk_wait_all();  // the K stores are complete
     }
 }
 

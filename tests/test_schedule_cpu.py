@@ -321,3 +321,50 @@ def test_band_ring_stays_small_on_a_swept_mesh(band_planner):
     rmax = 1 << int(np.ceil(np.log2(P["n_blocks"])))
     assert P["span"] <= P["n_blocks"] / 2 and P["R"] < rmax
     check_bands(P)
+
+
+# ---- item bounds of the bulk-copy conversion pass (csr_convert_kernel) ----
+
+def _bulk_limits():
+    """kBulkNodes, kBulkStage and kBulkBlocks as the kernel header defines them."""
+    import re
+    src = open(os.path.join(ROOT, "ceos-eems_b200", "csrc", "element_kernel.cuh")).read()
+    nodes = int(re.search(r"constexpr int kBulkNodes = (\d+);", src).group(1))
+    stage = int(re.search(r"constexpr int kBulkStage = (\d+);", src).group(1))
+    assert "constexpr int kBulkBlocks = kBulkNodes + kBulkStage / 9 + 1;" in src
+    return nodes, stage, nodes + stage // 9 + 1
+
+
+def _check_bulk_items(P, nodes_max, stage_max, blocks_max):
+    rs, nup = P["rs"], P["nup"]
+    bb = np.arange(P["N"]) + (rs - 6 * np.arange(P["N"])) // 9
+    for n0, n1, _, _ in P["conv"]:
+        nval = rs[n1 - 1] + 6 + 9 * nup[n1 - 1] - rs[n0]
+        nblk = bb[n1 - 1] + 1 + nup[n1 - 1] - bb[n0]
+        assert 1 <= n1 - n0 <= nodes_max
+        assert nval <= stage_max - 1  # the staging holds the values and one alignment slot
+        assert nblk <= blocks_max     # one block buffer holds the item's blocks
+        assert nblk * 48 % 16 == 0
+
+
+@pytest.mark.parametrize("case", ["cube", "plate", "shuffled"])
+def test_conversion_items_fit_the_bulk_buffers(planner, band_planner, case):
+    """Items planned with the conversion kernel's limits (two-pass items from plan_schedule, banded
+    items from plan_bands) fit its shared-memory buffers: at most kBulkNodes nodes, kBulkStage - 1 K
+    values and kBulkBlocks node-pair blocks, the bounds the kernel checks before each bulk copy."""
+    nodes_max, stage_max, blocks_max = _bulk_limits()
+    if case == "cube":
+        X, conn = meshgen.structured_box(14, 14, 14, jitter=0.05, seed=0)
+    elif case == "plate":
+        X, conn = meshgen.structured_box(24, 24, 6, lx=2.0, ly=2.0, jitter=0.05, seed=0)
+    else:
+        X, conn = meshgen.structured_box(9, 8, 7, jitter=0.05, seed=1)
+        rng = np.random.default_rng(5)
+        perm = rng.permutation(X.shape[0])
+        Xn = np.empty_like(X)
+        Xn[perm] = X
+        X, conn = Xn, (perm[conn - 1] + 1)[rng.permutation(conn.shape[0])].astype(np.int32)
+    P = plan(planner, X, conn, ns=2, stage_max=stage_max, max_nodes=nodes_max)
+    _check_bulk_items(P, nodes_max, stage_max, blocks_max)
+    B = plan_bands(band_planner, X, conn, band_elems=128, depth=3, stage_max=stage_max, max_nodes=nodes_max)
+    _check_bulk_items(B, nodes_max, stage_max, blocks_max)
