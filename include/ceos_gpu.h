@@ -103,6 +103,11 @@ int ceos_evaluate(void* handle, double time, const double* U, double* fint, doub
  * asynchronous: the status is read by ceos_status() after the caller synchronizes. */
 int ceos_evaluate_device(void* handle, double time, const double* U_device, double* fint_device,
                          double* kval_device, void* stream);
+/* Status of the last evaluation: 0; when elements failed (n_failed of them; ceos_last_error names
+ * them) the reference's ClassStatus code of the worst one (1 det J <= 1e-13, 2 a failed constitutive
+ * update, 3 a non-finite stress); or CEOS_E_CUDA when a bounded wait of the mixed-precision K assembly
+ * gave up (a dependency wait of the fused assembly or a block copy of the conversion pass; K is
+ * incomplete and the next evaluation clears the FP32 blocks). */
 int ceos_status(void* handle, int* n_failed);
 
 /* SwitchConvergedState (ModFEMAnalysis.f90:1349-1353) for every Gauss point; the time of the
