@@ -130,9 +130,11 @@ struct SmemLayout {
         total = o;
     }
 };
-// The conversion of a run of CSR rows stages its FP64 values in the g and ds regions (unused
-// between tiles), followed by a table of its nodes (first block, first K value, upper neighbours),
-// so an item holds at most kConvNodes nodes and kStageDoubles K values.
+// The fused kernel's conversion of a run of CSR rows stages its FP64 values in the g and ds regions
+// (unused between tiles), followed by a table of its nodes (first block, first K value, upper
+// neighbours), so an item it converts holds at most kConvNodes nodes and kStageDoubles K values.  The
+// items are planned to the tighter bounds of the conversion pass (kBulkNodes, kBulkStage), which
+// both kernels then hold.
 constexpr int kConvNodes = 256;
 constexpr int kStageRegion = (int)(sizeof(float) * 8 * 8 * kTileE * 4 + sizeof(float) * 8 * 7 * kTileE * 4);
 constexpr int kStageDoubles = (kStageRegion - 3 * kConvNodes * (int)sizeof(int)) / 8 - 2;
