@@ -140,8 +140,7 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
             a.kblk = h->d_kblk;
             a.ring_mask = h->band_ring - 1;
             a.csr_rs = h->d_rs;
-            a.conv = static_cast<const int4*>(h->d_bconv);
-            a.conv_meta = static_cast<const longlong2*>(h->d_bconv_meta);
+            a.conv_meta = static_cast<const longlong2*>(h->d_bconv_meta);  // the bands' conversion items
             a.sched_err = h->d_sched_err;
             {
                 const int r = ensure_band_streams(h);
@@ -201,10 +200,9 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
             a.kblk = h->d_kblk;
             a.ring_mask = h->scratch_mask;  // covers every block: no slot is shared
             a.csr_rs = h->d_rs;
-            a.conv = static_cast<const int4*>(h->d_conv);
-            a.conv_meta = static_cast<const longlong2*>(h->d_conv_meta);
+            a.conv_meta = static_cast<const longlong2*>(h->d_conv_meta);  // the two-pass conversion items
             a.sched_err = h->d_sched_err;
-            const int j0 = slab < 0 ? 0 : h->slab_conv[slab], j1 = slab < 0 ? h->n_conv : h->slab_conv[slab + 1];
+            const int j0 = slab < 0 ? 0 : h->slab_conv[slab], j1 = slab < 0 ? h->n_conv2 : h->slab_conv[slab + 1];
             CK(cudaFuncSetAttribute(element_loop_kernel<float, MODEL, SCATTER_RING>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             const int n_tiles = (e1 - e0 + kTileE - 1) / kTileE;
@@ -635,11 +633,23 @@ static int upload_conv_meta(Handle* h, const std::vector<ConvItem>& items, void*
 // (plan_schedule, schedule.cpp), uploaded with the ring of node-pair blocks it sizes.
 static int build_schedule(Handle* h) {
     SchedulePlan p;
+    // the fused queue, with conversion items sized to the fused kernel's staging
     const int rc = plan_schedule(h->n_nodes, h->n_elem, h->conn0.data(), h->rs.data(), h->nup.data(), h->n_blocks,
-                                 h->slab_e, h->slab_node_end, kTileE, h->grid_cap, kBulkStage, kBulkNodes, p);
+                                 h->slab_e, h->slab_node_end, kTileE, h->grid_cap, kStageDoubles, kConvNodes, p);
     if (rc) {
         h->msg = p.err;
         return rc;
+    }
+    // the two-pass conversion items, sized to the conversion pass's buffers (same cuts at the slab prefixes)
+    SchedulePlan p2;
+    {
+        const int rc2 = plan_schedule(h->n_nodes, h->n_elem, h->conn0.data(), h->rs.data(), h->nup.data(),
+                                      h->n_blocks, h->slab_e, h->slab_node_end, kTileE, h->grid_cap, kBulkStage,
+                                      kBulkNodes, p2);
+        if (rc2) {
+            h->msg = p2.err;
+            return rc2;
+        }
     }
     h->queue = p.queue;
     h->slab_q = p.slab_q;
@@ -652,8 +662,9 @@ static int build_schedule(Handle* h) {
     static_assert(sizeof(ConvItem) == sizeof(int4) && sizeof(TileWait) == sizeof(int2), "item layouts");
     CK(cudaMalloc(&h->d_conv, J * sizeof(int4)));
     CK(cudaMemcpy(h->d_conv, p.conv.data(), J * sizeof(int4), cudaMemcpyHostToDevice));
+    h->n_conv2 = (int)p2.conv.size();
     {
-        const int mrc = upload_conv_meta(h, p.conv, &h->d_conv_meta);
+        const int mrc = upload_conv_meta(h, p2.conv, &h->d_conv_meta);
         if (mrc) return mrc;
     }
     CK(cudaMalloc(&h->d_tile_wait, T * sizeof(int2)));
@@ -668,24 +679,25 @@ static int build_schedule(Handle* h) {
     // two-pass assembly: the items of slab c are those whose last tile lies in slab c (their rows are
     // final after slab c); listed slab by slab, in item order within a slab
     {
+        const size_t J2 = h->n_conv2;
         std::vector<int> tile_slab(T, 0);
         for (int c = 0; c < h->n_slabs; ++c)
             for (int t = h->slab_e[c] / kTileE; t < (h->slab_e[c + 1] + kTileE - 1) / kTileE; ++t) tile_slab[t] = c;
         std::vector<int> order;
-        order.reserve(J);
+        order.reserve(J2);
         h->slab_conv.assign(h->n_slabs + 1, 0);
         for (int c = 0; c < h->n_slabs; ++c) {
             h->slab_conv[c] = (int)order.size();
-            for (int j = 0; j < (int)J; ++j)
-                if (tile_slab[p.conv[j].t1] == c) order.push_back(j);
+            for (int j = 0; j < (int)J2; ++j)
+                if (tile_slab[p2.conv[j].t1] == c) order.push_back(j);
         }
         h->slab_conv[h->n_slabs] = (int)order.size();
-        if (order.size() != J) {
+        if (order.size() != J2) {
             h->msg = "schedule: conversion items not assigned to slabs";
             return CEOS_E_MESH;
         }
-        CK(cudaMalloc(&h->d_conv_order, J * sizeof(int)));
-        CK(cudaMemcpy(h->d_conv_order, order.data(), J * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&h->d_conv_order, std::max<size_t>(J2, 1) * sizeof(int)));
+        CK(cudaMemcpy(h->d_conv_order, order.data(), J2 * sizeof(int), cudaMemcpyHostToDevice));
     }
     uint32_t pow2 = 1;
     while ((long long)pow2 < h->n_blocks) pow2 <<= 1;
@@ -1024,7 +1036,7 @@ extern "C" int ceos_launch_count(void* handle, int tangent, int* n_launches) {
     int n = 1;  // the element loop
     if (tangent && h->precision == CEOS_MIXED) {
         if (h->assembly == CEOS_ASSEMBLY_TWO_PASS) {
-            n = 1 + (h->n_conv > 0 ? 1 : 0);
+            n = 1 + (h->n_conv2 > 0 ? 1 : 0);
         } else if (h->assembly == CEOS_ASSEMBLY_BANDED) {
             n = h->n_bands;
             for (int c = 0; c < h->n_bands; ++c) n += h->band_conv[c + 1] > h->band_conv[c] ? 1 : 0;

@@ -72,7 +72,8 @@ struct Handle {
     uint32_t ring_blocks = 0;             // power of two; block b lives in slot b & (ring_blocks - 1)
     int* d_queue = nullptr;
     void* d_conv = nullptr;               // int4 [n_conv] {first node, end node, first tile, last tile}
-    void* d_conv_meta = nullptr;          // longlong2 [2 n_conv] metadata of the items for the conversion pass
+    int n_conv2 = 0;                      // two-pass conversion items (planned to the conversion pass's bounds)
+    void* d_conv_meta = nullptr;          // longlong2 [2 n_conv2] their metadata for the conversion pass
     void* d_tile_wait = nullptr;          // int2 [n_tiles] conversion items that last used the tile's slots
     unsigned* d_flags = nullptr;          // [n_tiles] tile done, [n_conv] conversion done (epoch values)
     unsigned* d_ticket = nullptr;         // work counter of the running launch
