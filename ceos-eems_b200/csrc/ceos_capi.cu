@@ -111,6 +111,7 @@ int launch_model(Handle* h, double dt, const double* dU, double* dfint, double* 
         for (int k = 0; k < 4 && k < (int)h->host_params[2]; ++k)
             a.ebr[k] = (T)std::exp(-dt / (2.0 * h->host_params[4 + 2 * k]));
     a.X = h->d_X;
+    a.jxi = h->d_jxi;
     a.U = dU;
     a.conn = h->d_conn;
     a.nup = h->d_nup;
@@ -1138,6 +1139,29 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
         CK(cudaMalloc(&d_blk0, N * sizeof(long long)));
         CK(cudaMemcpy(d_blk0, blk0.data(), N * sizeof(long long), cudaMemcpyHostToDevice));
     }
+    if (precision == CEOS_MIXED) {
+        // reference geometry of every Gauss point for the FP32 element arithmetic: J_X^-1 and det J_X
+        // in FP64 (J_X = sum_n dN_n/dxi (x) X_n, ModElement.f90:1210-1300), rounded once to FP32
+        double tab[8][8][3];
+        hexa8_dN_table(tab);
+        std::vector<float> G((size_t)10 * 8 * ld, 0.f);
+        for (size_t e = 0; e < E; ++e) {
+            const int* cn = conn0.data() + 8 * e;
+            for (int gp = 0; gp < 8; ++gp) {
+                double J[3][3] = {};
+                for (int n = 0; n < 8; ++n)
+                    for (int i = 0; i < 3; ++i)
+                        for (int j = 0; j < 3; ++j) J[i][j] += tab[gp][n][i] * mesh->X[3 * (size_t)cn[n] + j];
+                const double d = det3(J);
+                double Ji[3][3] = {};
+                if (std::fabs(d) > 1e-300) inv3(J, d, Ji);
+                for (int k = 0; k < 9; ++k) G[((size_t)k * 8 + gp) * ld + e] = (float)Ji[k / 3][k % 3];
+                G[((size_t)9 * 8 + gp) * ld + e] = (float)d;
+            }
+        }
+        CK(cudaMalloc(&d_jxi, G.size() * sizeof(float)));
+        CK(cudaMemcpy(d_jxi, G.data(), G.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
     CK(cudaMalloc(&d_nup, N * sizeof(int)));
     CK(cudaMemcpy(d_nup, nup.data(), N * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&d_ranks, E * 32));
@@ -1213,7 +1237,7 @@ int Handle::allocate_device(const ceos_mesh* mesh, const ceos_material* mats, in
 
 Handle::~Handle() {
     if (stream) cudaStreamSynchronize(stream);
-    void* ptrs[] = {d_X, d_U, d_fint, d_kval, d_conn, d_rs, d_blk0, d_nup, d_ranks, d_elem_status, d_status_count,
+    void* ptrs[] = {d_X, d_jxi, d_U, d_fint, d_kval, d_conn, d_rs, d_blk0, d_nup, d_ranks, d_elem_status, d_status_count,
                     d_params, d_mat_id, d_state[0], d_state[1], d_gp_stress, d_kblk, d_queue, d_conv,
                     d_tile_wait, d_flags, d_ticket, d_sched_err, d_conv_order, d_bconv, d_conv_meta, d_bconv_meta};
     for (void* p : ptrs)

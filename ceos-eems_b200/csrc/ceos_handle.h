@@ -39,6 +39,7 @@ struct Handle {
     int* d_mat_id = nullptr;
     void* d_state[2] = {nullptr, nullptr};
     void* d_gp_stress = nullptr;
+    float* d_jxi = nullptr;               // mixed mode: [10][8][ld] J_X^-1 and det J_X per Gauss point (FP32 of FP64)
     float* d_kblk = nullptr;              // mixed mode: FP32 node-pair block slots, kblk_slots of them: every
                                           // block (two-pass) or the ring of the fused / banded assembly
     long long kblk_slots = 0;

@@ -65,6 +65,7 @@ struct ElemArgs {
     int n_elem;
     int e_begin, e_end;     // element range of this launch (static schedule)
     const double* X;        // [3*n_nodes] reference coordinates (CoordX)
+    const float* jxi;       // FP32 mode: [10][8][ld] J_X^-1 (row-major, 9) and det J_X of every Gauss point
     const double* U;        // [3*n_nodes] displacements, DOF 3n+d
     const int* conn;        // [n_elem*8] 0-based node ids
     const long long* rs;    // [n_nodes] CSR position of the first entry of row 3n (0-based); blocked
@@ -339,6 +340,15 @@ CEOS_D void local_node_f32(const SmemPtrs<float>& s, int n, int el, float X[3], 
     }
 }
 
+// FP32 mode: the displacement of node n of element el relative to the element's node 0, formed in
+// FP64 (J_u is unchanged by the shift because sum_n dN_n/dxi = 0).
+CEOS_D void local_u_f32(const SmemPtrs<float>& s, int n, int el, float u[3]) {
+    const double* up = s.u + (n * kTileE + el) * 3;
+    const double* u0 = s.u + el * 3;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) u[d] = n == 0 ? 0.f : (float)(up[d] - u0[d]);
+}
+
 // Phase A for thread (gp = warp, element = lane) of the tile at e0.
 template <typename T, int MODEL>
 CEOS_D void phase_a(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp, int lane) {
@@ -349,49 +359,83 @@ CEOS_D void phase_a(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp
     // J_X = sum dN/dxi (x) X and J_u = sum dN/dxi (x) u; the current Jacobian is J_X + J_u, and
     // F = I + (J_X^-1 J_u)^T equals DeformationGradient's I + sum u (x) grad_X N with the
     // displacement gradient formed from small numbers (no I + O(1) cancellation in FP32)
-    T JX[3][3] = {}, Ju[3][3] = {};
+    T F[3][3], Jci[3][3], detJ;
+    if constexpr (sizeof(T) == 4) {
+        // J_X^-1 and det J_X of the reference configuration, computed once per mesh in FP64 on the
+        // host ([k][gp][e] rows like the state); J_X + J_u = J_X F^T, so (J_X + J_u)^-1 = F^-T J_X^-1
+        // and det = det J_X det F
+        const float* q = a.jxi + (size_t)gp * a.ld + e;
+        const size_t rstride = (size_t)8 * a.ld;
+        float JXi[3][3];
 #pragma unroll
-    for (int n = 0; n < 8; ++n) {
-        T X[3], u[3];
-        if constexpr (sizeof(T) == 4) {
-            local_node_f32(s, n, el, X, u);
-        } else {
+        for (int k = 0; k < 9; ++k) JXi[k / 3][k % 3] = __ldg(q + k * rstride);
+        const float detJX = __ldg(q + 9 * rstride);
+        float Ju[3][3] = {};
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            float u[3];
+            local_u_f32(s, n, el, u);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const float dn = dN_at<float>(gp, n, i);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) Ju[i][j] += dn * u[j];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                F[i][j] = (i == j ? 1.f : 0.f) + (JXi[j][0] * Ju[0][i] + JXi[j][1] * Ju[1][i] + JXi[j][2] * Ju[2][i]);
+        const float detF = det3(F);
+        detJ = detJX * detF;
+        if (!(detJX > 1.0e-13f) || !(detJ > 1.0e-13f)) status |= 1;
+        float Fi[3][3];
+        inv3(F, detF, Fi);
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) Jci[j][i] = Fi[0][j] * JXi[0][i] + Fi[1][j] * JXi[1][i] + Fi[2][j] * JXi[2][i];
+    } else {
+        T JX[3][3] = {}, Ju[3][3] = {};
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
             const double* xp = s.x + (n * kTileE + el) * 3;
             const double* up = s.u + (n * kTileE + el) * 3;
+            T X[3], u[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 X[d] = (T)xp[d];
                 u[d] = (T)up[d];
             }
-        }
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const T dn = dN_at<T>(gp, n, i);
+            for (int i = 0; i < 3; ++i) {
+                const T dn = dN_at<T>(gp, n, i);
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                JX[i][j] += dn * X[j];
-                Ju[i][j] += dn * u[j];
+                for (int j = 0; j < 3; ++j) {
+                    JX[i][j] += dn * X[j];
+                    Ju[i][j] += dn * u[j];
+                }
             }
         }
+        T Jc[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) Jc[i][j] = JX[i][j] + Ju[i][j];
+        const T detJX = det3(JX);
+        detJ = det3(Jc);
+        if (!(detJX > T(1.0e-13)) || !(detJ > T(1.0e-13))) status |= 1;
+        T JXi[3][3];
+        inv3(JX, detJX, JXi);
+        inv3(Jc, detJ, Jci);
+        // F[i][j] = delta_ij + sum_k JXi[j][k] Ju[k][i]
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                F[i][j] = (i == j ? T(1) : T(0)) + (JXi[j][0] * Ju[0][i] + JXi[j][1] * Ju[1][i] + JXi[j][2] * Ju[2][i]);
     }
-    T Jc[3][3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) Jc[i][j] = JX[i][j] + Ju[i][j];
-    const T detJX = det3(JX);
-    const T detJ = det3(Jc);
-    if (!(detJX > T(1.0e-13)) || !(detJ > T(1.0e-13))) status |= 1;
-    T JXi[3][3], Jci[3][3];
-    inv3(JX, detJX, JXi);
-    inv3(Jc, detJ, Jci);
-    // F[i][j] = delta_ij + sum_k JXi[j][k] Ju[k][i]
-    T F[3][3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-            F[i][j] = (i == j ? T(1) : T(0)) + (JXi[j][0] * Ju[0][i] + JXi[j][1] * Ju[1][i] + JXi[j][2] * Ju[2][i]);
     // current gradients grad_x N of the 8 nodes for phase B
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
