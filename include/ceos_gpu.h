@@ -78,7 +78,10 @@ typedef struct ceos_material {
 /* Build the handle: uploads the mesh, builds the upper CSR pattern
  * (AllocateKgSparseUpperTriangular, ModFEMAnalysis.f90:209-273) and the element-to-CSR
  * slot map, allocates Gauss-point state (virgin state, ConstitutiveModelConstructor) and
- * one CUDA stream.  device = CUDA ordinal. */
+ * one CUDA stream.  CEOS_MIXED also plans the K assembly (conversion items, the fused queue,
+ * the bands) and caches the reference geometry of every Gauss point (J_X^-1 and det J_X,
+ * computed in FP64, 320 bytes per element): the reference coordinates are fixed for the
+ * handle's lifetime.  device = CUDA ordinal. */
 int ceos_create(const ceos_mesh* mesh, const ceos_material* mats, int n_mat, int precision_mode,
                 int device, void** handle);
 
