@@ -244,6 +244,24 @@ def fma_roofline(n_elem, element_ms, clocks, dev):
                     "per SM at the sampled SM clock (the Gauss-point update and phase-A geometry are extra work)"}
 
 
+def conversion_roofline(workload, n_elem, conv_ms, peak):
+    """The conversion pass is HBM-bound: its DRAM bytes (the committed ncu capture, scaled by elements)
+    over its CUDA-event time, against the copy peak."""
+    p = os.path.join(ROOT, "profiles", "element_loop_traffic.json")
+    try:
+        with open(p) as f:
+            per = json.load(f)[workload]["kernel_dram_bytes_per_element"]["csr_convert_kernel"]
+    except Exception:
+        return None
+    if not conv_ms or conv_ms <= 0:
+        return None
+    b = per * n_elem
+    a = b / (conv_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "unit": "GB/s", "dram_bytes": b, "achieved": a, "peak": peak, "frac": a / peak,
+            "what": "csr_convert_kernel: DRAM bytes of one launch (ncu capture, scaled by elements) / its CUDA-event "
+                    "time (FP32 blocks read and re-zeroed, FP64 K written)"}
+
+
 def profile_traffic(workload, n_elem):
     """DRAM bytes of one evaluation (all its kernels) from the committed ncu summary, scaled by elements."""
     p = os.path.join(ROOT, "profiles", "element_loop_traffic.json")
@@ -408,6 +426,8 @@ def run_element_loop(args, w, config, world, rank, local_rank):
                          "algorithmic_bytes_per_launch": alg,
                          "kernel_split_ms": {"element_loop": k_mean, "conversion": c_mean},
                          "compute": fma_roofline(w.n_elem, k_mean, clocks, dev),
+                         "conversion": (conversion_roofline(w.name, w.n_elem, c_mean, peak)
+                                        if getattr(args, "assembly", "two-pass") == "two-pass" else None),
                          "what": "algorithmic bytes of one evaluation / device time of all its kernels (the "
                                  "element loop and the K conversion, CUDA events on the launching stream)"},
             "clocks": clocks}
