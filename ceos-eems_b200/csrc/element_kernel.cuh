@@ -90,7 +90,8 @@ struct ElemArgs {
     int* status_count;      // failed elements
     T* gp_stress;           // [6][8][n_elem] or nullptr
     // ---- mixed-precision K assembly (two-pass element pass and conversion; fused kernel) ----
-    float* kblk;            // FP32 node-pair blocks, 12 floats each, zero between evaluations
+    float* kblk;            // FP32 node-pair blocks, 12 floats each (3 rows of 4; a diagonal block packs its upper
+                            // 6 entries into the first 6 floats), zero between evaluations
     uint32_t ring_mask;     // block b lives in slot b & ring_mask (two-pass: every block its own slot)
     const long long* csr_rs;   // [n_nodes] CSR position of row 3n (0-based)
     const int* queue;       // work items: >= 0 element tile, < 0 conversion item -(j+1)
@@ -320,6 +321,9 @@ CEOS_D void prefetch_nodes_state(const ElemArgs<T>& a, int e0, const int* node_s
 
 CEOS_D void red_v4(float* p, float a, float b, float c, float d) {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+CEOS_D void red_v2(float* p, float a, float b) {
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};\n" ::"l"(p), "f"(a), "f"(b) : "memory");
 }
 
 // FP32 mode: node n of element el as differences to the element's node 0, formed in FP64 from the
@@ -778,9 +782,9 @@ CEOS_D void phase_b(const ElemArgs<T>& a, const SmemPtrs<T>& s, int e0, int warp
         const uint32_t mask = a.ring_mask;
         {
             float* blk = a.kblk + (size_t)((uint32_t)rs_c[b * kTileE + el] & mask) * 12;
-            red_v4(blk + 0, (float)Kd[0], (float)Kd[1], (float)Kd[2], 0.f);
-            red_v4(blk + 4, 0.f, (float)Kd[3], (float)Kd[4], 0.f);
-            red_v4(blk + 8, 0.f, 0.f, (float)Kd[5], 0.f);
+            // diagonal block: its upper 6 entries packed as K00 K01 K02 K11 | K12 K22 (two reductions)
+            red_v4(blk + 0, (float)Kd[0], (float)Kd[1], (float)Kd[2], (float)Kd[3]);
+            red_v2(blk + 4, (float)Kd[4], (float)Kd[5]);
         }
         const uint8_t* rk = reinterpret_cast<const uint8_t*>(ranks_c + el * 8);
 #pragma unroll
@@ -912,10 +916,10 @@ CEOS_D void convert_rows(const ElemArgs<float>& a, int n0, int n1, double* stage
             }
             const int j = q - fb[lo], m = fm[lo], rel = fk[lo];
             const int r1 = rel + 3 + 3 * m, r2 = r1 + 2 + 3 * m;  // rows 3n+1 and 3n+2
-            if (j == 0) {  // diagonal block: entries l = k..2 of row k
+            if (j == 0) {  // diagonal block, packed: K00 K01 K02 K11 | K12 K22
                 stage[rel] = v[u][0].x; stage[rel + 1] = v[u][0].y; stage[rel + 2] = v[u][0].z;
-                stage[r1] = v[u][1].y; stage[r1 + 1] = v[u][1].z;
-                stage[r2] = v[u][2].z;
+                stage[r1] = v[u][0].w; stage[r1 + 1] = v[u][1].x;
+                stage[r2] = v[u][1].y;
             } else {
                 double* d0 = stage + rel + 3 + 3 * (j - 1);
                 double* d1 = stage + r1 + 2 + 3 * (j - 1);
@@ -1137,10 +1141,10 @@ __global__ void __launch_bounds__(kThreads, 3) csr_convert_kernel(ElemArgs<float
             }
             const int jb = q - fb[lo], m = fm[lo], rel = fk[lo];
             const int r1 = rel + 3 + 3 * m, r2 = r1 + 2 + 3 * m;  // rows 3n+1 and 3n+2
-            if (jb == 0) {  // diagonal block: entries l = k..2 of row k
+            if (jb == 0) {  // diagonal block, packed: K00 K01 K02 K11 | K12 K22
                 stage[rel] = v0.x; stage[rel + 1] = v0.y; stage[rel + 2] = v0.z;
-                stage[r1] = v1.y; stage[r1 + 1] = v1.z;
-                stage[r2] = v2.z;
+                stage[r1] = v0.w; stage[r1 + 1] = v1.x;
+                stage[r2] = v1.y;
             } else {
                 double* d0 = stage + rel + 3 + 3 * (jb - 1);
                 double* d1 = stage + r1 + 2 + 3 * (jb - 1);
