@@ -951,8 +951,8 @@ CEOS_D void convert_rows(const ElemArgs<float>& a, int n0, int n1, double* stage
 // Items of this pass hold at most kBulkNodes nodes and kBulkStage - 1 K values, so at most
 // kBulkBlocks node-pair blocks (blocks = nodes + sum of upper neighbours <= nodes + values / 9).
 // Shared memory: two block buffers | FP64 staging of one item | node table | two mbarriers.
-constexpr int kBulkNodes = 128;
-constexpr int kBulkStage = 3072;
+constexpr int kBulkNodes = 96;
+constexpr int kBulkStage = 2048;
 constexpr int kBulkBlocks = kBulkNodes + kBulkStage / 9 + 1;
 constexpr int kBulkRawBytes = kBulkBlocks * 48;
 constexpr int kBulkStageOff = 2 * kBulkRawBytes;
@@ -1018,7 +1018,7 @@ struct ConvRow {
 // Every wait is bounded: a copy that does not land within kWaitNs sets *sched_err (reported as
 // CEOS_E_CUDA, and the next evaluation clears the blocks) and the CTA stops after waiting, again
 // bounded, for the copies it still has in flight.
-__global__ void __launch_bounds__(kThreads, 3) csr_convert_kernel(ElemArgs<float> a, const int* order, int j0, int j1) {
+__global__ void __launch_bounds__(kThreads, 4) csr_convert_kernel(ElemArgs<float> a, const int* order, int j0, int j1) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* raw0 = reinterpret_cast<float*>(smem_raw);
     float* raw1 = reinterpret_cast<float*>(smem_raw + kBulkRawBytes);
